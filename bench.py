@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark: a 30-qubit depth-20 Google-style random circuit in complex64.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: random grid circuit on a 5x6 grid (30 qubits), depth 20: each layer
+applies sqrt(X), sqrt(Y) or sqrt(W) to every qubit (never the qubit's
+previous gate), then CZ on one of four coupler sets; complex64 state (8 GiB)
+from |0...0>. Synthetic: the circuit comes from a fixed seed.
+
+Our arm ("ours"): a step is one run of the circuit through a plan executed
+on the device (the state reset to |0...0> between steps, outside the timed
+work), timed with CUDA events on the library's stream. `value` is seconds per
+circuit (tuned path); the plain path (one pass per fused gate), the per-pass
+HBM roofline, the amplitude error against a complex128 run, the end-to-end
+time of the public `run()` call (host planning, uploads from pinned memory,
+1000 shots, outcomes back to the host) and the CPU baseline are reported
+beside it. With N GPUs each rank runs its own circuit (replicas; the state
+does not shard in this engine) and the step time is the max over ranks.
+
+Reference arm (--impl reference): the reference's CPU engine, restated in C++
+(oracle/; the Rust crate cannot be built here), on all host threads, on a
+bounded prefix of the same circuit scaled to the full depth.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "30q random-circuit s & HBM GB/s vs peak, tuned vs plain GPU at <=1e-6 amp err"
+ROWS, COLS, DEPTH, SEED = 5, 6, 20, 2024
+SHOTS = 1000
+
+
+def workload_config(n: int, depth: int) -> dict:
+    return {
+        "workload": f"random grid circuit {n} qubits, depth {depth}, complex64, from |0...0>",
+        "grid": f"{ROWS}x{COLS}" if n == ROWS * COLS else "custom",
+        "gates": "sqrt(X)/sqrt(Y)/sqrt(W) with no repeat + CZ on 4 coupler sets",
+        "state_bytes": (1 << n) * 8,
+        "l2": "inputs larger than L2 (8 GiB state vs 126 MB)",
+        "parallelism": "replicas (one circuit per GPU)",
+    }
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(ops_all, n: int, layers_ops, budget_s: float = 25.0) -> dict:
+    """The restated reference engine (fusion 4, region_bits 14 = the
+    reference defaults) on the host cores: the full circuit if it fits the
+    time budget, else a prefix of layers scaled to the full depth."""
+    from oracle import oracle
+
+    threads = oracle.max_threads()
+    t0 = time.perf_counter()
+    st = oracle.OracleState(n, 32)
+    alloc = time.perf_counter() - t0
+    try:
+        prefix = 2
+        t0 = time.perf_counter()
+        st.apply_ops(layers_ops(prefix), max_fused=4, region_bits=14)
+        t_prefix = time.perf_counter() - t0
+        estimate = t_prefix * DEPTH / prefix
+        if estimate <= budget_s:
+            st.close()
+            st = oracle.OracleState(n, 32)
+            t0 = time.perf_counter()
+            st.apply_ops(ops_all, max_fused=4, region_bits=14)
+            value = time.perf_counter() - t0
+            sample = f"full circuit ({DEPTH} layers), {n} qubits"
+        else:
+            layers = max(prefix, int(DEPTH * budget_s / estimate))
+            st.close()
+            st = oracle.OracleState(n, 32)
+            t0 = time.perf_counter()
+            st.apply_ops(layers_ops(layers), max_fused=4, region_bits=14)
+            value = (time.perf_counter() - t0) * DEPTH / layers
+            sample = f"first {layers} of {DEPTH} layers, {n} qubits, time scaled by {DEPTH}/{layers}"
+    finally:
+        st.close()
+    return {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample,
+            "alloc_s": alloc, "engine": "C++ restatement of the reference's AVX2 engine (fusion 4, region_bits 14)"}
+
+
+def host_cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def build_circuit(n: int, depth: int):
+    from qevedo_simulator_b200 import library
+
+    if n == ROWS * COLS:
+        rows, cols = ROWS, COLS
+    else:
+        rows, cols = library.grid_shape(n)
+    return library.random_grid_circuit(rows, cols, depth, SEED)
+
+
+def layer_prefix_ops(circuit, n: int):
+    """Ops of the first `layers` layers (each layer: n one-qubit gates + its CZs)."""
+    ins = [i for i in circuit._instructions if i[0] == "gate"]
+    from qevedo_simulator_b200.circuit import gate_op
+
+    def ops(layers: int):
+        out, layer, seen1 = [], 0, 0
+        for g in ins:
+            if g[1].name != "cz":
+                if seen1 == n:
+                    layer += 1
+                    seen1 = 0
+                    if layer == layers:
+                        break
+                seen1 += 1
+            out.append(gate_op(g[1], g[2]))
+        return out
+
+    return ops
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    from oracle import oracle
+
+    n, depth = args.qubits, DEPTH
+    circuit = build_circuit(n, depth)
+    ops = circuit.ops()
+    layers = layer_prefix_ops(circuit, n)
+    steps = []
+    for i in range(args.warmup + args.steps):
+        base = cpu_baseline(ops, n, layers, budget_s=args.cpu_budget)
+        if i >= args.warmup:
+            steps.append(base["value"])
+    value = float(np.mean(steps))
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 (f32 re/im)", "data": "synthetic (seeded random circuit)", "impl": "reference",
+        "config": workload_config(n, depth),
+        "cpu_baseline": {"value": value, "unit": "s", "cores": base["cores"], "kind": "port", "sample": base["sample"],
+                         "cpu": host_cpu_model()},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference Rust crate cannot be built here (no Rust toolchain); timed its C++ restatement (oracle/)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int):
+    import torch
+
+    from qevedo_simulator_b200 import DeviceState, Plan, options, run, set_device
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    n, depth = args.qubits, DEPTH
+    circuit = build_circuit(n, depth)
+    ops = circuit.ops()
+    fused = args.fusion
+    tuned = Plan(ops, n, 32, options(fused, staged=True))
+    plain = Plan(ops, n, 32, options(4, staged=False))
+    st = DeviceState(n, 32)
+    st.set_pass_timing(True)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # Warm-up.
+    for _ in range(args.warmup):
+        st.zero()
+        st.execute(tuned)
+    # Timed steps: device time of each run (CUDA events on the library stream).
+    barrier()
+    torch.cuda.synchronize()
+    times, pass_t, pass_b, pass_k = [], [], [], []
+    wall0 = time.perf_counter()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            st.zero()
+            s = st.execute(tuned)
+            times.append(s["gate_seconds"])
+            sec, byt, kind = st.pass_times()
+            pass_t.append(sec)
+            pass_b.append(byt)
+            pass_k.append(kind)
+    torch.cuda.synchronize()
+    barrier()
+    wall = time.perf_counter() - wall0
+    step = float(np.mean(times))
+    if dist is not None:
+        t = torch.tensor([step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step = float(t.item())
+    info = tuned.info()
+    # Plain path (one pass per fused gate, the reference's region_bits=None).
+    plain_times = []
+    for _ in range(max(1, min(2, args.steps))):
+        st.zero()
+        plain_times.append(st.execute(plain)["gate_seconds"])
+    plain_s = float(np.mean(plain_times))
+    plain_info = plain.info()
+    # Roofline of the dominant kernel: the staged tile pass.
+    sec = np.concatenate(pass_t)
+    byt = np.concatenate(pass_b)
+    kind = np.concatenate(pass_k)
+    peaks = measured_peaks()
+    staged_sec = sec[kind == 1]
+    staged_bytes = byt[kind == 1]
+    avg = float(staged_sec.mean()) if staged_sec.size else float(sec.mean())
+    per_launch = float(staged_bytes.mean()) if staged_bytes.size else float(byt.mean())
+    achieved = per_launch / avg / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": args.traffic, "kernel": "k_stage<float>",
+                "peak_source": peaks["source"], "bytes_per_launch": per_launch, "avg_launch_s": avg,
+                "whole_run_gbs": info["bytes"] / step / 1e9}
+    # Accuracy: tuned complex64 against a complex128 run of the same circuit.
+    err = None
+    if not args.skip_check:
+        st.zero()
+        st.execute(tuned)
+        with DeviceState(n, 64) as ref:
+            ref.apply_ops(ops, options(4, staged=False))
+            err = ref.max_abs_diff(st)
+    # End to end through the public API: plan on the host, upload gate data
+    # from pinned memory, run, sample SHOTS shots, outcomes back to the host.
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        res = run(circuit.copy().measure_all(), SHOTS, seed=7 + i, max_fused_qubits=fused, state=st)
+        if i >= args.warmup:
+            e2e.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(e2e))
+    h2d = tuned_upload_bytes(ops) + 8 * SHOTS
+    d2h = 8 * SHOTS + 16
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = cpu_baseline(ops, n, layer_prefix_ops(circuit, n), budget_s=args.cpu_budget)
+        cpu["cpu"] = host_cpu_model()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": step, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64 (f32 re/im)", "data": "synthetic (seeded random circuit)",
+            "config": workload_config(n, depth),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "call": f"qevedo_simulator_b200.run(circuit, shots={SHOTS}) on a reused device state"},
+            "gpu_launches": int(info["passes"]) * args.steps,
+            "clocks": clocks.summary(),
+            "tuned": {"s": step, "passes": info["passes"], "stages": info["stages"], "kernels": info["kernels"],
+                      "max_fused_qubits": fused},
+            "plain": {"s": plain_s, "passes": plain_info["passes"], "kernels": plain_info["kernels"]},
+            "tuned_over_plain": step / plain_s,
+            "max_amp_err_vs_c128": err,
+            "gates": info["gates"],
+            "wall_s_timed_region": wall,
+        }
+        print(json.dumps(line), flush=True)
+    tuned.close()
+    plain.close()
+    st.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def tuned_upload_bytes(ops) -> int:
+    """Upper bound of the gate-program and matrix bytes a plan uploads per
+    run (complex64 matrices plus a 96-byte descriptor per op)."""
+    return int(sum(8 * 4 ** len(o.targets) for o in ops) + 96 * len(ops))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--fusion", type=int, default=4)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-check", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=25.0)
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="DRAM bytes per stage launch from an ncu capture (reported as roofline.traffic)")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,242 @@
+/*
+ * qvdg.h — C ABI of the B200 state-vector engine (libqvdgpu.so).
+ *
+ * The engine replaces the CPU state-vector backend of the qvd crate
+ * (qevedo-simulator 0.1.18). Every entry point names the reference function
+ * or method it stands in for, as `file:line` inside the reference crate.
+ *
+ * Conventions (the same as the reference, src/state.rs:10-16 and
+ * src/matrix.rs:3-5):
+ *   - amplitude `i` has qubit `q` equal to bit `q` of `i` (qubit 0 is the
+ *     least significant bit, as in Qiskit);
+ *   - a gate matrix on qubits [q0, q1, ...] has index bit j = qubit qj; it is
+ *     given as 2^k x 2^k complex128 values, row-major, (re, im) interleaved;
+ *   - amplitudes cross the ABI in logical order as complex128 (re, im)
+ *     interleaved, whatever the device precision.
+ *
+ * Every call returns a status and never aborts; `qvdg_last_error` gives the
+ * message of the last failing call on the calling thread. A state handle is
+ * used by one caller at a time (the reference takes `&mut self`). All calls
+ * are synchronous from the host's point of view.
+ */
+#ifndef QVDG_H
+#define QVDG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  QVDG_OK = 0,
+  /* invalid input: qubit out of range or repeated, bad matrix shape, ...
+   * (reference: assert!/panic!, src/state.rs:182-188, src/kernels.rs:511-514) */
+  QVDG_ERR_INVALID = 1,
+  /* device memory could not be allocated (reference: io::Error from mmap,
+   * src/memory.rs:121-123) */
+  QVDG_ERR_OUT_OF_MEMORY = 2,
+  /* a CUDA runtime call failed; the message names it */
+  QVDG_ERR_CUDA = 3,
+  /* the request is valid but this build does not run it */
+  QVDG_ERR_UNSUPPORTED = 4,
+  /* a bounded device-side wait gave up (batched persistent launch) */
+  QVDG_ERR_TIMEOUT = 5
+} qvdg_status;
+
+/* Widest dense gate a kernel applies (targets only; controls are handled by
+ * restricting the index range). Reference: MAX_GATE_QUBITS, src/kernels.rs:476. */
+#define QVDG_MAX_GATE_QUBITS 6
+/* Widest diagonal gate (diagonals are one complex multiply per amplitude). */
+#define QVDG_MAX_DIAGONAL_QUBITS 10
+
+/* A unitary operation on logical qubits: `matrix` on `targets`, applied where
+ * every control qubit holds its value. Reference: fusion::Op,
+ * src/fusion.rs:15-23. */
+typedef struct {
+  uint32_t num_targets;
+  uint32_t num_controls;
+  const uint32_t* targets;        /* matrix index bit j = targets[j] */
+  const uint32_t* controls;       /* control qubits */
+  const uint8_t* control_values;  /* required value (0/1) of each control */
+  const double* matrix;           /* 2^k x 2^k complex128, row-major */
+} qvdg_op;
+
+/* Planner choice for the staged path. */
+enum { QVDG_PLANNER_GREEDY = 0, QVDG_PLANNER_LEARNED = 1 };
+
+/* Simulator options. Reference: simulator::Options, src/simulator.rs:37-66
+ * (defaults max_fused_qubits = 4, region_bits = Some(14)). */
+typedef struct {
+  /* Largest fused gate in qubits (1 disables fusion). */
+  uint32_t max_fused_qubits;
+  /* Staged execution: 0 runs one kernel per fused gate (the reference's
+   * region_bits = None); 1 runs shared-memory staged tiles (the reference's
+   * cache blocking, src/blocking.rs). */
+  uint32_t staged;
+  /* Local qubits per staged tile; 0 picks the default for the precision.
+   * Small values force many stages on small states (as region_bits 1..4 do in
+   * the reference's tests, tests/simulator.rs:256-285). */
+  uint32_t tile_qubits;
+  /* QVDG_PLANNER_GREEDY or QVDG_PLANNER_LEARNED. */
+  uint32_t planner;
+} qvdg_options;
+
+/* What a run did. Reference: simulator::Stats, src/simulator.rs:70-93, plus
+ * the bytes each pass moved. */
+typedef struct {
+  uint64_t gates;       /* ops given */
+  uint64_t kernels;     /* fused ops applied */
+  uint64_t passes;      /* full passes over the state (stages + relabels, or one per fused op) */
+  uint64_t stages;      /* staged passes */
+  double gate_seconds;  /* device time of the gate work (CUDA events) */
+  double bytes;         /* algorithmic HBM bytes of the gate work */
+} qvdg_stats;
+
+typedef struct qvdg_state qvdg_state;
+
+/* Fill `opt` with the reference defaults (max_fused_qubits 4, staged). */
+void qvdg_default_options(qvdg_options* opt);
+
+/* The message of the last failing call on this thread ("" if none). */
+const char* qvdg_last_error(void);
+
+/* Library version string. */
+const char* qvdg_version(void);
+
+/* The state |0...0> of `num_qubits` qubits in single (32) or double (64)
+ * precision, on the current CUDA device.
+ * Reference: StateVector::zero, src/state.rs:39-49. */
+qvdg_status qvdg_state_create(uint32_t num_qubits, uint32_t precision_bits, qvdg_state** out);
+
+/* Free the state and its device memory (reference: Drop of Buffer,
+ * src/memory.rs:91-96). NULL is accepted. */
+qvdg_status qvdg_state_destroy(qvdg_state* state);
+
+/* Set the state to |0...0> and the identity layout. */
+qvdg_status qvdg_state_zero(qvdg_state* state);
+
+/* Number of qubits and precision of a state. */
+qvdg_status qvdg_state_info(const qvdg_state* state, uint32_t* num_qubits, uint32_t* precision_bits);
+
+/* Replace the amplitudes with `amplitudes` (2^n complex128, logical order).
+ * Reference: StateVector::from_amplitudes, src/state.rs:52-63. */
+qvdg_status qvdg_state_set_amplitudes(qvdg_state* state, const double* amplitudes, size_t count);
+
+/* Copy the amplitudes out (2^n complex128, logical order).
+ * Reference: StateVector::to_vec, src/state.rs:146-159. */
+qvdg_status qvdg_state_get_amplitudes(const qvdg_state* state, double* amplitudes, size_t count);
+
+/* Apply ops in order, fusing them first; fills `stats` if not NULL.
+ * Reference: simulator::apply_ops, src/simulator.rs:122-147 (fusion
+ * src/fusion.rs:63-170, blocking src/blocking.rs:230-302). */
+qvdg_status qvdg_apply_ops(qvdg_state* state, const qvdg_op* ops, size_t num_ops,
+                           const qvdg_options* options, qvdg_stats* stats);
+
+/* Apply one unitary `matrix` (index bit j = qubits[j]) where every control
+ * holds. Reference: StateVector::apply, src/state.rs:181-198. */
+qvdg_status qvdg_apply(qvdg_state* state, const double* matrix, const uint32_t* qubits,
+                       uint32_t num_qubits, const uint32_t* controls,
+                       const uint8_t* control_values, uint32_t num_controls);
+
+/* <psi|psi> accumulated in double precision.
+ * Reference: StateVector::norm_sqr, src/state.rs:172-177. */
+qvdg_status qvdg_norm_sqr(const qvdg_state* state, double* out);
+
+/* Multiply every amplitude by `factor`. Reference: StateVector::scale,
+ * src/state.rs:201-207. */
+qvdg_status qvdg_scale(qvdg_state* state, double factor);
+
+/* Probability that `qubit` measures 1, in double precision.
+ * Reference: StateVector::probability_one, src/measure.rs:43-65. */
+qvdg_status qvdg_probability_one(const qvdg_state* state, uint32_t qubit, double* out);
+
+/* <Z_q> = 1 - 2 P(q = 1) for every qubit in one pass (out: num_qubits
+ * values). Built on probability_one, src/measure.rs:43-65. */
+qvdg_status qvdg_expect_z_all(const qvdg_state* state, double* out);
+
+/* Probability of every basis state in logical order (2^n doubles).
+ * Reference: StateVector::probabilities, src/measure.rs:25-40. */
+qvdg_status qvdg_probabilities(const qvdg_state* state, double* out, size_t count);
+
+/* Measure `qubit` with the caller's uniform draw in [0, 1), collapse the
+ * state, and write the outcome (0/1).
+ * Reference: StateVector::measure, src/measure.rs:68-80. */
+qvdg_status qvdg_measure(qvdg_state* state, uint32_t qubit, double uniform, int32_t* outcome);
+
+/* Reset `qubit` to |0>: measure with `uniform`, flip on outcome 1.
+ * Reference: StateVector::reset, src/measure.rs:83-87. */
+qvdg_status qvdg_reset(qvdg_state* state, uint32_t qubit, double uniform);
+
+/* Draw `shots` basis-state indices (logical) from |amplitude|^2 with the
+ * caller's uniforms (`shots` values in [0, 1)), in two passes over the state,
+ * the outcome of each uniform bit-exact with the reference's arithmetic.
+ * `out` has room for `shots` indices; `*count` receives how many were written
+ * (fewer than `shots` only when rounding puts a target at the very total, as
+ * in the reference). Reference: StateVector::sample_unordered,
+ * src/measure.rs:104-174. */
+qvdg_status qvdg_sample_unordered(const qvdg_state* state, size_t shots, const double* uniforms,
+                                  uint64_t* out, size_t* count);
+
+/* Exchange physical bit positions pairwise in one pass and relabel the
+ * logical qubits that lived there. Reference: StateVector::swap_physical,
+ * src/state.rs:212-268 (any bit positions are allowed here). */
+qvdg_status qvdg_swap_physical(qvdg_state* state, const uint32_t* pairs, uint32_t num_pairs);
+
+/* layout[logical] = physical bit position (num_qubits values).
+ * Reference: StateVector::layout, src/state.rs:93-96. */
+qvdg_status qvdg_state_layout(const qvdg_state* state, uint32_t* layout);
+
+/* Device address and byte size of the amplitude buffer (interleaved complex
+ * in the state's precision, physical order), for callers that keep data on
+ * the device. The pointer stays valid until the state is destroyed. */
+qvdg_status qvdg_state_device_buffer(const qvdg_state* state, void** pointer, size_t* bytes);
+
+/* Block the host until the state's stream is idle. */
+qvdg_status qvdg_synchronize(const qvdg_state* state);
+
+/* A circuit planned once (fused and cut into stages) and uploaded to the
+ * current device, for states of `num_qubits` qubits in `precision_bits`
+ * precision with the identity layout. Executing a plan repeats the work of
+ * qvdg_apply_ops without host planning. Reference: the planning half of
+ * apply_ops (src/simulator.rs:122-147, src/fusion.rs:63, src/blocking.rs:230). */
+typedef struct qvdg_plan qvdg_plan;
+
+qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                             const qvdg_options* options, qvdg_plan** out);
+
+/* Free a plan (NULL is accepted). */
+qvdg_status qvdg_plan_destroy(qvdg_plan* plan);
+
+/* Gates, fused kernels, passes, stages and algorithmic bytes of a plan. */
+qvdg_status qvdg_plan_info(const qvdg_plan* plan, qvdg_stats* stats);
+
+/* Apply a plan to a state of its size, precision and layout (the execution
+ * half of apply_ops, src/simulator.rs:122-147). */
+qvdg_status qvdg_plan_execute(qvdg_state* state, const qvdg_plan* plan, qvdg_stats* stats);
+
+/* Record the device time of every pass of later gate runs on this state
+ * (off by default; the reference's timing counters, src/simulator.rs:128-146). */
+qvdg_status qvdg_set_pass_timing(qvdg_state* state, int32_t enabled);
+
+/* Per-pass device seconds, algorithmic bytes and kind (1 staged tile pass,
+ * 0 single-gate pass) of the last gate run; `*count` receives the number of
+ * passes, at most `capacity` entries are written. */
+qvdg_status qvdg_pass_times(const qvdg_state* state, double* seconds, double* bytes, int32_t* staged,
+                            size_t capacity, size_t* count);
+
+/* Make `device` the current CUDA device of the calling thread for this
+ * library (states and plans are created on the current device). */
+qvdg_status qvdg_set_device(int32_t device);
+
+/* max_i |a_i - b_i| over all logical amplitudes of two states of the same
+ * size (any precisions, any layouts), accumulated in double precision on the
+ * device. */
+qvdg_status qvdg_max_abs_diff(const qvdg_state* a, const qvdg_state* b, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QVDG_H */

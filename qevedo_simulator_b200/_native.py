@@ -1,0 +1,290 @@
+"""ctypes binding of libqvdgpu.so (include/qvdg.h).
+
+The library is the product: there is no CPU fallback. Loading fails loudly
+when it has not been built (python -m qevedo_simulator_b200.build) or when
+no CUDA device is present at the first call that needs one.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+from ._abi import PackedOps, QvdgOp, QvdgOptions, QvdgStats, as_double_ptr, as_u64_ptr
+
+LIBRARY = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libqvdgpu.so")
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error", 4: "unsupported", 5: "timeout"}
+
+# Every exported function: name -> (restype, argtypes).
+_P = ct.c_void_p
+_SIGNATURES = {
+    "qvdg_default_options": (None, [ct.POINTER(QvdgOptions)]),
+    "qvdg_last_error": (ct.c_char_p, []),
+    "qvdg_version": (ct.c_char_p, []),
+    "qvdg_state_create": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(_P)]),
+    "qvdg_state_destroy": (ct.c_int, [_P]),
+    "qvdg_state_zero": (ct.c_int, [_P]),
+    "qvdg_state_info": (ct.c_int, [_P, ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint32)]),
+    "qvdg_state_set_amplitudes": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.c_size_t]),
+    "qvdg_state_get_amplitudes": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.c_size_t]),
+    "qvdg_apply_ops": (ct.c_int, [_P, ct.POINTER(QvdgOp), ct.c_size_t, ct.POINTER(QvdgOptions),
+                                  ct.POINTER(QvdgStats)]),
+    "qvdg_apply": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.POINTER(ct.c_uint32), ct.c_uint32,
+                              ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint8), ct.c_uint32]),
+    "qvdg_norm_sqr": (ct.c_int, [_P, ct.POINTER(ct.c_double)]),
+    "qvdg_scale": (ct.c_int, [_P, ct.c_double]),
+    "qvdg_probability_one": (ct.c_int, [_P, ct.c_uint32, ct.POINTER(ct.c_double)]),
+    "qvdg_expect_z_all": (ct.c_int, [_P, ct.POINTER(ct.c_double)]),
+    "qvdg_probabilities": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.c_size_t]),
+    "qvdg_measure": (ct.c_int, [_P, ct.c_uint32, ct.c_double, ct.POINTER(ct.c_int32)]),
+    "qvdg_reset": (ct.c_int, [_P, ct.c_uint32, ct.c_double]),
+    "qvdg_sample_unordered": (ct.c_int, [_P, ct.c_size_t, ct.POINTER(ct.c_double), ct.POINTER(ct.c_uint64),
+                                         ct.POINTER(ct.c_size_t)]),
+    "qvdg_swap_physical": (ct.c_int, [_P, ct.POINTER(ct.c_uint32), ct.c_uint32]),
+    "qvdg_state_layout": (ct.c_int, [_P, ct.POINTER(ct.c_uint32)]),
+    "qvdg_state_device_buffer": (ct.c_int, [_P, ct.POINTER(_P), ct.POINTER(ct.c_size_t)]),
+    "qvdg_synchronize": (ct.c_int, [_P]),
+    "qvdg_plan_create": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(QvdgOp), ct.c_size_t,
+                                    ct.POINTER(QvdgOptions), ct.POINTER(_P)]),
+    "qvdg_plan_destroy": (ct.c_int, [_P]),
+    "qvdg_plan_info": (ct.c_int, [_P, ct.POINTER(QvdgStats)]),
+    "qvdg_plan_execute": (ct.c_int, [_P, _P, ct.POINTER(QvdgStats)]),
+    "qvdg_set_device": (ct.c_int, [ct.c_int32]),
+    "qvdg_max_abs_diff": (ct.c_int, [_P, _P, ct.POINTER(ct.c_double)]),
+    "qvdg_set_pass_timing": (ct.c_int, [_P, ct.c_int32]),
+    "qvdg_pass_times": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), ct.POINTER(ct.c_int32),
+                                   ct.c_size_t, ct.POINTER(ct.c_size_t)]),
+}
+
+_lib = None
+
+
+def lib() -> ct.CDLL:
+    """The loaded library (raises if it is missing: no fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBRARY):
+            raise ImportError(f"{LIBRARY} is missing: build it with `python -m qevedo_simulator_b200.build`")
+        L = ct.CDLL(LIBRARY)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class QvdgError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} ({STATUS.get(status, status)})")
+        self.status = status
+
+
+def check(status: int):
+    if status != 0:
+        msg = lib().qvdg_last_error().decode()
+        if status == 1:
+            raise ValueError(msg)
+        if status == 2:
+            raise MemoryError(msg)
+        raise QvdgError(status, msg)
+
+
+def set_device(device: int):
+    """Select the CUDA device for states and plans created by this thread."""
+    check(lib().qvdg_set_device(int(device)))
+
+
+def options(max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0, planner: int = 0) -> QvdgOptions:
+    o = QvdgOptions()
+    o.max_fused_qubits = int(max_fused_qubits)
+    o.staged = 1 if staged else 0
+    o.tile_qubits = int(tile_qubits)
+    o.planner = int(planner)
+    return o
+
+
+class DeviceState:
+    """A state vector on the current CUDA device (a qvdg_state handle).
+
+    Mirrors the reference's StateVector<T> (src/state.rs, src/measure.rs):
+    logical qubits and indices everywhere, precision 32 (complex64) or 64
+    (complex128)."""
+
+    def __init__(self, num_qubits: int, precision_bits: int = 32):
+        self._h = ct.c_void_p()
+        check(lib().qvdg_state_create(int(num_qubits), int(precision_bits), ct.byref(self._h)))
+        self.num_qubits = int(num_qubits)
+        self.precision_bits = int(precision_bits)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().qvdg_state_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state management
+    def zero(self):
+        check(lib().qvdg_state_zero(self._h))
+
+    def set_amplitudes(self, amplitudes):
+        a = np.ascontiguousarray(amplitudes, dtype=np.complex128)
+        check(lib().qvdg_state_set_amplitudes(self._h, as_double_ptr(a.view(np.float64)), a.size))
+
+    def amplitudes(self) -> np.ndarray:
+        out = np.empty(1 << self.num_qubits, dtype=np.complex128)
+        check(lib().qvdg_state_get_amplitudes(self._h, as_double_ptr(out.view(np.float64)), out.size))
+        return out
+
+    # -- gates
+    def apply_ops(self, ops, opts: QvdgOptions | None = None) -> dict:
+        packed = PackedOps(ops)
+        stats = QvdgStats()
+        check(lib().qvdg_apply_ops(self._h, packed.array, packed.count, ct.byref(opts) if opts else None,
+                                   ct.byref(stats)))
+        return stats.as_dict()
+
+    def apply_packed(self, packed: PackedOps, opts: QvdgOptions | None = None) -> dict:
+        stats = QvdgStats()
+        check(lib().qvdg_apply_ops(self._h, packed.array, packed.count, ct.byref(opts) if opts else None,
+                                   ct.byref(stats)))
+        return stats.as_dict()
+
+    def apply(self, matrix, qubits, controls=()):
+        m = np.ascontiguousarray(matrix, dtype=np.complex128)
+        q = np.array(list(qubits) or [0], dtype=np.uint32)
+        cq = np.array([c for c, _ in controls] or [0], dtype=np.uint32)
+        cv = np.array([1 if v else 0 for _, v in controls] or [0], dtype=np.uint8)
+        check(lib().qvdg_apply(self._h, as_double_ptr(m.view(np.float64)), q.ctypes.data_as(ct.POINTER(ct.c_uint32)),
+                               len(qubits), cq.ctypes.data_as(ct.POINTER(ct.c_uint32)),
+                               cv.ctypes.data_as(ct.POINTER(ct.c_uint8)), len(controls)))
+
+    def scale(self, factor: float):
+        check(lib().qvdg_scale(self._h, float(factor)))
+
+    def swap_physical(self, pairs):
+        flat = np.array([x for p in pairs for x in p] or [0], dtype=np.uint32)
+        check(lib().qvdg_swap_physical(self._h, flat.ctypes.data_as(ct.POINTER(ct.c_uint32)), len(pairs)))
+
+    def layout(self) -> list:
+        out = (ct.c_uint32 * self.num_qubits)()
+        check(lib().qvdg_state_layout(self._h, out))
+        return list(out)
+
+    # -- measurement
+    def norm_sqr(self) -> float:
+        v = ct.c_double()
+        check(lib().qvdg_norm_sqr(self._h, ct.byref(v)))
+        return v.value
+
+    def probability_one(self, qubit: int) -> float:
+        v = ct.c_double()
+        check(lib().qvdg_probability_one(self._h, int(qubit), ct.byref(v)))
+        return v.value
+
+    def expect_z_all(self) -> np.ndarray:
+        out = np.empty(self.num_qubits, dtype=np.float64)
+        check(lib().qvdg_expect_z_all(self._h, as_double_ptr(out)))
+        return out
+
+    def probabilities(self) -> np.ndarray:
+        out = np.empty(1 << self.num_qubits, dtype=np.float64)
+        check(lib().qvdg_probabilities(self._h, as_double_ptr(out), out.size))
+        return out
+
+    def measure(self, qubit: int, uniform: float) -> int:
+        v = ct.c_int32()
+        check(lib().qvdg_measure(self._h, int(qubit), float(uniform), ct.byref(v)))
+        return v.value
+
+    def reset(self, qubit: int, uniform: float):
+        check(lib().qvdg_reset(self._h, int(qubit), float(uniform)))
+
+    def sample_unordered(self, uniforms) -> np.ndarray:
+        u = np.ascontiguousarray(uniforms, dtype=np.float64)
+        out = np.empty(max(u.size, 1), dtype=np.uint64)
+        count = ct.c_size_t()
+        check(lib().qvdg_sample_unordered(self._h, u.size, as_double_ptr(u), as_u64_ptr(out), ct.byref(count)))
+        return out[:count.value]
+
+    def execute(self, plan: "Plan") -> dict:
+        stats = QvdgStats()
+        check(lib().qvdg_plan_execute(self._h, plan._h, ct.byref(stats)))
+        return stats.as_dict()
+
+    def set_pass_timing(self, enabled: bool = True):
+        check(lib().qvdg_set_pass_timing(self._h, 1 if enabled else 0))
+
+    def pass_times(self):
+        """(seconds, bytes, staged) per pass of the last gate run."""
+        count = ct.c_size_t()
+        check(lib().qvdg_pass_times(self._h, None, None, None, 0, ct.byref(count)))
+        n = count.value
+        sec = np.zeros(max(n, 1))
+        byt = np.zeros(max(n, 1))
+        kind = np.zeros(max(n, 1), dtype=np.int32)
+        check(lib().qvdg_pass_times(self._h, as_double_ptr(sec), as_double_ptr(byt),
+                                    kind.ctypes.data_as(ct.POINTER(ct.c_int32)), n, ct.byref(count)))
+        return sec[:n], byt[:n], kind[:n]
+
+    def max_abs_diff(self, other: "DeviceState") -> float:
+        v = ct.c_double()
+        check(lib().qvdg_max_abs_diff(self._h, other._h, ct.byref(v)))
+        return v.value
+
+    def device_buffer(self):
+        p, n = ct.c_void_p(), ct.c_size_t()
+        check(lib().qvdg_state_device_buffer(self._h, ct.byref(p), ct.byref(n)))
+        return p.value, n.value
+
+    def synchronize(self):
+        check(lib().qvdg_synchronize(self._h))
+
+
+class Plan:
+    """A circuit fused, cut into stages and uploaded once (qvdg_plan), for
+    states of `num_qubits` qubits in `precision_bits` precision."""
+
+    def __init__(self, ops, num_qubits: int, precision_bits: int = 32, opts: QvdgOptions | None = None):
+        packed = PackedOps(ops)
+        self._h = ct.c_void_p()
+        check(lib().qvdg_plan_create(int(num_qubits), int(precision_bits), packed.array, packed.count,
+                                     ct.byref(opts) if opts else None, ct.byref(self._h)))
+        self.num_qubits = int(num_qubits)
+        self.precision_bits = int(precision_bits)
+
+    def info(self) -> dict:
+        stats = QvdgStats()
+        check(lib().qvdg_plan_info(self._h, ct.byref(stats)))
+        return stats.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().qvdg_plan_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

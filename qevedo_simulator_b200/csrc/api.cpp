@@ -1,0 +1,557 @@
+// The C ABI (include/qvdg.h): state handles, op lowering and planning on the
+// host, kernel launches on the state's stream, and status codes instead of
+// exceptions at the boundary.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+#include "host.hpp"
+#include "qvdg.h"
+#include "program.hpp"
+#include "stage.hpp"
+
+struct qvdg_state {
+  qvdg::StateImpl s;
+};
+
+// A planned, uploaded circuit for states of one size, precision and layout.
+struct qvdg_plan {
+  qvdg::Program program;
+  qvdg::DeviceUpload dev;
+  void* device = nullptr;  // owned copy of the gate programs and matrices
+  int device_id = 0;
+};
+
+namespace qvdg {
+
+void* DeviceScratch::get(size_t need) {
+  if (need == 0) need = 1;
+  if (need <= bytes) return ptr;
+  release();
+  size_t want = std::max(need, bytes * 2);
+  if (cudaMalloc(&ptr, want) != cudaSuccess) {
+    cudaGetLastError();
+    ptr = nullptr;
+    if (cudaMalloc(&ptr, need) != cudaSuccess) {
+      cudaGetLastError();
+      ptr = nullptr;
+      bytes = 0;
+      throw Error(QVDG_ERR_OUT_OF_MEMORY, "device workspace allocation failed");
+    }
+    want = need;
+  }
+  bytes = want;
+  return ptr;
+}
+
+void DeviceScratch::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+void* HostScratch::get(size_t need) {
+  if (need == 0) need = 1;
+  if (need <= bytes) return ptr;
+  release();
+  if (cudaMallocHost(&ptr, need) != cudaSuccess) {
+    cudaGetLastError();
+    ptr = nullptr;
+    throw Error(QVDG_ERR_OUT_OF_MEMORY, "pinned host allocation failed");
+  }
+  bytes = need;
+  return ptr;
+}
+
+void HostScratch::release() {
+  if (ptr) cudaFreeHost(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+}  // namespace qvdg
+
+namespace {
+
+using namespace qvdg;
+
+thread_local std::string g_error;
+
+template <class F>
+qvdg_status guarded(F&& f) {
+  try {
+    f();
+    g_error.clear();
+    return QVDG_OK;
+  } catch (const Error& e) {
+    g_error = e.what();
+    return qvdg_status(e.status);
+  } catch (const std::bad_alloc&) {
+    g_error = "host allocation failed";
+    return QVDG_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return QVDG_ERR_INVALID;
+  }
+}
+
+void require(bool ok, const std::string& message) {
+  if (!ok) throw Error(QVDG_ERR_INVALID, message);
+}
+
+StateImpl& impl(qvdg_state* st) {
+  require(st != nullptr, "null state");
+  return st->s;
+}
+const StateImpl& impl(const qvdg_state* st) {
+  require(st != nullptr, "null state");
+  return st->s;
+}
+
+// Lower ABI ops to host ops on logical qubits, validating them as the
+// reference does (qubits in range and distinct, src/circuit.rs:467-476 and
+// src/state.rs:182-188).
+std::vector<HOp> lower_ops(const qvdg_op* ops, size_t n, uint32_t num_qubits) {
+  require(n == 0 || ops != nullptr, "null ops");
+  std::vector<HOp> out;
+  out.reserve(n);
+  for (size_t i = 0; i < n; ++i) {
+    const qvdg_op& o = ops[i];
+    require(o.num_targets <= 16 && o.num_controls <= 64, "op " + std::to_string(i) + " is too wide");
+    require(o.num_targets == 0 || (o.targets && o.matrix), "op " + std::to_string(i) + " has no targets or matrix");
+    require(o.num_controls == 0 || o.controls, "op " + std::to_string(i) + " has no control list");
+    HOp h;
+    std::vector<uint32_t> seen;
+    for (uint32_t j = 0; j < o.num_targets; ++j) h.targets.push_back(o.targets[j]);
+    for (uint32_t j = 0; j < o.num_controls; ++j)
+      h.controls.push_back({o.controls[j], o.control_values ? o.control_values[j] != 0 : true});
+    for (uint32_t q : h.qubits()) {
+      require(q < num_qubits, "qubit " + std::to_string(q) + " out of range for " + std::to_string(num_qubits) +
+                                  " qubits");
+      require(std::find(seen.begin(), seen.end(), q) == seen.end(),
+              "op " + std::to_string(i) + " uses qubit " + std::to_string(q) + " twice");
+      seen.push_back(q);
+    }
+    const size_t dim = size_t(1) << o.num_targets;
+    h.matrix = HMatrix(dim);
+    for (size_t e = 0; e < dim * dim; ++e) h.matrix.a[e] = {o.matrix[2 * e], o.matrix[2 * e + 1]};
+    h.diagonal = h.matrix.is_diagonal();
+    if (h.targets.empty()) continue;  // StateVector::apply returns on no qubits (src/state.rs:189-191)
+    out.push_back(std::move(h));
+  }
+  return out;
+}
+
+// Plan, upload and run `ops` on the state (the reference's apply_ops,
+// src/simulator.rs:122-147).
+void apply_program(StateImpl& s, const std::vector<HOp>& ops, const qvdg_options& opt, qvdg_stats* stats) {
+  const Program prog = build_program(target_of(s), ops, opt);
+  const DeviceUpload dev = upload_program(s, prog, s.work);
+  run_program(s, prog, dev, stats);
+}
+
+// One op as a single plain pass (StateVector::apply, src/state.rs:181-198).
+void apply_single(StateImpl& s, const HOp& op) {
+  qvdg_options opt;
+  qvdg_default_options(&opt);
+  opt.staged = 0;
+  opt.max_fused_qubits = 1;
+  apply_program(s, {op}, opt, nullptr);
+}
+
+}  // namespace
+
+extern "C" {
+
+void qvdg_default_options(qvdg_options* opt) {
+  if (!opt) return;
+  opt->max_fused_qubits = 4;
+  opt->staged = 1;
+  opt->tile_qubits = 0;
+  opt->planner = QVDG_PLANNER_GREEDY;
+}
+
+const char* qvdg_last_error(void) { return g_error.c_str(); }
+
+const char* qvdg_version(void) { return "qvdgpu 0.1.0 (sm_100a)"; }
+
+qvdg_status qvdg_state_create(uint32_t num_qubits, uint32_t precision_bits, qvdg_state** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output handle");
+    *out = nullptr;
+    require(precision_bits == 32 || precision_bits == 64, "precision must be 32 or 64 bits");
+    require(num_qubits >= 1 && num_qubits <= 40, "a state needs 1 to 40 qubits");
+    qvdg_state* st = new qvdg_state();
+    StateImpl& s = st->s;
+    try {
+      s.n = num_qubits;
+      s.bits = int(precision_bits);
+      QVDG_CUDA(cudaGetDevice(&s.device));
+      QVDG_CUDA(cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, s.device));
+      s.amp_bytes = size_t(s.elem_bytes()) << num_qubits;
+      if (cudaMalloc(&s.amp, s.amp_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        s.amp = nullptr;
+        throw Error(QVDG_ERR_OUT_OF_MEMORY, "cannot allocate " + std::to_string(s.amp_bytes) +
+                                                " bytes of device memory for " + std::to_string(num_qubits) +
+                                                " qubits");
+      }
+      QVDG_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+      QVDG_CUDA(cudaEventCreate(&s.ev_start));
+      QVDG_CUDA(cudaEventCreate(&s.ev_stop));
+      s.layout.resize(num_qubits);
+      for (uint32_t q = 0; q < num_qubits; ++q) s.layout[q] = q;
+      launch_zero(s);
+      QVDG_CUDA(cudaStreamSynchronize(s.stream));
+    } catch (...) {
+      qvdg_state_destroy(st);
+      throw;
+    }
+    *out = st;
+  });
+}
+
+qvdg_status qvdg_state_destroy(qvdg_state* st) {
+  if (!st) return QVDG_OK;
+  StateImpl& s = st->s;
+  if (s.stream) cudaStreamSynchronize(s.stream);
+  if (s.amp) cudaFree(s.amp);
+  s.work.release();
+  s.work2.release();
+  s.host.release();
+  for (cudaEvent_t e : s.pass_events) cudaEventDestroy(e);
+  if (s.ev_start) cudaEventDestroy(s.ev_start);
+  if (s.ev_stop) cudaEventDestroy(s.ev_stop);
+  if (s.stream) cudaStreamDestroy(s.stream);
+  delete st;
+  return QVDG_OK;
+}
+
+qvdg_status qvdg_state_zero(qvdg_state* st) {
+  return guarded([&] {
+    StateImpl& s = impl(st);
+    for (uint32_t q = 0; q < s.n; ++q) s.layout[q] = q;
+    launch_zero(s);
+    QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+qvdg_status qvdg_state_info(const qvdg_state* st, uint32_t* num_qubits, uint32_t* precision_bits) {
+  return guarded([&] {
+    const StateImpl& s = impl(st);
+    if (num_qubits) *num_qubits = s.n;
+    if (precision_bits) *precision_bits = uint32_t(s.bits);
+  });
+}
+
+qvdg_status qvdg_state_set_amplitudes(qvdg_state* st, const double* amplitudes, size_t count) {
+  return guarded([&] {
+    StateImpl& s = impl(st);
+    require(amplitudes != nullptr, "null amplitudes");
+    require(count == s.size(), "expected " + std::to_string(s.size()) + " amplitudes");
+    for (uint32_t q = 0; q < s.n; ++q) s.layout[q] = q;
+    const uint64_t chunk = uint64_t(1) << 22;
+    for (uint64_t first = 0; first < count; first += chunk) {
+      const uint64_t c = std::min<uint64_t>(chunk, count - first);
+      double* d = static_cast<double*>(s.work.get(c * 16));
+      QVDG_CUDA(cudaMemcpyAsync(d, amplitudes + 2 * first, c * 16, cudaMemcpyHostToDevice, s.stream));
+      launch_import(s, first, c, d);
+      QVDG_CUDA(cudaStreamSynchronize(s.stream));
+    }
+  });
+}
+
+qvdg_status qvdg_state_get_amplitudes(const qvdg_state* cst, double* amplitudes, size_t count) {
+  return guarded([&] {
+    StateImpl& s = const_cast<StateImpl&>(impl(cst));
+    require(amplitudes != nullptr, "null output");
+    require(count == s.size(), "expected room for " + std::to_string(s.size()) + " amplitudes");
+    const uint64_t chunk = uint64_t(1) << 22;
+    for (uint64_t first = 0; first < count; first += chunk) {
+      const uint64_t c = std::min<uint64_t>(chunk, count - first);
+      double* d = static_cast<double*>(s.work.get(c * 16));
+      launch_export(s, first, c, d);
+      QVDG_CUDA(cudaMemcpyAsync(amplitudes + 2 * first, d, c * 16, cudaMemcpyDeviceToHost, s.stream));
+      QVDG_CUDA(cudaStreamSynchronize(s.stream));
+    }
+  });
+}
+
+qvdg_status qvdg_apply_ops(qvdg_state* st, const qvdg_op* ops, size_t num_ops, const qvdg_options* options,
+                           qvdg_stats* stats) {
+  return guarded([&] {
+    StateImpl& s = impl(st);
+    qvdg_options opt;
+    qvdg_default_options(&opt);
+    if (options) opt = *options;
+    std::vector<HOp> host_ops = lower_ops(ops, num_ops, s.n);
+    if (stats) stats->gates += num_ops;
+    apply_program(s, host_ops, opt, stats);
+  });
+}
+
+qvdg_status qvdg_apply(qvdg_state* st, const double* matrix, const uint32_t* qubits, uint32_t num_qubits,
+                       const uint32_t* controls, const uint8_t* control_values, uint32_t num_controls) {
+  return guarded([&] {
+    StateImpl& s = impl(st);
+    qvdg_op op{num_qubits, num_controls, qubits, controls, control_values, matrix};
+    std::vector<HOp> host_ops = lower_ops(&op, 1, s.n);
+    if (!host_ops.empty()) apply_single(s, host_ops[0]);
+  });
+}
+
+qvdg_status qvdg_norm_sqr(const qvdg_state* st, double* out) {
+  return guarded([&] {
+    require(out != nullptr, "null output");
+    *out = norm_sqr(const_cast<StateImpl&>(impl(st)));
+  });
+}
+
+qvdg_status qvdg_scale(qvdg_state* st, double factor) {
+  return guarded([&] {
+    StateImpl& s = impl(st);
+    launch_scale(s, factor);
+    QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+qvdg_status qvdg_probability_one(const qvdg_state* st, uint32_t qubit, double* out) {
+  return guarded([&] {
+    StateImpl& s = const_cast<StateImpl&>(impl(st));
+    require(out != nullptr, "null output");
+    require(qubit < s.n, "qubit out of range");
+    *out = probability_one(s, s.layout[qubit]);
+  });
+}
+
+qvdg_status qvdg_expect_z_all(const qvdg_state* st, double* out) {
+  return guarded([&] {
+    StateImpl& s = const_cast<StateImpl&>(impl(st));
+    require(out != nullptr, "null output");
+    std::vector<double> p1;
+    double total = 0.0;
+    bit_probabilities(s, p1, total);
+    for (uint32_t q = 0; q < s.n; ++q) out[q] = total - 2.0 * p1[s.layout[q]];
+  });
+}
+
+qvdg_status qvdg_probabilities(const qvdg_state* st, double* out, size_t count) {
+  return guarded([&] {
+    StateImpl& s = const_cast<StateImpl&>(impl(st));
+    require(out != nullptr, "null output");
+    require(count == s.size(), "expected room for " + std::to_string(s.size()) + " probabilities");
+    probabilities(s, out);
+  });
+}
+
+qvdg_status qvdg_measure(qvdg_state* st, uint32_t qubit, double uniform, int32_t* outcome) {
+  return guarded([&] {
+    StateImpl& s = impl(st);
+    require(qubit < s.n, "qubit out of range");
+    // src/measure.rs:68-80
+    const double p1 = std::min(std::max(probability_one(s, s.layout[qubit]), 0.0), 1.0);
+    const bool one = uniform < p1;
+    const double p = one ? p1 : 1.0 - p1;
+    const C keep{1.0 / std::sqrt(p), 0.0}, zero{0.0, 0.0};
+    HOp op;
+    op.targets = {qubit};
+    op.matrix = HMatrix::diagonal(one ? std::vector<C>{zero, keep} : std::vector<C>{keep, zero});
+    op.diagonal = true;
+    apply_single(s, op);
+    if (outcome) *outcome = one ? 1 : 0;
+  });
+}
+
+qvdg_status qvdg_reset(qvdg_state* st, uint32_t qubit, double uniform) {
+  int32_t outcome = 0;
+  qvdg_status rc = qvdg_measure(st, qubit, uniform, &outcome);
+  if (rc != QVDG_OK || !outcome) return rc;
+  return guarded([&] {
+    StateImpl& s = impl(st);
+    HOp x;
+    x.targets = {qubit};
+    x.matrix = HMatrix(2);
+    x.matrix.at(0, 1) = {1.0, 0.0};
+    x.matrix.at(1, 0) = {1.0, 0.0};
+    apply_single(s, x);
+  });
+}
+
+qvdg_status qvdg_sample_unordered(const qvdg_state* st, size_t shots, const double* uniforms, uint64_t* out,
+                                  size_t* count) {
+  return guarded([&] {
+    StateImpl& s = const_cast<StateImpl&>(impl(st));
+    require(shots == 0 || (uniforms && out), "null uniforms or output");
+    const size_t found = sample_unordered(s, shots, uniforms, out);
+    if (count) *count = found;
+  });
+}
+
+qvdg_status qvdg_swap_physical(qvdg_state* st, const uint32_t* pairs, uint32_t num_pairs) {
+  return guarded([&] {
+    StateImpl& s = impl(st);
+    require(num_pairs == 0 || pairs, "null pairs");
+    require(num_pairs <= 32, "too many pairs");
+    std::vector<std::pair<uint32_t, uint32_t>> p;
+    uint64_t seen = 0;
+    for (uint32_t i = 0; i < num_pairs; ++i) {
+      const uint32_t a = pairs[2 * i], b = pairs[2 * i + 1];
+      require(a < s.n && b < s.n && a != b, "invalid bit pair");
+      const uint64_t m = (uint64_t(1) << a) | (uint64_t(1) << b);
+      require((seen & m) == 0, "bit swapped twice in one pass");
+      seen |= m;
+      p.push_back({a, b});
+    }
+    launch_swap_bits(s, p);
+    QVDG_CUDA(cudaStreamSynchronize(s.stream));
+    for (auto& q : s.layout)
+      for (auto& pr : p) {
+        if (q == pr.first)
+          q = pr.second;
+        else if (q == pr.second)
+          q = pr.first;
+      }
+  });
+}
+
+qvdg_status qvdg_state_layout(const qvdg_state* st, uint32_t* layout) {
+  return guarded([&] {
+    const StateImpl& s = impl(st);
+    require(layout != nullptr, "null output");
+    for (uint32_t q = 0; q < s.n; ++q) layout[q] = s.layout[q];
+  });
+}
+
+qvdg_status qvdg_state_device_buffer(const qvdg_state* st, void** pointer, size_t* bytes) {
+  return guarded([&] {
+    const StateImpl& s = impl(st);
+    if (pointer) *pointer = s.amp;
+    if (bytes) *bytes = s.amp_bytes;
+  });
+}
+
+qvdg_status qvdg_synchronize(const qvdg_state* st) {
+  return guarded([&] { QVDG_CUDA(cudaStreamSynchronize(impl(st).stream)); });
+}
+
+qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                             const qvdg_options* options, qvdg_plan** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output handle");
+    *out = nullptr;
+    require(precision_bits == 32 || precision_bits == 64, "precision must be 32 or 64 bits");
+    require(num_qubits >= 1 && num_qubits <= 40, "a state needs 1 to 40 qubits");
+    qvdg_options opt;
+    qvdg_default_options(&opt);
+    if (options) opt = *options;
+    Target t;
+    t.n = num_qubits;
+    t.bits = int(precision_bits);
+    QVDG_CUDA(cudaGetDevice(&t.sms));
+    int dev = t.sms;
+    QVDG_CUDA(cudaDeviceGetAttribute(&t.sms, cudaDevAttrMultiProcessorCount, dev));
+    for (uint32_t q = 0; q < num_qubits; ++q) t.layout.push_back(q);
+    qvdg_plan* plan = new qvdg_plan();
+    plan->device_id = dev;
+    try {
+      plan->program = build_program(t, lower_ops(ops, num_ops, num_qubits), opt);
+      plan->program.gates = num_ops;
+      // Gate programs and matrices in the plan's precision, one device copy.
+      const StageUpload& up = plan->program.upload;
+      auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+      const size_t gate_bytes = up.gates.size() * sizeof(TileGate);
+      const size_t mat_bytes = up.mats.size() * (precision_bits == 32 ? 4 : 8);
+      std::vector<char> h(align(gate_bytes) + align(mat_bytes) + 256, 0);
+      if (gate_bytes) std::memcpy(h.data(), up.gates.data(), gate_bytes);
+      if (precision_bits == 32) {
+        float* f = reinterpret_cast<float*>(h.data() + align(gate_bytes));
+        for (size_t i = 0; i < up.mats.size(); ++i) f[i] = float(up.mats[i]);
+      } else if (mat_bytes) {
+        std::memcpy(h.data() + align(gate_bytes), up.mats.data(), mat_bytes);
+      }
+      if (cudaMalloc(&plan->device, h.size()) != cudaSuccess) {
+        cudaGetLastError();
+        plan->device = nullptr;
+        throw Error(QVDG_ERR_OUT_OF_MEMORY, "cannot allocate the plan's device memory");
+      }
+      QVDG_CUDA(cudaMemcpy(plan->device, h.data(), h.size(), cudaMemcpyHostToDevice));
+      plan->dev.gates = static_cast<const TileGate*>(plan->device);
+      plan->dev.mats = static_cast<const char*>(plan->device) + align(gate_bytes);
+    } catch (...) {
+      qvdg_plan_destroy(plan);
+      throw;
+    }
+    *out = plan;
+  });
+}
+
+qvdg_status qvdg_plan_destroy(qvdg_plan* plan) {
+  if (!plan) return QVDG_OK;
+  if (plan->device) cudaFree(plan->device);
+  delete plan;
+  return QVDG_OK;
+}
+
+qvdg_status qvdg_plan_info(const qvdg_plan* plan, qvdg_stats* stats) {
+  return guarded([&] {
+    require(plan != nullptr && stats != nullptr, "null plan or output");
+    const Program& p = plan->program;
+    stats->gates = p.gates;
+    stats->kernels = p.kernels;
+    stats->passes = p.passes.size();
+    stats->stages = p.stages;
+    stats->gate_seconds = 0.0;
+    stats->bytes = p.bytes;
+  });
+}
+
+qvdg_status qvdg_plan_execute(qvdg_state* st, const qvdg_plan* plan, qvdg_stats* stats) {
+  return guarded([&] {
+    StateImpl& s = impl(st);
+    require(plan != nullptr, "null plan");
+    const Target& t = plan->program.target;
+    require(t.n == s.n && t.bits == s.bits, "the plan was made for another state size or precision");
+    require(t.layout == s.layout, "the plan was made for another qubit layout");
+    require(plan->device_id == s.device, "the plan lives on another device");
+    if (stats) stats->gates += plan->program.gates;
+    run_program(s, plan->program, plan->dev, stats);
+  });
+}
+
+qvdg_status qvdg_set_pass_timing(qvdg_state* st, int32_t enabled) {
+  return guarded([&] { impl(st).record_passes = enabled != 0; });
+}
+
+qvdg_status qvdg_pass_times(const qvdg_state* st, double* seconds, double* bytes, int32_t* staged, size_t capacity,
+                            size_t* count) {
+  return guarded([&] {
+    const StateImpl& s = impl(st);
+    const size_t n = s.pass_seconds.size();
+    if (count) *count = n;
+    for (size_t i = 0; i < n && i < capacity; ++i) {
+      if (seconds) seconds[i] = s.pass_seconds[i];
+      if (bytes) bytes[i] = s.pass_bytes[i];
+      if (staged) staged[i] = s.pass_kinds[i];
+    }
+  });
+}
+
+qvdg_status qvdg_set_device(int32_t device) {
+  return guarded([&] { QVDG_CUDA(cudaSetDevice(device)); });
+}
+
+qvdg_status qvdg_max_abs_diff(const qvdg_state* a, const qvdg_state* b, double* out) {
+  return guarded([&] {
+    require(out != nullptr, "null output");
+    *out = max_abs_diff(const_cast<StateImpl&>(impl(a)), const_cast<StateImpl&>(impl(b)));
+  });
+}
+
+}  // extern "C"

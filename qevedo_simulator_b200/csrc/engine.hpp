@@ -1,0 +1,97 @@
+// Internal interface between the C ABI (api.cpp) and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace qvdg {
+
+// A device buffer that grows on demand (never shrinks while its owner lives).
+struct DeviceScratch {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void* get(size_t need);  // may reallocate (contents are lost)
+  void release();
+};
+
+// A pinned host buffer that grows on demand.
+struct HostScratch {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void* get(size_t need);
+  void release();
+};
+
+// One fused gate ready for a plain (one pass) launch, on physical bits.
+struct PlainGate {
+  bool diagonal = false;
+  std::vector<uint32_t> targets;                      // physical, matrix bit j = targets[j]
+  std::vector<std::pair<uint32_t, bool>> controls;    // physical
+  size_t matrix_offset = 0;  // element offset (complex) of its matrix / diagonal in the upload
+};
+
+struct StateImpl {
+  uint32_t n = 0;
+  int bits = 32;
+  void* amp = nullptr;  // 2^n interleaved complex in `bits` precision
+  size_t amp_bytes = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  std::vector<uint32_t> layout;  // logical -> physical
+  DeviceScratch work;            // device workspace (uploads, reductions, sampling)
+  DeviceScratch work2;
+  HostScratch host;              // pinned staging
+  int device = 0;
+  int sms = 148;
+  // Per-pass device timings of the last gate run (when enabled).
+  bool record_passes = false;
+  std::vector<cudaEvent_t> pass_events;
+  std::vector<double> pass_seconds, pass_bytes;
+  std::vector<int> pass_kinds;  // 1 staged tile pass, 0 plain gate pass
+
+  size_t elem_bytes() const { return bits == 32 ? 8 : 16; }
+  uint64_t size() const { return uint64_t(1) << n; }
+  bool identity_layout() const {
+    for (size_t q = 0; q < layout.size(); ++q)
+      if (layout[q] != q) return false;
+    return true;
+  }
+};
+
+// ---- gates.cu
+// Launch one plain gate pass; `matrices` is the device copy of the upload
+// (complex in the state's precision).
+void launch_plain_gate(StateImpl& s, const PlainGate& g, const void* matrices);
+// Exchange physical bit pairs in one pass.
+void launch_swap_bits(StateImpl& s, const std::vector<std::pair<uint32_t, uint32_t>>& pairs);
+// |0...0>.
+void launch_zero(StateImpl& s);
+// Convert `count` logical amplitudes starting at `first` to complex128 (out)
+// or from complex128 (in), through the layout.
+void launch_export(StateImpl& s, uint64_t first, uint64_t count, double* out_dev);
+void launch_import(StateImpl& s, uint64_t first, uint64_t count, const double* in_dev);
+void launch_scale(StateImpl& s, double factor);
+
+// ---- measure.cu
+double norm_sqr(StateImpl& s);
+double probability_one(StateImpl& s, uint32_t physical_bit);
+// P(bit = 1) for every physical bit, and the total.
+void bit_probabilities(StateImpl& s, std::vector<double>& p1, double& total);
+void probabilities(StateImpl& s, double* out_host);
+// Bit-exact restatement of the reference sampler; outcomes are physical
+// indices in chunk order, then mapped to logical with the layout.
+size_t sample_unordered(StateImpl& s, size_t shots, const double* uniforms_host, uint64_t* out_host);
+
+// max over logical indices of |a - b| (both states the same size).
+double max_abs_diff(StateImpl& a, StateImpl& b);
+
+// ---- sort.cu
+// Ascending stable LSD radix sort of `count` 64-bit keys in place (`tmp` has
+// room for `count` keys). `work` provides temporary device memory.
+void radix_sort_u64(uint64_t* keys, uint64_t* tmp, size_t count, DeviceScratch& work, cudaStream_t stream);
+
+}  // namespace qvdg

@@ -1,0 +1,375 @@
+// Plain-path gate kernels: one pass over the state per fused gate.
+//
+// These replace the reference's AVX2 sweeps (src/kernels.rs:252-473). The
+// state is interleaved complex in physical index order; a gate on physical
+// target bits t_0..t_{k-1} with controls acts on groups of 2^k amplitudes
+// whose index differs only in the target bits and whose control bits hold.
+// Group bases are enumerated by inserting zero bits at the (sorted) target
+// and control positions of a running counter, so a controlled gate touches
+// only the 2^-c of the state its controls select (the reference's
+// `free_mask`/`control_value`, src/kernels.rs:78-135). Consecutive threads
+// take consecutive bases: when bit 0 is free, a warp's loads of each group
+// member are one contiguous 256-byte (complex64) or 512-byte (complex128)
+// run, and complex64 threads take two neighbouring groups with one 16-byte
+// load per member.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "engine.hpp"
+
+namespace qvdg {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct DenseGeom {
+  uint64_t n_iter;         // number of groups
+  uint64_t control_value;  // control bits that must be 1
+  uint64_t offsets[64];    // index offset of each group member (matrix index order)
+  uint8_t fixed[40];       // sorted target and control positions
+  int32_t num_fixed;
+};
+
+template <typename T, int K, int G, bool VEC>
+__global__ void __launch_bounds__(kThreads) k_dense(cplx_t<T>* __restrict__ psi, const DenseGeom g,
+                                                    const cplx_t<T>* __restrict__ mat) {
+  constexpr int D = 1 << K;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx_t<T>* sm = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  __shared__ uint8_t fixed[40];
+  for (int i = threadIdx.x; i < D * D; i += blockDim.x) sm[i] = mat[i];
+  if (threadIdx.x < 40) fixed[threadIdx.x] = g.fixed[threadIdx.x];
+  __syncthreads();
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x * G;
+  for (uint64_t it = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) * G; it < g.n_iter; it += stride) {
+    uint64_t base[G];
+#pragma unroll
+    for (int q = 0; q < G; ++q) base[q] = insert_zeros(it + q, fixed, g.num_fixed) | g.control_value;
+    cplx_t<T> x[G][D];
+    if constexpr (VEC) {
+      // complex64 with bit 0 free: groups it and it+1 are neighbours.
+#pragma unroll
+      for (int h = 0; h < D; ++h) {
+        const float4 v = *reinterpret_cast<const float4*>(psi + base[0] + g.offsets[h]);
+        x[0][h] = make_c<T>(v.x, v.y);
+        x[G - 1][h] = make_c<T>(v.z, v.w);
+      }
+    } else {
+#pragma unroll
+      for (int h = 0; h < D; ++h)
+#pragma unroll
+        for (int q = 0; q < G; ++q) x[q][h] = psi[base[q] + g.offsets[h]];
+    }
+#pragma unroll 1
+    for (int r = 0; r < D; ++r) {
+      cplx_t<T> acc[G];
+#pragma unroll
+      for (int q = 0; q < G; ++q) acc[q] = make_c<T>(T(0), T(0));
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        const cplx_t<T> m = sm[r * D + c];
+#pragma unroll
+        for (int q = 0; q < G; ++q) cmac<T>(acc[q], m, x[q][c]);
+      }
+      if constexpr (VEC) {
+        *reinterpret_cast<float4*>(psi + base[0] + g.offsets[r]) =
+            make_float4(acc[0].x, acc[0].y, acc[G - 1].x, acc[G - 1].y);
+      } else {
+#pragma unroll
+        for (int q = 0; q < G; ++q) psi[base[q] + g.offsets[r]] = acc[q];
+      }
+    }
+  }
+}
+
+struct DiagGeom {
+  uint64_t n_iter;         // amplitudes in the controlled subspace
+  uint64_t control_value;
+  uint8_t ctrl[40];        // sorted control positions
+  int32_t num_ctrl;
+  uint8_t targets[16];     // diagonal index bit j = targets[j]
+  int32_t k;
+};
+
+template <typename T, int G>
+__global__ void __launch_bounds__(kThreads) k_diag(cplx_t<T>* __restrict__ psi, const DiagGeom g,
+                                                   const cplx_t<T>* __restrict__ diag) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx_t<T>* sm = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  __shared__ uint8_t ctrl[40], tgt[16];
+  for (int i = threadIdx.x; i < (1 << g.k); i += blockDim.x) sm[i] = diag[i];
+  if (threadIdx.x < 40) ctrl[threadIdx.x] = g.ctrl[threadIdx.x];
+  if (threadIdx.x < 16) tgt[threadIdx.x] = g.targets[threadIdx.x];
+  __syncthreads();
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x * G;
+  for (uint64_t it = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) * G; it < g.n_iter; it += stride) {
+    // With G == 2, bit 0 is not a control: indices i and i+1 are neighbours.
+    const uint64_t i = insert_zeros(it, ctrl, g.num_ctrl) | g.control_value;
+    uint32_t d[G];
+#pragma unroll
+    for (int q = 0; q < G; ++q) {
+      d[q] = 0;
+      for (int j = 0; j < g.k; ++j) d[q] |= uint32_t(((i + q) >> tgt[j]) & 1) << j;
+    }
+    if constexpr (G == 2 && sizeof(T) == 4) {
+      float4 v = *reinterpret_cast<float4*>(psi + i);
+      const cplx_t<T> a = cmul<T>(sm[d[0]], make_c<T>(v.x, v.y));
+      const cplx_t<T> b = cmul<T>(sm[d[1]], make_c<T>(v.z, v.w));
+      *reinterpret_cast<float4*>(psi + i) = make_float4(a.x, a.y, b.x, b.y);
+    } else {
+#pragma unroll
+      for (int q = 0; q < G; ++q) psi[i + q] = cmul<T>(sm[d[q]], psi[i + q]);
+    }
+  }
+}
+
+struct SwapGeom {
+  uint64_t mask;  // every swapped bit
+  int32_t np;
+  uint8_t a[32], b[32];
+};
+
+template <typename T>
+__global__ void k_swap_bits(cplx_t<T>* __restrict__ psi, uint64_t len, const SwapGeom g) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < len; i += stride) {
+    uint64_t j = i & ~g.mask;
+    for (int p = 0; p < g.np; ++p)
+      j |= (((i >> g.a[p]) & 1) << g.b[p]) | (((i >> g.b[p]) & 1) << g.a[p]);
+    if (i < j) {
+      const cplx_t<T> t = psi[i];
+      psi[i] = psi[j];
+      psi[j] = t;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_set_one(cplx_t<T>* psi) {
+  psi[0] = make_c<T>(T(1), T(0));
+}
+
+// Logical index -> physical index through per-byte lookup tables.
+__device__ __forceinline__ uint64_t to_physical(uint64_t i, const uint64_t* tables, int ntables) {
+  if (ntables == 0) return i;
+  uint64_t p = 0;
+  for (int b = 0; b < ntables; ++b) p |= tables[b * 256 + ((i >> (8 * b)) & 255)];
+  return p;
+}
+
+template <typename T>
+__global__ void k_export(const cplx_t<T>* __restrict__ psi, double2* __restrict__ out, uint64_t first,
+                         uint64_t count, const uint64_t* __restrict__ tables, int ntables) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < count; t += stride) {
+    const cplx_t<T> a = psi[to_physical(first + t, tables, ntables)];
+    out[t] = make_double2(double(a.x), double(a.y));
+  }
+}
+
+template <typename T>
+__global__ void k_import(cplx_t<T>* __restrict__ psi, const double2* __restrict__ in, uint64_t first,
+                         uint64_t count, const uint64_t* __restrict__ tables, int ntables) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < count; t += stride) {
+    const double2 a = in[t];
+    psi[to_physical(first + t, tables, ntables)] = make_c<T>(T(a.x), T(a.y));
+  }
+}
+
+template <typename T>
+__global__ void k_scale(cplx_t<T>* __restrict__ psi, uint64_t len, double factor) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < len; i += stride) {
+    cplx_t<T> a = psi[i];
+    a.x = T(double(a.x) * factor);
+    a.y = T(double(a.y) * factor);
+    psi[i] = a;
+  }
+}
+
+unsigned grid_for(const StateImpl& s, uint64_t work_items) {
+  const uint64_t blocks = (work_items + kThreads - 1) / kThreads;
+  return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(blocks, uint64_t(s.sms) * 16)));
+}
+
+template <typename T, int K, int G, bool VEC>
+void dense_launch(StateImpl& s, const DenseGeom& g, const void* mat) {
+  const size_t smem = size_t(1) << (2 * K);
+  const size_t bytes = smem * sizeof(cplx_t<T>);
+  static bool configured = false;  // per instantiation
+  if (!configured) {
+    QVDG_CUDA(cudaFuncSetAttribute(k_dense<T, K, G, VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    configured = true;
+  }
+  k_dense<T, K, G, VEC><<<grid_for(s, g.n_iter / G), kThreads, bytes, s.stream>>>(
+      static_cast<cplx_t<T>*>(s.amp), g, static_cast<const cplx_t<T>*>(mat));
+  QVDG_LAUNCH_CHECK();
+}
+
+template <typename T, int K>
+void dense_pick(StateImpl& s, const DenseGeom& g, const void* mat, bool bit0_free) {
+  if constexpr (K <= 4) {
+    if (g.n_iter >= 2) {
+      if (sizeof(T) == 4 && bit0_free)
+        return dense_launch<T, K, 2, true>(s, g, mat);
+      return dense_launch<T, K, 2, false>(s, g, mat);
+    }
+  }
+  dense_launch<T, K, 1, false>(s, g, mat);
+}
+
+template <typename T>
+void plain_gate(StateImpl& s, const PlainGate& pg, const void* matrices) {
+  const int k = int(pg.targets.size());
+  const int c = int(pg.controls.size());
+  uint64_t control_value = 0;
+  std::vector<uint8_t> ctrl;
+  for (auto& cv : pg.controls) {
+    ctrl.push_back(uint8_t(cv.first));
+    if (cv.second) control_value |= uint64_t(1) << cv.first;
+  }
+  std::sort(ctrl.begin(), ctrl.end());
+  const cplx_t<T>* mat = static_cast<const cplx_t<T>*>(matrices) + pg.matrix_offset;
+  if (pg.diagonal) {
+    DiagGeom g{};
+    g.n_iter = uint64_t(1) << (s.n - c);
+    g.control_value = control_value;
+    g.num_ctrl = c;
+    for (int i = 0; i < c; ++i) g.ctrl[i] = ctrl[i];
+    g.k = k;
+    for (int j = 0; j < k; ++j) g.targets[j] = uint8_t(pg.targets[j]);
+    const bool bit0_ctrl = c > 0 && ctrl[0] == 0;
+    const size_t bytes = (size_t(1) << k) * sizeof(cplx_t<T>);
+    if (g.n_iter >= 2 && !bit0_ctrl)
+      k_diag<T, 2><<<grid_for(s, g.n_iter / 2), kThreads, bytes, s.stream>>>(static_cast<cplx_t<T>*>(s.amp), g, mat);
+    else
+      k_diag<T, 1><<<grid_for(s, g.n_iter), kThreads, bytes, s.stream>>>(static_cast<cplx_t<T>*>(s.amp), g, mat);
+    QVDG_LAUNCH_CHECK();
+    return;
+  }
+  DenseGeom g{};
+  g.n_iter = uint64_t(1) << (s.n - k - c);
+  g.control_value = control_value;
+  std::vector<uint8_t> fixed(ctrl);
+  for (uint32_t t : pg.targets) fixed.push_back(uint8_t(t));
+  std::sort(fixed.begin(), fixed.end());
+  g.num_fixed = int(fixed.size());
+  for (size_t i = 0; i < fixed.size(); ++i) g.fixed[i] = fixed[i];
+  for (int h = 0; h < (1 << k); ++h) {
+    uint64_t o = 0;
+    for (int j = 0; j < k; ++j) o |= uint64_t((h >> j) & 1) << pg.targets[j];
+    g.offsets[h] = o;
+  }
+  const bool bit0_free = fixed.empty() || fixed[0] != 0;
+  switch (k) {
+    case 1: return dense_pick<T, 1>(s, g, mat, bit0_free);
+    case 2: return dense_pick<T, 2>(s, g, mat, bit0_free);
+    case 3: return dense_pick<T, 3>(s, g, mat, bit0_free);
+    case 4: return dense_pick<T, 4>(s, g, mat, bit0_free);
+    case 5: return dense_pick<T, 5>(s, g, mat, bit0_free);
+    case 6: return dense_pick<T, 6>(s, g, mat, bit0_free);
+    default: throw Error(4, "dense gates on more than 6 qubits are not supported");
+  }
+}
+
+// Byte-wise logical->physical tables for a non-identity layout (uploaded to
+// the workspace); returns the number of tables (0 for the identity).
+int layout_tables(StateImpl& s, uint64_t** dev_tables) {
+  if (s.identity_layout()) {
+    *dev_tables = nullptr;
+    return 0;
+  }
+  const int ntables = int((s.n + 7) / 8);
+  std::vector<uint64_t> t(size_t(ntables) * 256, 0);
+  for (int b = 0; b < ntables; ++b)
+    for (int v = 0; v < 256; ++v) {
+      uint64_t p = 0;
+      for (int bit = 0; bit < 8; ++bit) {
+        const uint32_t q = uint32_t(8 * b + bit);
+        if (q < s.n && ((v >> bit) & 1)) p |= uint64_t(1) << s.layout[q];
+      }
+      t[size_t(b) * 256 + v] = p;
+    }
+  uint64_t* d = static_cast<uint64_t*>(s.work2.get(t.size() * sizeof(uint64_t)));
+  QVDG_CUDA(cudaMemcpyAsync(d, t.data(), t.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, s.stream));
+  QVDG_CUDA(cudaStreamSynchronize(s.stream));  // `t` is pageable and goes out of scope
+  *dev_tables = d;
+  return ntables;
+}
+
+}  // namespace
+
+void launch_plain_gate(StateImpl& s, const PlainGate& g, const void* matrices) {
+  if (s.bits == 32)
+    plain_gate<float>(s, g, matrices);
+  else
+    plain_gate<double>(s, g, matrices);
+}
+
+void launch_swap_bits(StateImpl& s, const std::vector<std::pair<uint32_t, uint32_t>>& pairs) {
+  if (pairs.empty()) return;
+  SwapGeom g{};
+  g.np = int(pairs.size());
+  for (size_t p = 0; p < pairs.size(); ++p) {
+    g.a[p] = uint8_t(pairs[p].first);
+    g.b[p] = uint8_t(pairs[p].second);
+    g.mask |= (uint64_t(1) << pairs[p].first) | (uint64_t(1) << pairs[p].second);
+  }
+  if (s.bits == 32)
+    k_swap_bits<float><<<grid_for(s, s.size()), kThreads, 0, s.stream>>>(static_cast<float2*>(s.amp), s.size(), g);
+  else
+    k_swap_bits<double><<<grid_for(s, s.size()), kThreads, 0, s.stream>>>(static_cast<double2*>(s.amp), s.size(), g);
+  QVDG_LAUNCH_CHECK();
+}
+
+void launch_zero(StateImpl& s) {
+  QVDG_CUDA(cudaMemsetAsync(s.amp, 0, s.amp_bytes, s.stream));
+  if (s.bits == 32)
+    k_set_one<float><<<1, 1, 0, s.stream>>>(static_cast<float2*>(s.amp));
+  else
+    k_set_one<double><<<1, 1, 0, s.stream>>>(static_cast<double2*>(s.amp));
+  QVDG_LAUNCH_CHECK();
+}
+
+void launch_export(StateImpl& s, uint64_t first, uint64_t count, double* out_dev) {
+  uint64_t* tables;
+  const int nt = layout_tables(s, &tables);
+  if (s.bits == 32)
+    k_export<float><<<grid_for(s, count), kThreads, 0, s.stream>>>(static_cast<const float2*>(s.amp),
+                                                                    reinterpret_cast<double2*>(out_dev), first,
+                                                                    count, tables, nt);
+  else
+    k_export<double><<<grid_for(s, count), kThreads, 0, s.stream>>>(static_cast<const double2*>(s.amp),
+                                                                     reinterpret_cast<double2*>(out_dev), first,
+                                                                     count, tables, nt);
+  QVDG_LAUNCH_CHECK();
+}
+
+void launch_import(StateImpl& s, uint64_t first, uint64_t count, const double* in_dev) {
+  uint64_t* tables;
+  const int nt = layout_tables(s, &tables);
+  if (s.bits == 32)
+    k_import<float><<<grid_for(s, count), kThreads, 0, s.stream>>>(static_cast<float2*>(s.amp),
+                                                                    reinterpret_cast<const double2*>(in_dev), first,
+                                                                    count, tables, nt);
+  else
+    k_import<double><<<grid_for(s, count), kThreads, 0, s.stream>>>(static_cast<double2*>(s.amp),
+                                                                     reinterpret_cast<const double2*>(in_dev),
+                                                                     first, count, tables, nt);
+  QVDG_LAUNCH_CHECK();
+}
+
+void launch_scale(StateImpl& s, double factor) {
+  if (s.bits == 32)
+    k_scale<float><<<grid_for(s, s.size()), kThreads, 0, s.stream>>>(static_cast<float2*>(s.amp), s.size(), factor);
+  else
+    k_scale<double><<<grid_for(s, s.size()), kThreads, 0, s.stream>>>(static_cast<double2*>(s.amp), s.size(),
+                                                                       factor);
+  QVDG_LAUNCH_CHECK();
+}
+
+}  // namespace qvdg

@@ -1,0 +1,185 @@
+// Host gate algebra and greedy fusion (see host.hpp for the reference map).
+#include "host.hpp"
+
+#include <stdexcept>
+
+namespace qvdg {
+
+HMatrix HMatrix::identity(size_t qubits) {
+  HMatrix m(size_t(1) << qubits);
+  for (size_t i = 0; i < m.dim; ++i) m.at(i, i) = {1.0, 0.0};
+  return m;
+}
+
+HMatrix HMatrix::diagonal(const std::vector<C>& d) {
+  HMatrix m(d.size());
+  for (size_t i = 0; i < d.size(); ++i) m.at(i, i) = d[i];
+  return m;
+}
+
+bool HMatrix::is_diagonal() const {
+  for (size_t r = 0; r < dim; ++r)
+    for (size_t c = 0; c < dim; ++c)
+      if (r != c && norm2(at(r, c)) != 0.0) return false;
+  return true;
+}
+
+std::vector<C> HMatrix::diagonal_entries() const {
+  std::vector<C> d(dim);
+  for (size_t i = 0; i < dim; ++i) d[i] = at(i, i);
+  return d;
+}
+
+HMatrix HMatrix::mul(const HMatrix& o) const {
+  HMatrix out(dim);
+  for (size_t r = 0; r < dim; ++r)
+    for (size_t k = 0; k < dim; ++k) {
+      const C x = at(r, k);
+      if (norm2(x) == 0.0) continue;
+      for (size_t c = 0; c < dim; ++c) {
+        C p = x * o.at(k, c);
+        C& t = out.at(r, c);
+        t.re += p.re;
+        t.im += p.im;
+      }
+    }
+  return out;
+}
+
+HMatrix HMatrix::embed(const std::vector<uint32_t>& gate_qubits, const std::vector<uint32_t>& qubits) const {
+  std::vector<size_t> position;
+  for (uint32_t q : gate_qubits) {
+    auto it = std::find(qubits.begin(), qubits.end(), q);
+    if (it == qubits.end()) throw std::logic_error("qubit missing from embedding");
+    position.push_back(size_t(it - qubits.begin()));
+  }
+  size_t gate_mask = 0;
+  for (size_t p : position) gate_mask |= size_t(1) << p;
+  HMatrix out(size_t(1) << qubits.size());
+  auto local = [&](size_t index) {
+    size_t l = 0;
+    for (size_t j = 0; j < position.size(); ++j) l |= ((index >> position[j]) & 1) << j;
+    return l;
+  };
+  for (size_t r = 0; r < out.dim; ++r)
+    for (size_t c = 0; c < out.dim; ++c)
+      if ((r & ~gate_mask) == (c & ~gate_mask)) out.at(r, c) = at(local(r), local(c));
+  return out;
+}
+
+HMatrix HMatrix::controlled(size_t controls, size_t state) const {
+  HMatrix out = identity(controls + qubits());
+  const size_t mask = (size_t(1) << controls) - 1;
+  for (size_t r = 0; r < out.dim; ++r)
+    for (size_t c = 0; c < out.dim; ++c) {
+      const bool rc = (r & mask) == state, cc = (c & mask) == state;
+      if (rc && cc)
+        out.at(r, c) = at(r >> controls, c >> controls);
+      else if (rc || cc)
+        out.at(r, c) = {0.0, 0.0};
+    }
+  return out;
+}
+
+std::vector<uint32_t> HOp::qubits() const {
+  std::vector<uint32_t> q(targets);
+  for (auto& c : controls) q.push_back(c.first);
+  return q;
+}
+
+void HOp::full(std::vector<uint32_t>& qs, HMatrix& m) const {
+  if (controls.empty()) {
+    qs = targets;
+    m = matrix;
+    return;
+  }
+  size_t state = 0;
+  qs.clear();
+  for (size_t i = 0; i < controls.size(); ++i) {
+    state |= size_t(controls[i].second) << i;
+    qs.push_back(controls[i].first);
+  }
+  qs.insert(qs.end(), targets.begin(), targets.end());
+  m = matrix.controlled(controls.size(), state);
+}
+
+namespace {
+
+bool contains(const std::vector<uint32_t>& v, uint32_t x) { return std::find(v.begin(), v.end(), x) != v.end(); }
+
+// One growth sweep of a fused group over the ops after its seed
+// (src/fusion.rs:126-170).
+void grow(const std::vector<HOp>& ops, std::vector<bool>& done, size_t seed, std::vector<size_t>& members,
+          std::vector<uint32_t>& qubits, size_t max_qubits, bool connected_only,
+          const std::function<size_t(const HOp&)>& width) {
+  std::vector<uint32_t> blocked;
+  for (size_t i = seed + 1; i < ops.size(); ++i) {
+    if (done[i]) continue;
+    if (connected_only &&
+        std::all_of(qubits.begin(), qubits.end(), [&](uint32_t q) { return contains(blocked, q); }))
+      break;
+    const std::vector<uint32_t> oq = ops[i].qubits();
+    bool touches_blocked = false;
+    std::vector<uint32_t> fresh;
+    for (uint32_t q : oq) {
+      if (contains(blocked, q)) touches_blocked = true;
+      if (!contains(qubits, q)) fresh.push_back(q);
+    }
+    const bool connected = fresh.size() < oq.size();
+    const bool fits = width(ops[i]) <= max_qubits && qubits.size() + fresh.size() <= max_qubits;
+    if (!touches_blocked && fits && (connected || !connected_only)) {
+      done[i] = true;
+      members.push_back(i);
+      qubits.insert(qubits.end(), fresh.begin(), fresh.end());
+    } else {
+      for (uint32_t q : oq)
+        if (!contains(blocked, q)) blocked.push_back(q);
+    }
+  }
+  std::sort(members.begin(), members.end());
+}
+
+}  // namespace
+
+std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
+                            const std::function<bool(const HOp&)>& fusable) {
+  const std::function<size_t(const HOp&)> width = [&](const HOp& op) {
+    return fusable(op) ? op.width() : SIZE_MAX;
+  };
+  std::vector<bool> done(ops.size(), false);
+  std::vector<HOp> fused;
+  for (size_t seed = 0; seed < ops.size(); ++seed) {
+    if (done[seed]) continue;
+    done[seed] = true;
+    std::vector<size_t> members{seed};
+    std::vector<uint32_t> qubits = ops[seed].qubits();
+    if (width(ops[seed]) <= max_qubits) {
+      grow(ops, done, seed, members, qubits, max_qubits, true, width);
+      grow(ops, done, seed, members, qubits, max_qubits, false, width);
+    }
+    if (members.size() == 1) {
+      fused.push_back(ops[seed]);
+      continue;
+    }
+    std::sort(qubits.begin(), qubits.end());
+    HMatrix m = HMatrix::identity(qubits.size());
+    for (size_t i : members) {
+      std::vector<uint32_t> oq;
+      HMatrix om;
+      ops[i].full(oq, om);
+      m = om.embed(oq, qubits).mul(m);
+    }
+    HOp f;
+    f.targets = qubits;
+    f.matrix = std::move(m);
+    f.diagonal = f.matrix.is_diagonal();
+    fused.push_back(std::move(f));
+  }
+  return fused;
+}
+
+std::vector<HOp> fuse(const std::vector<HOp>& ops, size_t max_qubits) {
+  return fuse_where(ops, max_qubits, [](const HOp&) { return true; });
+}
+
+}  // namespace qvdg

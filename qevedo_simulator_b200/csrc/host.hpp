@@ -1,0 +1,59 @@
+// Host-side gate algebra and greedy fusion of the B200 engine.
+//
+// Matrix algebra follows src/matrix.rs:99-196 (index bit j = qubit j; `mul`
+// skips exact zeros; `embed` and `controlled` keep the reference's bit
+// order). Fusion follows src/fusion.rs:58-170: greedy and dependency-aware,
+// growing a group first along gates that share a qubit with it, then with
+// unrelated gates, up to `max_qubits`; groups of one op keep their controls.
+#pragma once
+
+#include <stdint.h>
+
+#include <algorithm>
+#include <functional>
+#include <vector>
+
+namespace qvdg {
+
+struct C {
+  double re, im;
+};
+inline C operator*(C a, C b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline double norm2(C a) { return a.re * a.re + a.im * a.im; }
+
+struct HMatrix {
+  size_t dim = 0;
+  std::vector<C> a;  // row-major
+
+  HMatrix() = default;
+  explicit HMatrix(size_t d) : dim(d), a(d * d, C{0.0, 0.0}) {}
+  static HMatrix identity(size_t qubits);
+  static HMatrix diagonal(const std::vector<C>& d);
+  C& at(size_t r, size_t c) { return a[r * dim + c]; }
+  const C& at(size_t r, size_t c) const { return a[r * dim + c]; }
+  size_t qubits() const { return size_t(__builtin_ctzll(dim)); }
+  bool is_diagonal() const;
+  std::vector<C> diagonal_entries() const;
+  HMatrix mul(const HMatrix& o) const;
+  HMatrix embed(const std::vector<uint32_t>& gate_qubits, const std::vector<uint32_t>& qubits) const;
+  HMatrix controlled(size_t controls, size_t state) const;
+};
+
+struct HOp {
+  std::vector<uint32_t> targets;
+  std::vector<std::pair<uint32_t, bool>> controls;
+  HMatrix matrix;
+  bool diagonal = false;  // cached matrix.is_diagonal()
+
+  std::vector<uint32_t> qubits() const;
+  size_t width() const { return targets.size() + controls.size(); }
+  // The op as one matrix on [controls..., targets...] (src/fusion.rs:38-55).
+  void full(std::vector<uint32_t>& qs, HMatrix& m) const;
+};
+
+// Greedy fusion; ops with !fusable(op) are never merged and block their qubits.
+std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
+                            const std::function<bool(const HOp&)>& fusable);
+std::vector<HOp> fuse(const std::vector<HOp>& ops, size_t max_qubits);
+
+}  // namespace qvdg

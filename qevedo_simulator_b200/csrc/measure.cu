@@ -1,0 +1,588 @@
+// Measurement on the device: FP64 reductions and the two-pass sampler.
+//
+// Reductions (norm, per-bit probabilities) accumulate in double precision in
+// a fixed order per launch shape, so repeated calls give identical results.
+//
+// The sampler restates StateVector::sample_unordered (src/measure.rs:104-174)
+// so that, for the same amplitudes and the same uniforms, every outcome is
+// bit-identical to the reference's:
+//   - the state is cut into chunks of CHUNK_BLOCKS * LANES amplitudes
+//     (4096 * 8 = 32768 for complex64, 4096 * 4 = 16384 for complex128,
+//     src/measure.rs:13 and src/simd.rs:71-97), in physical index order;
+//   - p = re*re + im*im in f64 without contraction (__dmul_rn/__dadd_rn);
+//   - each chunk sum is one sequential left fold in index order (one lane
+//     owns a chunk; a warp loads 32 chunks' data coalesced and transposes it
+//     through shared memory);
+//   - the chunk prefix is sequential; targets = u * total are sorted in f64
+//     total order; bounds are partition points of the prefix;
+//   - the walk adds nonzero p in index order from prefix[chunk] and emits an
+//     index while target < cumulative, pads with the last nonzero index.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace qvdg {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__host__ __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+template <typename T>
+__device__ __forceinline__ double prob(const cplx_t<T>& a) {
+  const double re = double(a.x), im = double(a.y);
+  return __dadd_rn(__dmul_rn(re, re), __dmul_rn(im, im));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block sum (result valid in thread 0).
+__device__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[w];
+  return t;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_sumsq(const cplx_t<T>* __restrict__ psi, uint64_t len,
+                                                    double* __restrict__ partials) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < len; i += stride) {
+    const cplx_t<T> a = psi[i];
+    acc += double(a.x) * double(a.x) + double(a.y) * double(a.y);
+  }
+  const double t = block_sum(acc, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+// Sums `count` vectors of `width` doubles (vector i at partials + i*width)
+// into out[0..width), each component in index order.
+__global__ void k_sum_columns(const double* __restrict__ partials, int count, int width, double* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= width) return;
+  double t = 0.0;
+  for (int i = 0; i < count; ++i) t += partials[size_t(i) * width + j];
+  out[j] = t;
+}
+
+// Per-bit probabilities. A segment is 1024 consecutive amplitudes: bits 0-1
+// inside a thread (4 elements), bits 2-9 from the thread index. Each block
+// takes `per_block` consecutive segments (a power of two), so the low
+// log2(per_block) segment bits vary inside the block and the others are fixed
+// by the block index. Each block writes P(bit = 1) for every bit, then the
+// total, to partials[block * (n + 1) + ...].
+constexpr int kMaxVarBits = 16;
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_bit_probs(const cplx_t<T>* __restrict__ psi, int n,
+                                                        uint64_t per_block, int var_bits,
+                                                        double* __restrict__ partials) {
+  __shared__ double red[32];
+  const uint64_t len = uint64_t(1) << n;
+  double tot = 0.0, lo0 = 0.0, lo1 = 0.0;
+  double hv[kMaxVarBits];
+#pragma unroll
+  for (int b = 0; b < kMaxVarBits; ++b) hv[b] = 0.0;
+  for (uint64_t i = 0; i < per_block; ++i) {
+    const uint64_t first = ((uint64_t(blockIdx.x) * per_block + i) << 10) + uint64_t(threadIdx.x) * 4;
+    double st = 0.0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (first + e < len) {
+        const double p = prob<T>(psi[first + e]);
+        st += p;
+        if (e & 1) lo0 += p;
+        if (e & 2) lo1 += p;
+      }
+    }
+    tot += st;
+#pragma unroll
+    for (int b = 0; b < kMaxVarBits; ++b)
+      if ((i >> b) & 1) hv[b] += st;
+  }
+  double* out = partials + size_t(blockIdx.x) * (n + 1);
+  for (int bit = 0; bit < n; ++bit) {
+    double v = 0.0;
+    if (bit == 0) {
+      v = lo0;
+    } else if (bit == 1) {
+      v = lo1;
+    } else if (bit < 10) {
+      v = ((threadIdx.x >> (bit - 2)) & 1) ? tot : 0.0;
+    } else if (bit < 10 + var_bits) {
+#pragma unroll
+      for (int b = 0; b < kMaxVarBits; ++b)
+        if (b == bit - 10) v = hv[b];
+    } else {
+      v = ((uint64_t(blockIdx.x) >> (bit - 10 - var_bits)) & 1) ? tot : 0.0;
+    }
+    const double s = block_sum(v, red);
+    if (threadIdx.x == 0) out[bit] = s;
+  }
+  const double s = block_sum(tot, red);
+  if (threadIdx.x == 0) out[n] = s;
+}
+
+template <typename T>
+__global__ void k_probs(const cplx_t<T>* __restrict__ psi, double* __restrict__ out, uint64_t first, uint64_t count,
+                        const uint64_t* __restrict__ tables, int ntables) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < count; t += stride) {
+    uint64_t i = first + t, p = i;
+    if (ntables) {
+      p = 0;
+      for (int b = 0; b < ntables; ++b) p |= tables[b * 256 + ((i >> (8 * b)) & 255)];
+    }
+    const cplx_t<T> a = psi[p];
+    out[t] = double(a.x) * double(a.x) + double(a.y) * double(a.y);
+  }
+}
+
+// ---------------------------------------------------------------- sampler
+// Amplitudes per lane per step: two complex64 (one 16-byte load) or one
+// complex128.
+template <typename T>
+struct Step {
+  static constexpr int per_lane = sizeof(T) == 4 ? 2 : 1;
+  static constexpr int width = 32 * per_lane;  // amplitudes per chunk per step
+};
+
+constexpr int kSampWarps = 2;
+
+// Pass 1: sequential f64 sum of p over each chunk (src/measure.rs:110-118).
+template <typename T>
+__global__ void __launch_bounds__(32 * kSampWarps) k_chunk_sums(const cplx_t<T>* __restrict__ psi, uint64_t len,
+                                                                 uint64_t chunk_len, uint64_t nchunks,
+                                                                 double* __restrict__ sums) {
+  constexpr int W = Step<T>::width;
+  __shared__ double sp[kSampWarps][32][W + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t chunk0 = (uint64_t(blockIdx.x) * kSampWarps + warp) * 32;
+  if (chunk0 >= nchunks) return;
+  const int live = int(umin64(32, nchunks - chunk0));
+  double s = 0.0;
+  for (uint64_t pos = 0; pos < chunk_len; pos += W) {
+    for (int c = 0; c < live; ++c) {
+      const uint64_t base = (chunk0 + c) * chunk_len + pos;
+#pragma unroll
+      for (int e = 0; e < Step<T>::per_lane; ++e) {
+        const uint64_t i = base + uint64_t(lane) * Step<T>::per_lane + e;
+        sp[warp][c][lane * Step<T>::per_lane + e] = (i < len && pos + lane * Step<T>::per_lane + e < chunk_len)
+                                                        ? prob<T>(psi[i])
+                                                        : 0.0;
+      }
+    }
+    __syncwarp();
+    if (lane < live)
+      for (int j = 0; j < W; ++j) s = __dadd_rn(s, sp[warp][lane][j]);
+    __syncwarp();
+  }
+  if (lane < live) sums[chunk0 + lane] = s;
+}
+
+// prefix[0] = 0, prefix[c + 1] = prefix[c] + sums[c], sequentially
+// (src/measure.rs:119-124).
+__global__ void k_prefix(const double* __restrict__ sums, uint64_t nchunks, double* __restrict__ prefix) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double p = 0.0;
+  prefix[0] = 0.0;
+  for (uint64_t c = 0; c < nchunks; ++c) {
+    p = __dadd_rn(p, sums[c]);
+    prefix[c + 1] = p;
+  }
+}
+
+// Total-order key of a double (f64::total_cmp order as unsigned integers).
+__device__ __forceinline__ uint64_t order_key(double x) {
+  const uint64_t b = uint64_t(__double_as_longlong(x));
+  return (b >> 63) ? ~b : (b | (uint64_t(1) << 63));
+}
+__device__ __forceinline__ double from_key(uint64_t k) {
+  const uint64_t b = (k >> 63) ? (k & ~(uint64_t(1) << 63)) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+// targets = u * total (src/measure.rs:125), as sort keys.
+__global__ void k_target_keys(const double* __restrict__ uniforms, size_t shots, const double* __restrict__ total,
+                              uint64_t* __restrict__ keys) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < shots) keys[i] = order_key(__dmul_rn(uniforms[i], *total));
+}
+
+__global__ void k_keys_to_targets(const uint64_t* __restrict__ keys, size_t shots, double* __restrict__ targets) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < shots) targets[i] = from_key(keys[i]);
+}
+
+// bounds[c] = number of targets < prefix[c] (partition_point,
+// src/measure.rs:128-131); chunks that hold shots are appended to `active`.
+__global__ void k_bounds(const double* __restrict__ targets, size_t shots, const double* __restrict__ prefix,
+                         uint64_t nchunks, uint64_t* __restrict__ bounds) {
+  const uint64_t c = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c > nchunks) return;
+  const double p = prefix[c];
+  size_t lo = 0, hi = shots;
+  while (lo < hi) {
+    const size_t mid = (lo + hi) >> 1;
+    if (targets[mid] < p)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  bounds[c] = lo;
+}
+
+__global__ void k_active(const uint64_t* __restrict__ bounds, uint64_t nchunks, size_t shots,
+                         uint32_t* __restrict__ active, uint32_t* __restrict__ count) {
+  const uint64_t c = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= nchunks) return;
+  const uint64_t lo = bounds[c], hi = umin64(bounds[c + 1], shots);
+  if (lo < hi) active[atomicAdd(count, 1u)] = uint32_t(c);
+}
+
+// Pass 2: each lane walks one chunk that holds shots (src/measure.rs:134-167).
+template <typename T>
+__global__ void __launch_bounds__(32 * kSampWarps) k_walk(const cplx_t<T>* __restrict__ psi, uint64_t len,
+                                                          uint64_t chunk_len, const uint32_t* __restrict__ active,
+                                                          const uint32_t* __restrict__ num_active,
+                                                          const double* __restrict__ prefix,
+                                                          const uint64_t* __restrict__ bounds, size_t shots,
+                                                          const double* __restrict__ targets,
+                                                          uint64_t* __restrict__ out) {
+  constexpr int W = Step<T>::width;
+  __shared__ double sp[kSampWarps][32][W + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t first = (blockIdx.x * kSampWarps + warp) * 32;
+  const uint32_t total_active = *num_active;
+  if (first >= total_active) return;
+  const int live = int(umin64(32, total_active - first));
+  uint64_t chunk = 0, shot = 0, hi = 0, last_nonzero = 0;
+  double cumulative = 0.0;
+  bool walking = false;
+  if (lane < live) {
+    chunk = active[first + lane];
+    shot = bounds[chunk];
+    hi = umin64(bounds[chunk + 1], shots);
+    cumulative = prefix[chunk];
+    last_nonzero = chunk * chunk_len;
+    walking = shot < hi;
+  }
+  for (uint64_t pos = 0; pos < chunk_len; pos += W) {
+    const unsigned busy = __ballot_sync(0xffffffffu, walking);
+    if (!busy) break;
+    for (int c = 0; c < live; ++c) {
+      if (!((busy >> c) & 1)) continue;
+      const uint64_t cc = __shfl_sync(0xffffffffu, chunk, c);
+      const uint64_t base = cc * chunk_len + pos;
+#pragma unroll
+      for (int e = 0; e < Step<T>::per_lane; ++e) {
+        const uint64_t off = uint64_t(lane) * Step<T>::per_lane + e;
+        sp[warp][c][off] = (base + off < len && pos + off < chunk_len) ? prob<T>(psi[base + off]) : 0.0;
+      }
+    }
+    __syncwarp();
+    if (walking) {
+      for (int j = 0; j < W; ++j) {
+        const double p = sp[warp][lane][j];
+        if (p == 0.0) continue;
+        const uint64_t index = chunk * chunk_len + pos + j;
+        last_nonzero = index;
+        cumulative = __dadd_rn(cumulative, p);
+        while (shot < hi && targets[shot] < cumulative) out[shot++] = index;
+        if (shot == hi) {
+          walking = false;
+          break;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (lane < live)
+    for (; shot < hi; ++shot) out[shot] = umin64(last_nonzero, len - 1);
+}
+
+// Physical -> logical index through byte tables.
+__global__ void k_remap(uint64_t* __restrict__ out, size_t count, const uint64_t* __restrict__ tables, int ntables) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint64_t x = out[i];
+  uint64_t l = 0;
+  for (int b = 0; b < ntables; ++b) l |= tables[b * 256 + ((x >> (8 * b)) & 255)];
+  out[i] = l;
+}
+
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(kThreads) k_max_diff(const cplx_t<TA>* __restrict__ a,
+                                                       const cplx_t<TB>* __restrict__ b, uint64_t len,
+                                                       const uint64_t* __restrict__ ta, int nta,
+                                                       const uint64_t* __restrict__ tb, int ntb,
+                                                       double* __restrict__ partials) {
+  __shared__ double red[32];
+  double m = 0.0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < len; i += stride) {
+    uint64_t pa = i, pb = i;
+    if (nta) {
+      pa = 0;
+      for (int k = 0; k < nta; ++k) pa |= ta[k * 256 + ((i >> (8 * k)) & 255)];
+    }
+    if (ntb) {
+      pb = 0;
+      for (int k = 0; k < ntb; ++k) pb |= tb[k * 256 + ((i >> (8 * k)) & 255)];
+    }
+    const cplx_t<TA> x = a[pa];
+    const cplx_t<TB> y = b[pb];
+    const double dr = double(x.x) - double(y.x), di = double(x.y) - double(y.y);
+    m = fmax(m, sqrt(dr * dr + di * di));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t = fmax(t, red[w]);
+    partials[blockIdx.x] = t;
+  }
+}
+
+unsigned blocks_for(uint64_t items, int threads) { return unsigned(std::max<uint64_t>(1, (items + threads - 1) / threads)); }
+
+template <typename T>
+double norm_t(StateImpl& s) {
+  const unsigned blocks = unsigned(umin64(uint64_t(s.sms) * 8, std::max<uint64_t>(1, s.size() / kThreads)));
+  double* d = static_cast<double*>(s.work.get((blocks + 1) * sizeof(double)));
+  k_sumsq<T><<<blocks, kThreads, 0, s.stream>>>(static_cast<const cplx_t<T>*>(s.amp), s.size(), d);
+  QVDG_LAUNCH_CHECK();
+  k_sum_columns<<<1, 32, 0, s.stream>>>(d, int(blocks), 1, d + blocks);
+  QVDG_LAUNCH_CHECK();
+  double* h = static_cast<double*>(s.host.get(sizeof(double)));
+  QVDG_CUDA(cudaMemcpyAsync(h, d + blocks, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+  QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  return *h;
+}
+
+template <typename T>
+void bit_probs_t(StateImpl& s, std::vector<double>& p1, double& total) {
+  const int n = int(s.n);
+  const uint64_t segments = (s.size() + 1023) >> 10;  // a power of two
+  uint64_t blocks = 1;
+  while (blocks * 2 <= segments && blocks * 2 <= uint64_t(s.sms) * 4) blocks *= 2;
+  while (segments / blocks > (uint64_t(1) << kMaxVarBits)) blocks *= 2;
+  const uint64_t per_block = segments / blocks;
+  int var_bits = 0;
+  while ((uint64_t(1) << var_bits) < per_block) ++var_bits;
+  const size_t width = size_t(n) + 1;
+  double* d = static_cast<double*>(s.work.get((size_t(blocks) + 1) * width * sizeof(double)));
+  k_bit_probs<T><<<unsigned(blocks), kThreads, 0, s.stream>>>(static_cast<const cplx_t<T>*>(s.amp), n, per_block,
+                                                              var_bits, d);
+  QVDG_LAUNCH_CHECK();
+  double* sum = d + size_t(blocks) * width;
+  k_sum_columns<<<blocks_for(width, 64), 64, 0, s.stream>>>(d, int(blocks), int(width), sum);
+  QVDG_LAUNCH_CHECK();
+  double* h = static_cast<double*>(s.host.get(width * sizeof(double)));
+  QVDG_CUDA(cudaMemcpyAsync(h, sum, width * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+  QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  p1.assign(h, h + n);
+  total = h[n];
+}
+
+// Byte tables mapping an index through a bit permutation: table bit q of
+// the input -> bit perm[q] of the output.
+int permutation_tables(StateImpl& s, const std::vector<uint32_t>& perm, uint64_t* dev) {
+  const int ntables = int((s.n + 7) / 8);
+  std::vector<uint64_t> t(size_t(std::max(ntables, 1)) * 256, 0);
+  for (int b = 0; b < ntables; ++b)
+    for (int v = 0; v < 256; ++v) {
+      uint64_t p = 0;
+      for (int bit = 0; bit < 8; ++bit) {
+        const uint32_t q = uint32_t(8 * b + bit);
+        if (q < s.n && ((v >> bit) & 1)) p |= uint64_t(1) << perm[q];
+      }
+      t[size_t(b) * 256 + v] = p;
+    }
+  QVDG_CUDA(cudaMemcpyAsync(dev, t.data(), t.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, s.stream));
+  QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  return ntables;
+}
+
+template <typename T>
+void probabilities_t(StateImpl& s, double* out_host) {
+  uint64_t* tables = nullptr;
+  int nt = 0;
+  if (!s.identity_layout()) {
+    tables = static_cast<uint64_t*>(s.work2.get(size_t((s.n + 7) / 8) * 256 * sizeof(uint64_t)));
+    nt = permutation_tables(s, s.layout, tables);
+  }
+  const uint64_t chunk = uint64_t(1) << 24;
+  const uint64_t len = s.size();
+  double* d = static_cast<double*>(s.work.get(std::min(chunk, len) * sizeof(double)));
+  for (uint64_t first = 0; first < len; first += chunk) {
+    const uint64_t count = std::min(chunk, len - first);
+    k_probs<T><<<unsigned(umin64(blocks_for(count, kThreads), uint64_t(s.sms) * 16)), kThreads, 0,
+                 s.stream>>>(static_cast<const cplx_t<T>*>(s.amp), d, first, count, tables, nt);
+    QVDG_LAUNCH_CHECK();
+    QVDG_CUDA(cudaMemcpyAsync(out_host + first, d, count * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  }
+}
+
+template <typename T>
+size_t sample_t(StateImpl& s, size_t shots, const double* uniforms_host, uint64_t* out_host) {
+  if (shots == 0) return 0;
+  const uint64_t len = s.size();
+  // CHUNK_BLOCKS (4096) blocks of LANES amplitudes (8 for f32, 4 for f64).
+  const uint64_t chunk_len = sizeof(T) == 4 ? 32768 : 16384;
+  const uint64_t nchunks = (len + chunk_len - 1) / chunk_len;
+  auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t o_sums = 0;
+  const size_t o_prefix = o_sums + align(nchunks * 8);
+  const size_t o_bounds = o_prefix + align((nchunks + 1) * 8);
+  const size_t o_active = o_bounds + align((nchunks + 1) * 8);
+  const size_t o_count = o_active + align(nchunks * 4);
+  const size_t o_uni = o_count + 256;
+  const size_t o_keys = o_uni + align(shots * 8);
+  const size_t o_tmp = o_keys + align(shots * 8);
+  const size_t o_targets = o_tmp + align(shots * 8);
+  const size_t o_out = o_targets + align(shots * 8);
+  const size_t o_tables = o_out + align(shots * 8);
+  const size_t total_bytes = o_tables + align(size_t((s.n + 7) / 8 + 1) * 256 * 8);
+  char* w = static_cast<char*>(s.work.get(total_bytes));
+  double* sums = reinterpret_cast<double*>(w + o_sums);
+  double* prefix = reinterpret_cast<double*>(w + o_prefix);
+  uint64_t* bounds = reinterpret_cast<uint64_t*>(w + o_bounds);
+  uint32_t* active = reinterpret_cast<uint32_t*>(w + o_active);
+  uint32_t* count = reinterpret_cast<uint32_t*>(w + o_count);
+  double* uni = reinterpret_cast<double*>(w + o_uni);
+  uint64_t* keys = reinterpret_cast<uint64_t*>(w + o_keys);
+  uint64_t* tmp = reinterpret_cast<uint64_t*>(w + o_tmp);
+  double* targets = reinterpret_cast<double*>(w + o_targets);
+  uint64_t* out = reinterpret_cast<uint64_t*>(w + o_out);
+  uint64_t* tables = reinterpret_cast<uint64_t*>(w + o_tables);
+  const cplx_t<T>* psi = static_cast<const cplx_t<T>*>(s.amp);
+
+  QVDG_CUDA(cudaMemcpyAsync(uni, uniforms_host, shots * 8, cudaMemcpyHostToDevice, s.stream));
+  const unsigned chunk_blocks = unsigned((nchunks + 32 * kSampWarps - 1) / (32 * kSampWarps));
+  k_chunk_sums<T><<<chunk_blocks, 32 * kSampWarps, 0, s.stream>>>(psi, len, chunk_len, nchunks, sums);
+  QVDG_LAUNCH_CHECK();
+  k_prefix<<<1, 1, 0, s.stream>>>(sums, nchunks, prefix);
+  QVDG_LAUNCH_CHECK();
+  k_target_keys<<<blocks_for(shots, kThreads), kThreads, 0, s.stream>>>(uni, shots, prefix + nchunks, keys);
+  QVDG_LAUNCH_CHECK();
+  DeviceScratch& sort_work = s.work2;
+  radix_sort_u64(keys, tmp, shots, sort_work, s.stream);
+  k_keys_to_targets<<<blocks_for(shots, kThreads), kThreads, 0, s.stream>>>(keys, shots, targets);
+  QVDG_LAUNCH_CHECK();
+  k_bounds<<<blocks_for(nchunks + 1, kThreads), kThreads, 0, s.stream>>>(targets, shots, prefix, nchunks, bounds);
+  QVDG_LAUNCH_CHECK();
+  QVDG_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t), s.stream));
+  k_active<<<blocks_for(nchunks, kThreads), kThreads, 0, s.stream>>>(bounds, nchunks, shots, active, count);
+  QVDG_LAUNCH_CHECK();
+  // Shots that land in chunks: min(bounds[nchunks], shots).
+  uint64_t* hb = static_cast<uint64_t*>(s.host.get(16));
+  QVDG_CUDA(cudaMemcpyAsync(hb, bounds + nchunks, 8, cudaMemcpyDeviceToHost, s.stream));
+  uint32_t* hc = reinterpret_cast<uint32_t*>(hb + 1);
+  QVDG_CUDA(cudaMemcpyAsync(hc, count, 4, cudaMemcpyDeviceToHost, s.stream));
+  QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  const size_t found = size_t(umin64(hb[0], shots));
+  const uint32_t num_active = *hc;
+  if (num_active > 0) {
+    const unsigned walk_blocks = unsigned((num_active + 32 * kSampWarps - 1) / (32 * kSampWarps));
+    k_walk<T><<<walk_blocks, 32 * kSampWarps, 0, s.stream>>>(psi, len, chunk_len, active, count, prefix, bounds,
+                                                            shots, targets, out);
+    QVDG_LAUNCH_CHECK();
+  }
+  if (!s.identity_layout() && found > 0) {
+    // physical bit p holds logical qubit q: inverse of the layout
+    std::vector<uint32_t> inverse(s.n);
+    for (uint32_t q = 0; q < s.n; ++q) inverse[s.layout[q]] = q;
+    const int nt = permutation_tables(s, inverse, tables);
+    k_remap<<<blocks_for(found, kThreads), kThreads, 0, s.stream>>>(out, found, tables, nt);
+    QVDG_LAUNCH_CHECK();
+  }
+  if (found > 0) QVDG_CUDA(cudaMemcpyAsync(out_host, out, found * 8, cudaMemcpyDeviceToHost, s.stream));
+  QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  return found;
+}
+
+}  // namespace
+
+double max_abs_diff(StateImpl& a, StateImpl& b) {
+  if (a.n != b.n) throw Error(1, "states of different sizes");
+  const int nt = int((a.n + 7) / 8);
+  const size_t tbytes = size_t(nt) * 256 * sizeof(uint64_t);
+  uint64_t* ta = static_cast<uint64_t*>(a.work2.get(tbytes));
+  uint64_t* tb = static_cast<uint64_t*>(b.work2.get(tbytes));
+  const int nta = a.identity_layout() ? 0 : permutation_tables(a, a.layout, ta);
+  const int ntb = b.identity_layout() ? 0 : permutation_tables(b, b.layout, tb);
+  QVDG_CUDA(cudaStreamSynchronize(b.stream));
+  const unsigned blocks = unsigned(umin64(uint64_t(a.sms) * 8, std::max<uint64_t>(1, a.size() / kThreads)));
+  double* d = static_cast<double*>(a.work.get(blocks * sizeof(double)));
+  if (a.bits == 32 && b.bits == 32)
+    k_max_diff<float, float><<<blocks, kThreads, 0, a.stream>>>(static_cast<const float2*>(a.amp),
+        static_cast<const float2*>(b.amp), a.size(), ta, nta, tb, ntb, d);
+  else if (a.bits == 32)
+    k_max_diff<float, double><<<blocks, kThreads, 0, a.stream>>>(static_cast<const float2*>(a.amp),
+        static_cast<const double2*>(b.amp), a.size(), ta, nta, tb, ntb, d);
+  else if (b.bits == 32)
+    k_max_diff<double, float><<<blocks, kThreads, 0, a.stream>>>(static_cast<const double2*>(a.amp),
+        static_cast<const float2*>(b.amp), a.size(), ta, nta, tb, ntb, d);
+  else
+    k_max_diff<double, double><<<blocks, kThreads, 0, a.stream>>>(static_cast<const double2*>(a.amp),
+        static_cast<const double2*>(b.amp), a.size(), ta, nta, tb, ntb, d);
+  QVDG_LAUNCH_CHECK();
+  std::vector<double> h(blocks);
+  QVDG_CUDA(cudaMemcpyAsync(h.data(), d, blocks * sizeof(double), cudaMemcpyDeviceToHost, a.stream));
+  QVDG_CUDA(cudaStreamSynchronize(a.stream));
+  double m = 0.0;
+  for (double x : h) m = std::max(m, x);
+  return m;
+}
+
+double norm_sqr(StateImpl& s) { return s.bits == 32 ? norm_t<float>(s) : norm_t<double>(s); }
+
+void bit_probabilities(StateImpl& s, std::vector<double>& p1, double& total) {
+  if (s.bits == 32)
+    bit_probs_t<float>(s, p1, total);
+  else
+    bit_probs_t<double>(s, p1, total);
+}
+
+double probability_one(StateImpl& s, uint32_t physical_bit) {
+  std::vector<double> p1;
+  double total;
+  bit_probabilities(s, p1, total);
+  return p1[physical_bit];
+}
+
+void probabilities(StateImpl& s, double* out_host) {
+  if (s.bits == 32)
+    probabilities_t<float>(s, out_host);
+  else
+    probabilities_t<double>(s, out_host);
+}
+
+size_t sample_unordered(StateImpl& s, size_t shots, const double* uniforms_host, uint64_t* out_host) {
+  return s.bits == 32 ? sample_t<float>(s, shots, uniforms_host, out_host)
+                      : sample_t<double>(s, shots, uniforms_host, out_host);
+}
+
+}  // namespace qvdg

@@ -1,0 +1,46 @@
+// A planned circuit: the passes of a run (staged tiles or plain gates) with
+// their gate programs, built on the host once and uploaded to the device.
+#pragma once
+
+#include <vector>
+
+#include "engine.hpp"
+#include "host.hpp"
+#include "qvdg.h"
+#include "stage.hpp"
+#include "stage_kernel.hpp"
+
+namespace qvdg {
+
+// What planning needs to know about the target state.
+struct Target {
+  uint32_t n = 0;
+  int bits = 32;
+  int sms = 148;
+  std::vector<uint32_t> layout;
+};
+
+struct Program {
+  Target target;
+  StageConfig cfg{};
+  std::vector<LoweredPass> passes;
+  std::vector<double> pass_bytes;  // algorithmic HBM bytes of each pass
+  StageUpload upload;              // host copy of the gate programs and matrices
+  uint64_t gates = 0, kernels = 0, stages = 0;
+  double bytes = 0.0;
+};
+
+Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt);
+
+// Copy the program's gate data to `dst` on `stream` through the state's
+// pinned staging buffer.
+DeviceUpload upload_program(StateImpl& s, const Program& p, DeviceScratch& dst);
+
+// Launch every pass on the state's stream and wait; fills stats (device
+// time between the first and last launch) and, when the state records pass
+// timings, the per-pass device times.
+void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_stats* stats);
+
+Target target_of(const StateImpl& s);
+
+}  // namespace qvdg

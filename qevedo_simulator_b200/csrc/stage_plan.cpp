@@ -1,0 +1,237 @@
+// Stage planning and orchestration on the host (see stage.hpp).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <functional>
+#include <cstring>
+#include <string>
+
+#include "program.hpp"
+#include "stage.hpp"
+#include "stage_kernel.hpp"
+
+namespace qvdg {
+
+namespace {
+
+bool contains(const std::vector<uint32_t>& v, uint32_t x) { return std::find(v.begin(), v.end(), x) != v.end(); }
+
+// Walk pending ops in program order and take each op that `can_run` accepts
+// and that no earlier pending op on one of its qubits holds back
+// (src/blocking.rs:157-179).
+std::vector<size_t> extract(const std::vector<HOp>& ops, const std::vector<bool>& done,
+                            const std::function<bool(const HOp&)>& can_run) {
+  std::vector<size_t> taken;
+  std::vector<uint32_t> blocked;
+  for (size_t i = 0; i < ops.size(); ++i) {
+    if (done[i]) continue;
+    const std::vector<uint32_t> qs = ops[i].qubits();
+    bool touches = false;
+    for (uint32_t q : qs)
+      if (contains(blocked, q)) touches = true;
+    if (!touches && can_run(ops[i])) {
+      taken.push_back(i);
+    } else {
+      for (uint32_t q : qs)
+        if (!contains(blocked, q)) blocked.push_back(q);
+    }
+  }
+  return taken;
+}
+
+}  // namespace
+
+StageConfig stage_config(const Target& s, uint32_t requested) {
+  StageConfig c{};
+  const uint32_t lmax = s.bits == 32 ? 13 : 12;  // 64 KiB tiles
+  uint32_t L = requested ? std::min<uint32_t>(requested, lmax) : lmax;
+  if (!requested) {
+    // Keep at least two tiles per SM on small states.
+    uint32_t spread = 0;
+    while ((uint32_t(1) << spread) < uint32_t(2 * s.sms)) ++spread;
+    while (L > 8 && s.n > L && s.n - L < spread) --L;
+  }
+  L = std::min<uint32_t>(L, s.n);
+  c.tile_bits = L;
+  // Contiguous low bits: 16 amplitudes (128 bytes of complex64, 256 of
+  // complex128) per run, fewer for tiny tiles so that half the tile is free.
+  c.low_bits = std::min<uint32_t>(4, L / 2);
+  return c;
+}
+
+std::vector<PlannedPass> plan_stages(const std::vector<HOp>& ops, const std::vector<uint32_t>& layout, uint32_t n,
+                                     const StageConfig& cfg, size_t max_fused) {
+  const uint32_t L = cfg.tile_bits, B = cfg.low_bits;
+  std::vector<PlannedPass> passes;
+  std::vector<bool> done(ops.size(), false);
+  size_t remaining = ops.size();
+  std::vector<uint32_t> physical_of(layout);  // logical -> physical
+  while (remaining > 0) {
+    // Qubits the next gates need, greedily in dependency order, up to the
+    // tile's free capacity (plan_swaps, src/blocking.rs:197-226).
+    std::vector<uint32_t> wanted;  // logical qubits
+    const uint32_t capacity = L - B;
+    extract(ops, done, [&](const HOp& op) {
+      if (op.diagonal) return true;
+      std::vector<uint32_t> fresh;
+      for (uint32_t q : op.targets)
+        if (physical_of[q] >= B && !contains(wanted, q)) fresh.push_back(q);
+      if (wanted.size() + fresh.size() > capacity) return false;
+      wanted.insert(wanted.end(), fresh.begin(), fresh.end());
+      return true;
+    });
+    std::vector<uint32_t> bits;
+    for (uint32_t p = 0; p < B; ++p) bits.push_back(p);
+    for (uint32_t q : wanted) bits.push_back(physical_of[q]);
+    // Fill the rest of the tile with the lowest unused bits (longer runs).
+    for (uint32_t p = B; p < n && bits.size() < L; ++p)
+      if (!contains(bits, p)) bits.push_back(p);
+    std::sort(bits.begin(), bits.end());
+    auto local = [&](uint32_t q) { return contains(bits, physical_of[q]); };
+    const std::vector<size_t> taken = extract(ops, done, [&](const HOp& op) {
+      if (op.diagonal) return true;
+      return std::all_of(op.targets.begin(), op.targets.end(), local);
+    });
+    if (taken.empty()) {
+      // The next gate has more targets than a tile holds: one plain pass.
+      const size_t i = size_t(std::find(done.begin(), done.end(), false) - done.begin());
+      done[i] = true;
+      --remaining;
+      PlannedPass p;
+      p.staged = false;
+      p.ops.push_back(ops[i]);
+      passes.push_back(std::move(p));
+      continue;
+    }
+    std::vector<HOp> stage_ops;
+    for (size_t i : taken) {
+      done[i] = true;
+      stage_ops.push_back(ops[i]);
+    }
+    remaining -= taken.size();
+    // Fuse only ops whose qubits are all local: a fused matrix on a global
+    // control or diagonal target would make it a global target
+    // (src/blocking.rs:265-267).
+    std::vector<HOp> fused = fuse_where(stage_ops, max_fused, [&](const HOp& op) {
+      for (uint32_t q : op.qubits())
+        if (!local(q)) return false;
+      return true;
+    });
+    // Split very long stages so one launch's gate program stays bounded.
+    for (size_t first = 0; first < fused.size(); first += kMaxStageGates) {
+      PlannedPass p;
+      p.tile_bits = bits;
+      const size_t last = std::min(fused.size(), first + kMaxStageGates);
+      p.ops.assign(fused.begin() + long(first), fused.begin() + long(last));
+      passes.push_back(std::move(p));
+    }
+  }
+  return passes;
+}
+
+Target target_of(const StateImpl& s) {
+  Target t;
+  t.n = s.n;
+  t.bits = s.bits;
+  t.sms = s.sms;
+  t.layout = s.layout;
+  return t;
+}
+
+Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt) {
+  Program prog;
+  prog.target = t;
+  prog.gates = ops.size();
+  const size_t max_fused = std::max<uint32_t>(opt.max_fused_qubits, 1);
+  prog.cfg = stage_config(t, opt.tile_qubits);
+  std::vector<PlannedPass> passes;
+  if (opt.staged) {
+    passes = plan_stages(ops, t.layout, t.n, prog.cfg, max_fused);
+  } else {
+    // One pass per fused op (src/simulator.rs:136-143).
+    for (HOp& op : fuse(ops, max_fused)) {
+      PlannedPass p;
+      p.staged = false;
+      p.ops.push_back(std::move(op));
+      passes.push_back(std::move(p));
+    }
+  }
+  const double state_bytes = double(uint64_t(t.bits == 32 ? 8 : 16) << t.n);
+  for (const PlannedPass& p : passes) {
+    prog.passes.push_back(lower_pass(t, p, prog.cfg, prog.upload));
+    prog.kernels += p.ops.size();
+    double b = 2.0 * state_bytes;
+    if (p.staged)
+      ++prog.stages;
+    else
+      b /= double(uint64_t(1) << p.ops[0].controls.size());
+    prog.pass_bytes.push_back(b);
+    prog.bytes += b;
+  }
+  return prog;
+}
+
+DeviceUpload upload_program(StateImpl& s, const Program& p, DeviceScratch& dst) {
+  auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const StageUpload& up = p.upload;
+  const size_t gate_bytes = up.gates.size() * sizeof(TileGate);
+  const size_t mat_bytes = up.mats.size() * (p.target.bits == 32 ? 4 : 8);
+  const size_t total = align(gate_bytes) + align(mat_bytes) + 256;
+  char* h = static_cast<char*>(s.host.get(total));
+  if (gate_bytes) std::memcpy(h, up.gates.data(), gate_bytes);
+  char* hm = h + align(gate_bytes);
+  if (p.target.bits == 32) {
+    float* f = reinterpret_cast<float*>(hm);
+    for (size_t i = 0; i < up.mats.size(); ++i) f[i] = float(up.mats[i]);
+  } else if (mat_bytes) {
+    std::memcpy(hm, up.mats.data(), mat_bytes);
+  }
+  char* d = static_cast<char*>(dst.get(total));
+  QVDG_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, s.stream));
+  DeviceUpload u;
+  u.gates = reinterpret_cast<const TileGate*>(d);
+  u.mats = d + align(gate_bytes);
+  return u;
+}
+
+void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_stats* stats) {
+  const bool timing = s.record_passes;
+  if (timing) {
+    while (s.pass_events.size() < p.passes.size() + 1) {
+      cudaEvent_t e;
+      QVDG_CUDA(cudaEventCreate(&e));
+      s.pass_events.push_back(e);
+    }
+  }
+  QVDG_CUDA(cudaEventRecord(s.ev_start, s.stream));
+  for (size_t i = 0; i < p.passes.size(); ++i) {
+    if (timing) QVDG_CUDA(cudaEventRecord(s.pass_events[i], s.stream));
+    launch_pass(s, p.passes[i], dev);
+  }
+  if (timing) QVDG_CUDA(cudaEventRecord(s.pass_events[p.passes.size()], s.stream));
+  QVDG_CUDA(cudaEventRecord(s.ev_stop, s.stream));
+  QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  float ms = 0.f;
+  QVDG_CUDA(cudaEventElapsedTime(&ms, s.ev_start, s.ev_stop));
+  if (timing) {
+    s.pass_seconds.clear();
+    s.pass_kinds.clear();
+    for (size_t i = 0; i < p.passes.size(); ++i) {
+      float t = 0.f;
+      QVDG_CUDA(cudaEventElapsedTime(&t, s.pass_events[i], s.pass_events[i + 1]));
+      s.pass_seconds.push_back(double(t) * 1e-3);
+      s.pass_kinds.push_back(p.passes[i].staged ? 1 : 0);
+    }
+    s.pass_bytes = p.pass_bytes;
+  }
+  if (stats) {
+    stats->kernels += p.kernels;
+    stats->passes += p.passes.size();
+    stats->stages += p.stages;
+    stats->gate_seconds += ms * 1e-3;
+    stats->bytes += p.bytes;
+  }
+}
+
+}  // namespace qvdg

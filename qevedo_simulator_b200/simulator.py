@@ -1,0 +1,178 @@
+"""`run` and `statevector` on the B200 state-vector engine.
+
+Mirrors the state-vector side of the reference's Python API
+(python/python/qevedo/simulator/__init__.py:96-158, native
+python/src/lib.rs:645-718) and of `run_on` (src/simulator.rs:329-427):
+circuits whose measurements all come at the end are simulated once and
+sampled in two passes; mid-circuit measurements, resets and classical
+feedback run shot by shot with the state resident on the device.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native
+from .circuit import Circuit, Gate, gate_op
+
+BACKENDS = ("auto", "statevector")
+
+
+@dataclass
+class RunResult:
+    """Counts per classical bitstring (classical bit 0 on the right, Qiskit's
+    convention) and run statistics (src/simulator.rs:70-101)."""
+
+    counts: dict
+    backend: str = "statevector"
+    gates: int = 0
+    kernels: int = 0
+    passes: int = 0
+    gate_seconds: float = 0.0
+    measure_seconds: float = 0.0
+    stats: dict = field(default_factory=dict)
+
+
+def _precision_bits(precision: str) -> int:
+    if precision == "single":
+        return 32
+    if precision == "double":
+        return 64
+    raise ValueError('precision must be "single" or "double"')
+
+
+def _check_backend(backend: str):
+    if backend not in BACKENDS:
+        if backend in ("stabilizer", "mps", "near_clifford"):
+            raise ValueError(f"backend `{backend}` is not part of the B200 state-vector engine")
+        raise ValueError(f"unknown backend `{backend}`")
+
+
+def uniforms(rng: np.random.Generator, count: int) -> np.ndarray:
+    """`count` uniforms in [0, 1) (53-bit, as rand's `random::<f64>()`)."""
+    return rng.random(count)
+
+
+def terminal_split(circuit: Circuit):
+    """Index of the first instruction after which only measurements and
+    barriers follow, if everything before is unitary (src/simulator.rs:170-182)."""
+    ins = circuit._instructions
+    split = len(ins)
+    for i in range(len(ins) - 1, -1, -1):
+        if ins[i][0] in ("measure", "barrier"):
+            split = i
+        else:
+            break
+    if all(x[0] in ("gate", "barrier") for x in ins[:split]):
+        return split
+    return None
+
+
+def bitstring(bits) -> str:
+    return "".join("1" if b else "0" for b in reversed(bits))
+
+
+def count_outcomes(outcomes: np.ndarray, measures, num_clbits: int) -> dict:
+    """Counts from sampled basis states (src/simulator.rs:187-230): each shot
+    becomes an integer key (bit c = classical bit c), keys are counted, and
+    only distinct keys are formatted."""
+    if num_clbits <= 64:
+        keys = np.zeros(outcomes.size, dtype=np.uint64)
+        for q, c in measures:
+            keys |= ((outcomes >> np.uint64(q)) & np.uint64(1)) << np.uint64(c)
+        uniq, cnt = np.unique(keys, return_counts=True)
+        out = {}
+        for k, n in zip(uniq.tolist(), cnt.tolist()):
+            out[bitstring([(k >> c) & 1 for c in range(num_clbits)])] = n
+        return dict(sorted(out.items()))
+    out = {}
+    for index in outcomes.tolist():
+        bits = [False] * num_clbits
+        for q, c in measures:
+            bits[c] = bool((index >> q) & 1)
+        key = bitstring(bits)
+        out[key] = out.get(key, 0) + 1
+    return dict(sorted(out.items()))
+
+
+def statevector(circuit: Circuit, *, precision: str = "double", max_fused_qubits: int = 4, staged: bool = True,
+                tile_qubits: int = 0) -> np.ndarray:
+    """The final state of a circuit without measurements, as complex128 in
+    logical order (index bit q = qubit q). Double precision by default, as
+    the reference's `statevector` (python/src/lib.rs:686-718)."""
+    ops = circuit.ops()
+    with _native.DeviceState(circuit.num_qubits, _precision_bits(precision)) as st:
+        st.apply_ops(ops, _native.options(max_fused_qubits, staged, tile_qubits))
+        return st.amplitudes()
+
+
+def run(circuit: Circuit, shots: int = 1024, *, backend: str = "auto", seed: int | None = None,
+        precision: str = "single", max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0,
+        state: _native.DeviceState | None = None) -> RunResult:
+    """Sample `shots` shots of `circuit` on the device state vector.
+
+    `seed` seeds the uniforms (numpy PCG64; the reference seeds rand_pcg's
+    Pcg64, whose streams this engine does not reproduce). Given the same
+    uniforms, every outcome is bit-identical to the reference sampler's. A
+    caller may pass a reusable `state` of the right size and precision.
+    """
+    _check_backend(backend)
+    bits = _precision_bits(precision)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    opts = _native.options(max_fused_qubits, staged, tile_qubits)
+    own = state is None
+    st = state or _native.DeviceState(circuit.num_qubits, bits)
+    try:
+        if not own:
+            st.zero()
+        split = terminal_split(circuit)
+        result = RunResult(counts={})
+        if split is not None:
+            ops = [gate_op(i[1], i[2]) for i in circuit._instructions[:split] if i[0] == "gate"]
+            stats = st.apply_ops(ops, opts)
+            result.gates, result.kernels, result.passes = stats["gates"], stats["kernels"], stats["passes"]
+            result.gate_seconds = stats["gate_seconds"]
+            result.stats = stats
+            t0 = time.perf_counter()
+            measures = [(i[1], i[2]) for i in circuit._instructions[split:] if i[0] == "measure"]
+            outcomes = st.sample_unordered(uniforms(rng, shots))
+            result.counts = count_outcomes(outcomes, measures, circuit.num_clbits)
+            result.measure_seconds = time.perf_counter() - t0
+            return result
+        counts = {}
+        for _ in range(shots):
+            st.zero()
+            clbits = [False] * circuit.num_clbits
+            pending = []
+            for ins in circuit._instructions:
+                kind = ins[0]
+                if kind == "gate":
+                    pending.append(gate_op(ins[1], ins[2]))
+                elif kind == "measure":
+                    s = st.apply_ops(pending, opts)
+                    result.gates += s["gates"]
+                    result.gate_seconds += s["gate_seconds"]
+                    pending = []
+                    t0 = time.perf_counter()
+                    clbits[ins[2]] = bool(st.measure(ins[1], float(rng.random())))
+                    result.measure_seconds += time.perf_counter() - t0
+                elif kind == "reset":
+                    s = st.apply_ops(pending, opts)
+                    result.gates += s["gates"]
+                    pending = []
+                    st.reset(ins[1], float(rng.random()))
+                elif kind == "feedback":
+                    if clbits[ins[3]]:
+                        pending.append(gate_op(Gate(ins[1].lower()), [ins[2]]))
+            s = st.apply_ops(pending, opts)
+            result.gates += s["gates"]
+            key = bitstring(clbits)
+            counts[key] = counts.get(key, 0) + 1
+        result.counts = dict(sorted(counts.items()))
+        return result
+    finally:
+        if own:
+            st.close()

@@ -1,0 +1,47 @@
+"""The C-ABI library loads and exports every entry point include/*.h
+declares (no device calls: these run without a GPU)."""
+
+import ctypes as ct
+import glob
+import os
+import re
+
+from qevedo_simulator_b200 import _native
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for header in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(header).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(qvdg_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_functions()
+    assert len(names) >= 20
+    lib = ct.CDLL(_native.LIBRARY)
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_the_header():
+    assert declared_functions() <= set(_native._SIGNATURES)
+
+
+def test_host_only_calls_need_no_device():
+    lib = _native.lib()
+    assert lib.qvdg_version().decode().startswith("qvdgpu")
+    o = _native.options()
+    lib.qvdg_default_options(ct.byref(o))
+    assert o.max_fused_qubits == 4 and o.staged == 1
+    # Invalid arguments are rejected before any device work, with a message.
+    h = ct.c_void_p()
+    assert lib.qvdg_state_create(10, 16, ct.byref(h)) == 1
+    assert "precision" in lib.qvdg_last_error().decode()
+    assert lib.qvdg_state_destroy(None) == 0
+    assert lib.qvdg_norm_sqr(None, None) == 1

@@ -1,0 +1,94 @@
+"""Device kernels against the naive oracle (tests/kernels.rs:12-92 through
+the C ABI), every precision, plain and staged paths."""
+
+import numpy as np
+import pytest
+
+from conftest import max_distance, random_diagonal, random_qubits, random_state, random_unitary
+from qevedo_simulator_b200 import DeviceState, Op, options
+
+pytestmark = pytest.mark.gpu
+
+# Amplitude tolerances of the reference's kernel tests (tests/kernels.rs:65-72).
+TOL = {64: 1e-12, 32: 2e-6}
+
+
+@pytest.mark.parametrize("bits", [64, 32])
+def test_every_kernel_shape_matches_naive(oracle, bits):
+    rng = np.random.Generator(np.random.PCG64(101 + bits))
+    for case in range(400):
+        n = int(rng.integers(1, 12))
+        k = int(rng.integers(1, min(n, 6) + 1))
+        qubits = random_qubits(rng, n, k)
+        rest = [q for q in range(n) if q not in qubits]
+        if not rest or rng.random() < 0.4:
+            controls = []
+        else:
+            c = int(rng.integers(1, min(len(rest), 3) + 1))
+            controls = [(q, bool(rng.random() < 0.7)) for q in rest[:c]]
+        diagonal = rng.random() < 0.3
+        m = random_diagonal(rng, k) if diagonal else random_unitary(rng, k)
+        initial = random_state(rng, n)
+        expected = oracle.naive_apply_ops(initial, [Op(qubits, controls, m)])
+        with DeviceState(n, bits) as st:
+            st.set_amplitudes(initial)
+            st.apply(m, qubits, controls)
+            d = max_distance(st.amplitudes(), expected)
+        assert d < TOL[bits], (case, n, qubits, controls, diagonal, d)
+
+
+@pytest.mark.parametrize("bits", [64, 32])
+@pytest.mark.parametrize("staged", [False, True])
+def test_large_state_every_width(oracle, bits, staged):
+    """tests/kernels.rs:74-92: n = 18, dense k = 1..6 on random qubits (the
+    grid-stride / many-tile paths)."""
+    rng = np.random.Generator(np.random.PCG64(3))
+    n = 18
+    initial = random_state(rng, n)
+    for k in range(1, 7):
+        qubits = random_qubits(rng, n, k)
+        m = random_unitary(rng, k)
+        expected = oracle.naive_apply_ops(initial, [Op(qubits, [], m)])
+        with DeviceState(n, bits) as st:
+            st.set_amplitudes(initial)
+            st.apply_ops([Op(qubits, [], m)], options(max_fused_qubits=1, staged=staged, tile_qubits=8))
+            assert max_distance(st.amplitudes(), expected) < TOL[bits] * 4, (k, qubits)
+
+
+@pytest.mark.parametrize("bits", [64, 32])
+def test_staged_gate_with_global_controls_and_diagonals(oracle, bits):
+    """Staged tiles with controls and diagonal targets outside the tile (the
+    RegionOp cases of src/blocking.rs:57-149)."""
+    rng = np.random.Generator(np.random.PCG64(17))
+    n = 12
+    for case in range(60):
+        ops = []
+        for _ in range(12):
+            k = int(rng.integers(1, 4))
+            qs = random_qubits(rng, n, k + 2)
+            diagonal = rng.random() < 0.4
+            m = random_diagonal(rng, k) if diagonal else random_unitary(rng, k)
+            nc = int(rng.integers(0, 3))
+            ops.append(Op(qs[:k], [(q, bool(rng.random() < 0.6)) for q in qs[k:k + nc]], m))
+        initial = random_state(rng, n)
+        expected = oracle.naive_apply_ops(initial, ops)
+        for tile in (3, 4, 6):
+            with DeviceState(n, bits) as st:
+                st.set_amplitudes(initial)
+                stats = st.apply_ops(ops, options(max_fused_qubits=3, staged=True, tile_qubits=tile))
+                assert stats["stages"] >= 1
+                assert max_distance(st.amplitudes(), expected) < TOL[bits] * 10, (case, tile)
+
+
+def test_invalid_input_is_rejected():
+    with DeviceState(4, 32) as st:
+        with pytest.raises(ValueError, match="out of range"):
+            st.apply(np.eye(2), [4])
+        with pytest.raises(ValueError, match="twice"):
+            st.apply(np.eye(4), [1, 1])
+        with pytest.raises(ValueError, match="expected"):
+            st.set_amplitudes(np.zeros(8))
+        with pytest.raises(ValueError):
+            st.swap_physical([(0, 0)])
+    with pytest.raises(ValueError, match="precision"):
+        DeviceState(4, 16)
