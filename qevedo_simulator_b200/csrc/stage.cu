@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(kStageThreads) k_stage(cplx_t<T>* __restrict__
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint8_t tile_bits[48];
   if (threadIdx.x < 48) tile_bits[threadIdx.x] = geo.tile_bits[threadIdx.x];
+  __syncthreads();  // every thread reads tile_bits below
   const int L = geo.L, B = geo.B;
   cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem);
   uint64_t* hi = reinterpret_cast<uint64_t*>(smem + (sizeof(cplx_t<T>) << L));

@@ -92,3 +92,39 @@ def test_invalid_input_is_rejected():
             st.swap_physical([(0, 0)])
     with pytest.raises(ValueError, match="precision"):
         DeviceState(4, 16)
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_full_size_tiles_and_plans(oracle, bits):
+    """The benchmark's tile shape (13 local qubits for complex64, 12 for
+    complex128) on a 20-qubit grid circuit, through apply_ops and through a
+    reusable plan; both match the plain path and the naive oracle."""
+    from qevedo_simulator_b200 import Plan, library
+
+    c = library.random_grid_circuit(4, 5, 12, seed=5)
+    ops = c.ops()
+    expected = oracle.naive_statevector(ops, 20)
+    tile = 13 if bits == 32 else 12
+    with DeviceState(20, bits) as st, Plan(ops, 20, bits, options(4, True, tile)) as plan:
+        info = plan.info()
+        assert info["stages"] == info["passes"] and info["passes"] < info["kernels"]
+        st.execute(plan)
+        a = st.amplitudes()
+        assert max_distance(a, expected) < TOL[bits] * 50
+        st.zero()
+        st.apply_ops(ops, options(4, True, tile))
+        assert max_distance(st.amplitudes(), a) == 0.0
+        st.zero()
+        st.set_pass_timing(True)
+        st.execute(plan)
+        sec, byt, kind = st.pass_times()
+        assert len(sec) == info["passes"] and np.all(kind == 1) and np.all(sec > 0)
+        assert max_distance(st.amplitudes(), a) == 0.0
+
+
+def test_plan_rejects_a_mismatched_state():
+    from qevedo_simulator_b200 import Plan
+
+    with DeviceState(6, 32) as st, Plan([Op([0], [], np.eye(2))], 7, 32) as plan:
+        with pytest.raises(ValueError, match="another state size"):
+            st.execute(plan)
