@@ -242,7 +242,7 @@ def run_ours(args, rank: int, world: int):
     circuit = build_circuit(n, depth)
     ops = circuit.ops()
     fused = args.fusion
-    tuned = Plan(ops, n, 32, options(fused, staged=True))
+    tuned = Plan(ops, n, 32, options(fused, staged=True, math=args.math))
     plain = Plan(ops, n, 32, options(4, staged=False))
     st = DeviceState(n, 32)
     st.set_pass_timing(True)
@@ -296,7 +296,8 @@ def run_ours(args, rank: int, world: int):
     per_launch = float(staged_bytes.mean()) if staged_bytes.size else float(byt.mean())
     achieved = per_launch / avg / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": args.traffic, "kernel": "k_stage<float>",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": args.traffic,
+                "kernel": "k_stage_tc" if args.math == "tensor" else "k_stage<float>",
                 "peak_source": peaks["source"], "bytes_per_launch": per_launch, "avg_launch_s": avg,
                 "whole_run_gbs": info["bytes"] / step / 1e9}
     # Accuracy: tuned complex64 against a complex128 run of the same circuit.
@@ -312,7 +313,8 @@ def run_ours(args, rank: int, world: int):
     e2e = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        res = run(circuit.copy().measure_all(), SHOTS, seed=7 + i, max_fused_qubits=fused, state=st)
+        res = run(circuit.copy().measure_all(), SHOTS, seed=7 + i, max_fused_qubits=fused, math=args.math,
+                  state=st)
         if i >= args.warmup:
             e2e.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e))
@@ -339,7 +341,7 @@ def run_ours(args, rank: int, world: int):
             "gpu_launches": int(info["passes"]) * args.steps,
             "clocks": clocks.summary(),
             "tuned": {"s": step, "passes": info["passes"], "stages": info["stages"], "kernels": info["kernels"],
-                      "max_fused_qubits": fused},
+                      "max_fused_qubits": fused, "math": args.math},
             "plain": {"s": plain_s, "passes": plain_info["passes"], "kernels": plain_info["kernels"]},
             "tuned_over_plain": step / plain_s,
             "max_amp_err_vs_c128": err,
@@ -367,7 +369,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--qubits", type=int, default=30)
-    ap.add_argument("--fusion", type=int, default=4)
+    ap.add_argument("--fusion", type=int, default=5)
+    ap.add_argument("--math", choices=["tensor", "fp32"], default="tensor")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-check", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0)

@@ -66,6 +66,13 @@ typedef struct {
 /* Planner choice for the staged path. */
 enum { QVDG_PLANNER_GREEDY = 0, QVDG_PLANNER_LEARNED = 1 };
 
+/* Arithmetic of the staged path's fused dense gates. FP32: CUDA-core fp32
+ * complex multiply-adds. TENSOR (complex64 states): gates on 3 to 6 qubits as
+ * real matrix products on the tensor cores, operands split into bf16 high and
+ * low parts with fp32 accumulation (hi*hi + hi*lo + lo*hi, about 16
+ * significant bits per product; diagonal and 1-2 qubit gates stay fp32). */
+enum { QVDG_MATH_FP32 = 0, QVDG_MATH_TENSOR = 1 };
+
 /* Simulator options. Reference: simulator::Options, src/simulator.rs:37-66
  * (defaults max_fused_qubits = 4, region_bits = Some(14)). */
 typedef struct {
@@ -81,6 +88,8 @@ typedef struct {
   uint32_t tile_qubits;
   /* QVDG_PLANNER_GREEDY or QVDG_PLANNER_LEARNED. */
   uint32_t planner;
+  /* QVDG_MATH_FP32 or QVDG_MATH_TENSOR. */
+  uint32_t math;
 } qvdg_options;
 
 /* What a run did. Reference: simulator::Stats, src/simulator.rs:70-93, plus

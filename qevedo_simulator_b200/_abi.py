@@ -25,6 +25,7 @@ class QvdgOptions(ct.Structure):
         ("staged", ct.c_uint32),
         ("tile_qubits", ct.c_uint32),
         ("planner", ct.c_uint32),
+        ("math", ct.c_uint32),
     ]
 
 

@@ -98,12 +98,20 @@ def set_device(device: int):
     check(lib().qvdg_set_device(int(device)))
 
 
-def options(max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0, planner: int = 0) -> QvdgOptions:
+MATH = {"fp32": 0, "tensor": 1}
+
+
+def options(max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0, planner: int = 0,
+            math: str = "fp32") -> QvdgOptions:
+    """Simulator options (the reference's Options, src/simulator.rs:37-66).
+    `math="tensor"` runs the staged path's fused 3-6 qubit gates on the
+    tensor cores (complex64 states only)."""
     o = QvdgOptions()
     o.max_fused_qubits = int(max_fused_qubits)
     o.staged = 1 if staged else 0
     o.tile_qubits = int(tile_qubits)
     o.planner = int(planner)
+    o.math = MATH[math]
     return o
 
 

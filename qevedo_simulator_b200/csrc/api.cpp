@@ -176,6 +176,7 @@ void qvdg_default_options(qvdg_options* opt) {
   opt->staged = 1;
   opt->tile_qubits = 0;
   opt->planner = QVDG_PLANNER_GREEDY;
+  opt->math = QVDG_MATH_FP32;
 }
 
 const char* qvdg_last_error(void) { return g_error.c_str(); }
@@ -203,6 +204,12 @@ qvdg_status qvdg_state_create(uint32_t num_qubits, uint32_t precision_bits, qvdg
                                                 " bytes of device memory for " + std::to_string(num_qubits) +
                                                 " qubits");
       }
+      if (cudaMalloc(&s.status, 256) != cudaSuccess) {
+        cudaGetLastError();
+        s.status = nullptr;
+        throw Error(QVDG_ERR_OUT_OF_MEMORY, "cannot allocate the state's status word");
+      }
+      QVDG_CUDA(cudaMemset(s.status, 0, 256));
       QVDG_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
       QVDG_CUDA(cudaEventCreate(&s.ev_start));
       QVDG_CUDA(cudaEventCreate(&s.ev_stop));
@@ -223,6 +230,7 @@ qvdg_status qvdg_state_destroy(qvdg_state* st) {
   StateImpl& s = st->s;
   if (s.stream) cudaStreamSynchronize(s.stream);
   if (s.amp) cudaFree(s.amp);
+  if (s.status) cudaFree(s.status);
   s.work.release();
   s.work2.release();
   s.host.release();
@@ -468,7 +476,7 @@ qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const
       auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
       const size_t gate_bytes = up.gates.size() * sizeof(TileGate);
       const size_t mat_bytes = up.mats.size() * (precision_bits == 32 ? 4 : 8);
-      std::vector<char> h(align(gate_bytes) + align(mat_bytes) + 256, 0);
+      std::vector<char> h(align(gate_bytes) + align(mat_bytes) + align(up.tc.size()) + 256, 0);
       if (gate_bytes) std::memcpy(h.data(), up.gates.data(), gate_bytes);
       if (precision_bits == 32) {
         float* f = reinterpret_cast<float*>(h.data() + align(gate_bytes));
@@ -476,6 +484,7 @@ qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const
       } else if (mat_bytes) {
         std::memcpy(h.data() + align(gate_bytes), up.mats.data(), mat_bytes);
       }
+      if (!up.tc.empty()) std::memcpy(h.data() + align(gate_bytes) + align(mat_bytes), up.tc.data(), up.tc.size());
       if (cudaMalloc(&plan->device, h.size()) != cudaSuccess) {
         cudaGetLastError();
         plan->device = nullptr;
@@ -484,6 +493,7 @@ qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const
       QVDG_CUDA(cudaMemcpy(plan->device, h.data(), h.size(), cudaMemcpyHostToDevice));
       plan->dev.gates = static_cast<const TileGate*>(plan->device);
       plan->dev.mats = static_cast<const char*>(plan->device) + align(gate_bytes);
+      plan->dev.tc = static_cast<const uint8_t*>(plan->device) + align(gate_bytes) + align(mat_bytes);
     } catch (...) {
       qvdg_plan_destroy(plan);
       throw;

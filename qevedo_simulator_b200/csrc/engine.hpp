@@ -47,6 +47,7 @@ struct StateImpl {
   HostScratch host;              // pinned staging
   int device = 0;
   int sms = 148;
+  int* status = nullptr;  // device word set by kernels whose bounded waits gave up
   // Per-pass device timings of the last gate run (when enabled).
   bool record_passes = false;
   std::vector<cudaEvent_t> pass_events;

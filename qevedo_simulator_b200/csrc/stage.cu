@@ -13,99 +13,13 @@
 #include "program.hpp"
 #include "stage.hpp"
 #include "stage_kernel.hpp"
+#include "tile_ops.cuh"
 
 namespace qvdg {
 
 namespace {
 
 constexpr int kStageThreads = 256;
-
-__device__ __forceinline__ uint32_t insert_zeros32(uint32_t x, const uint8_t* pos, int count) {
-  for (int i = 0; i < count; ++i) {
-    const uint32_t p = pos[i];
-    x = ((x >> p) << (p + 1)) | (x & ((1u << p) - 1u));
-  }
-  return x;
-}
-
-// Tile-local offset of group member h (matrix index bit j -> tgt[j]).
-template <int K>
-__device__ __forceinline__ uint32_t member(uint32_t h, const uint8_t* tgt) {
-  uint32_t o = 0;
-#pragma unroll
-  for (int j = 0; j < K; ++j) o |= ((h >> j) & 1u) << tgt[j];
-  return o;
-}
-
-// Dense gate with K <= 4: one thread per group, the group in registers,
-// matrix entries read as warp-wide broadcasts.
-template <typename T, int K>
-__device__ __forceinline__ void tile_dense(cplx_t<T>* tile, int L, const TileGate& g,
-                                           const cplx_t<T>* __restrict__ m) {
-  constexpr int D = 1 << K;
-  uint8_t tgt[K];
-#pragma unroll
-  for (int j = 0; j < K; ++j) tgt[j] = g.tgt[j];
-  uint32_t off[D];
-#pragma unroll
-  for (int h = 0; h < D; ++h) off[h] = member<K>(h, tgt);
-  const uint32_t groups = 1u << (L - g.nfixed);
-  for (uint32_t gi = threadIdx.x; gi < groups; gi += blockDim.x) {
-    const uint32_t b = insert_zeros32(gi, g.fixed, g.nfixed) | g.lcv;
-    cplx_t<T> x[D];
-#pragma unroll
-    for (int h = 0; h < D; ++h) x[h] = tile[b | off[h]];
-#pragma unroll 1
-    for (int r = 0; r < D; ++r) {
-      cplx_t<T> acc = make_c<T>(T(0), T(0));
-#pragma unroll
-      for (int c = 0; c < D; ++c) cmac<T>(acc, __ldg(&m[r * D + c]), x[c]);
-      tile[b | off[r]] = acc;
-    }
-  }
-}
-
-// Dense gate with K = 5, 6: D threads per group, one output row each; the
-// matrix is stored transposed so a warp's row entries are contiguous.
-template <typename T, int K>
-__device__ __forceinline__ void tile_dense_rows(cplx_t<T>* tile, int L, const TileGate& g,
-                                                const cplx_t<T>* __restrict__ mt) {
-  constexpr int D = 1 << K;
-  const uint32_t groups = 1u << (L - g.nfixed);
-  const uint32_t per_wave = blockDim.x / D;
-  const uint32_t r = threadIdx.x % D, slot = threadIdx.x / D;
-  const uint32_t out_off = member<K>(r, g.tgt);
-  for (uint32_t g0 = 0; g0 < groups; g0 += per_wave) {
-    const uint32_t gi = g0 + slot;
-    const bool active = gi < groups;
-    cplx_t<T> acc = make_c<T>(T(0), T(0));
-    uint32_t b = 0;
-    if (active) {
-      b = insert_zeros32(gi, g.fixed, g.nfixed) | g.lcv;
-#pragma unroll 8
-      for (int c = 0; c < D; ++c) cmac<T>(acc, __ldg(&mt[c * D + r]), tile[b | member<K>(c, g.tgt)]);
-    }
-    __syncthreads();
-    if (active) tile[b | out_off] = acc;
-    __syncthreads();
-  }
-}
-
-template <typename T>
-__device__ __forceinline__ void tile_diag(cplx_t<T>* tile, int L, const TileGate& g, const cplx_t<T>* __restrict__ d,
-                                          uint64_t base) {
-  uint32_t dglob = 0;
-  for (int j = 0; j < g.k; ++j)
-    if (g.tgt[j] & 0x80) dglob |= uint32_t((base >> (g.tgt[j] & 0x7f)) & 1) << j;
-  const uint32_t count = 1u << (L - g.nfixed);
-  for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) {
-    const uint32_t e = insert_zeros32(i, g.fixed, g.nfixed) | g.lcv;
-    uint32_t idx = dglob;
-    for (int j = 0; j < g.k; ++j)
-      if (!(g.tgt[j] & 0x80)) idx |= ((e >> g.tgt[j]) & 1u) << j;
-    tile[e] = cmul<T>(__ldg(&d[idx]), tile[e]);
-  }
-}
 
 template <typename T>
 __global__ void __launch_bounds__(kStageThreads) k_stage(cplx_t<T>* __restrict__ psi, const TileGeom geo,
@@ -189,6 +103,49 @@ void stage_launch(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev) 
 
 }  // namespace
 
+namespace {
+
+uint16_t to_bf16(float f) {  // round to nearest even
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
+  return uint16_t((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+}
+
+float from_bf16(uint16_t h) {
+  const uint32_t u = uint32_t(h) << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+// A gate as the real matrix B^T = [[Re M, -Im M], [Im M, Re M]] (row n =
+// output component, column kk = input component), split into bf16 high and
+// low parts, each in the canonical K-major core-matrix layout.
+void append_tc_gate(const HMatrix& m, std::vector<uint8_t>& blob) {
+  const size_t half = m.dim, kd = 2 * half;
+  const size_t base = blob.size();
+  blob.resize(base + 4 * kd * kd, 0);
+  uint8_t* hi = blob.data() + base;
+  uint8_t* lo = hi + 2 * kd * kd;
+  for (size_t n = 0; n < kd; ++n)
+    for (size_t kk = 0; kk < kd; ++kk) {
+      const C e = m.at(n % half, kk % half);
+      double v;
+      if (n < half)
+        v = kk < half ? e.re : -e.im;
+      else
+        v = kk < half ? e.im : e.re;
+      const uint16_t h = to_bf16(float(v));
+      const uint16_t l = to_bf16(float(v - double(from_bf16(h))));
+      const size_t off = (n / 8) * (kd * 16) + (kk / 8) * 128 + (n % 8) * 16 + (kk % 8) * 2;
+      std::memcpy(hi + off, &h, 2);
+      std::memcpy(lo + off, &l, 2);
+    }
+}
+
+}  // namespace
+
 LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig& cfg, StageUpload& up) {
   LoweredPass lp;
   lp.staged = p.staged;
@@ -217,6 +174,7 @@ LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig&
   std::vector<int> local(s.n, -1);
   for (size_t j = 0; j < p.tile_bits.size(); ++j) local[p.tile_bits[j]] = int(j);
   lp.gate_offset = up.gates.size();
+  geo.tc_offset = up.tc.size();
   for (const HOp& op : p.ops) {
     TileGate g{};
     std::vector<uint8_t> fixed;
@@ -251,7 +209,11 @@ LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig&
         g.tgt[j] = uint8_t(l);
         fixed.push_back(uint8_t(l));
       }
-      if (op.targets.size() >= 5) {
+      if (cfg.tensor && tensor_eligible(op, uint32_t(geo.L))) {
+        g.kind = 2;
+        g.mat = uint32_t(up.tc.size() - geo.tc_offset);
+        append_tc_gate(op.matrix, up.tc);
+      } else if (op.targets.size() >= 5) {
         // transposed for the row-parallel kernel
         const size_t D = op.matrix.dim;
         std::vector<C> t(D * D);
@@ -268,6 +230,10 @@ LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig&
     up.gates.push_back(g);
   }
   geo.num_gates = int(up.gates.size() - lp.gate_offset);
+  geo.tc_bytes = uint32_t(up.tc.size() - geo.tc_offset);
+  geo.tensor = geo.tc_bytes > 0 ? 1u : 0u;
+  if (geo.tensor && (geo.L - geo.B > 10 || tc_smem_bytes(geo) > size_t(227 * 1024)))
+    throw Error(QVDG_ERR_INVALID, "internal: tensor-core pass does not fit shared memory");
   return lp;
 }
 
@@ -276,7 +242,9 @@ void launch_pass(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev) {
     launch_plain_gate(s, lp.plain, dev.mats);
     return;
   }
-  if (s.bits == 32)
+  if (lp.geo.tensor)
+    launch_stage_tc(s, lp, dev);
+  else if (s.bits == 32)
     stage_launch<float>(s, lp, dev);
   else
     stage_launch<double>(s, lp, dev);

@@ -34,10 +34,14 @@ struct PlannedPass {
 struct StageConfig {
   uint32_t tile_bits;  // L
   uint32_t low_bits;   // B
+  bool tensor;         // fused 3-6 qubit gates on the tensor cores
 };
 
 struct Target;
-StageConfig stage_config(const Target& t, uint32_t requested_tile_bits);
+StageConfig stage_config(const Target& t, uint32_t requested_tile_bits, bool tensor);
+
+// Whether a fused op of a stage runs on the tensor cores.
+bool tensor_eligible(const HOp& op, uint32_t tile_bits);
 
 // Plan stages for `ops` on the state's current layout (greedy look-ahead in
 // the manner of plan_swaps/extract, src/blocking.rs:151-226).

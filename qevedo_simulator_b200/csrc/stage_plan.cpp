@@ -42,11 +42,17 @@ std::vector<size_t> extract(const std::vector<HOp>& ops, const std::vector<bool>
 
 }  // namespace
 
-StageConfig stage_config(const Target& s, uint32_t requested) {
+bool tensor_eligible(const HOp& op, uint32_t L) {
+  const size_t k = op.targets.size();
+  return !op.diagonal && op.controls.empty() && k >= 3 && k + 7 <= L && k <= 6;
+}
+
+StageConfig stage_config(const Target& s, uint32_t requested, bool tensor) {
   StageConfig c{};
+  c.tensor = tensor && s.bits == 32;
   const uint32_t lmax = s.bits == 32 ? 13 : 12;  // 64 KiB tiles
   uint32_t L = requested ? std::min<uint32_t>(requested, lmax) : lmax;
-  if (!requested) {
+  if (!requested && !c.tensor) {
     // Keep at least two tiles per SM on small states.
     uint32_t spread = 0;
     while ((uint32_t(1) << spread) < uint32_t(2 * s.sms)) ++spread;
@@ -62,6 +68,7 @@ StageConfig stage_config(const Target& s, uint32_t requested) {
 
 std::vector<PlannedPass> plan_stages(const std::vector<HOp>& ops, const std::vector<uint32_t>& layout, uint32_t n,
                                      const StageConfig& cfg, size_t max_fused) {
+  const size_t budget = cfg.tensor ? tc_budget(cfg.tile_bits) : 0;
   const uint32_t L = cfg.tile_bits, B = cfg.low_bits;
   std::vector<PlannedPass> passes;
   std::vector<bool> done(ops.size(), false);
@@ -118,14 +125,23 @@ std::vector<PlannedPass> plan_stages(const std::vector<HOp>& ops, const std::vec
         if (!local(q)) return false;
       return true;
     });
-    // Split very long stages so one launch's gate program stays bounded.
-    for (size_t first = 0; first < fused.size(); first += kMaxStageGates) {
-      PlannedPass p;
-      p.tile_bits = bits;
-      const size_t last = std::min(fused.size(), first + kMaxStageGates);
-      p.ops.assign(fused.begin() + long(first), fused.begin() + long(last));
-      passes.push_back(std::move(p));
+    // Split very long stages so one launch's gate program stays bounded,
+    // and so a tensor-core pass's gate matrices fit in shared memory.
+    PlannedPass p;
+    p.tile_bits = bits;
+    size_t tc_bytes = 0;
+    for (HOp& op : fused) {
+      const size_t b = cfg.tensor && tensor_eligible(op, L) ? tc_gate_bytes(op.targets.size()) : 0;
+      if (!p.ops.empty() && (p.ops.size() >= kMaxStageGates || (b > 0 && tc_bytes + b > budget))) {
+        passes.push_back(std::move(p));
+        p = PlannedPass();
+        p.tile_bits = bits;
+        tc_bytes = 0;
+      }
+      tc_bytes += b;
+      p.ops.push_back(std::move(op));
     }
+    if (!p.ops.empty()) passes.push_back(std::move(p));
   }
   return passes;
 }
@@ -144,7 +160,7 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
   prog.target = t;
   prog.gates = ops.size();
   const size_t max_fused = std::max<uint32_t>(opt.max_fused_qubits, 1);
-  prog.cfg = stage_config(t, opt.tile_qubits);
+  prog.cfg = stage_config(t, opt.tile_qubits, opt.staged && opt.math == QVDG_MATH_TENSOR);
   std::vector<PlannedPass> passes;
   if (opt.staged) {
     passes = plan_stages(ops, t.layout, t.n, prog.cfg, max_fused);
@@ -177,7 +193,8 @@ DeviceUpload upload_program(StateImpl& s, const Program& p, DeviceScratch& dst) 
   const StageUpload& up = p.upload;
   const size_t gate_bytes = up.gates.size() * sizeof(TileGate);
   const size_t mat_bytes = up.mats.size() * (p.target.bits == 32 ? 4 : 8);
-  const size_t total = align(gate_bytes) + align(mat_bytes) + 256;
+  const size_t tc_bytes = up.tc.size();
+  const size_t total = align(gate_bytes) + align(mat_bytes) + align(tc_bytes) + 256;
   char* h = static_cast<char*>(s.host.get(total));
   if (gate_bytes) std::memcpy(h, up.gates.data(), gate_bytes);
   char* hm = h + align(gate_bytes);
@@ -187,11 +204,13 @@ DeviceUpload upload_program(StateImpl& s, const Program& p, DeviceScratch& dst) 
   } else if (mat_bytes) {
     std::memcpy(hm, up.mats.data(), mat_bytes);
   }
+  if (tc_bytes) std::memcpy(hm + align(mat_bytes), up.tc.data(), tc_bytes);
   char* d = static_cast<char*>(dst.get(total));
   QVDG_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, s.stream));
   DeviceUpload u;
   u.gates = reinterpret_cast<const TileGate*>(d);
   u.mats = d + align(gate_bytes);
+  u.tc = reinterpret_cast<const uint8_t*>(d + align(gate_bytes) + align(mat_bytes));
   return u;
 }
 
@@ -212,6 +231,16 @@ void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_s
   if (timing) QVDG_CUDA(cudaEventRecord(s.pass_events[p.passes.size()], s.stream));
   QVDG_CUDA(cudaEventRecord(s.ev_stop, s.stream));
   QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  bool tensor = false;
+  for (const LoweredPass& lp : p.passes) tensor = tensor || (lp.staged && lp.geo.tensor);
+  if (tensor) {
+    int flag = 0;
+    QVDG_CUDA(cudaMemcpy(&flag, s.status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+      QVDG_CUDA(cudaMemset(s.status, 0, sizeof(int)));
+      throw Error(QVDG_ERR_TIMEOUT, "a tensor-core stage gave up waiting for its matrix products");
+    }
+  }
   float ms = 0.f;
   QVDG_CUDA(cudaEventElapsedTime(&ms, s.ev_start, s.ev_stop));
   if (timing) {

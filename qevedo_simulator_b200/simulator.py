@@ -99,19 +99,19 @@ def count_outcomes(outcomes: np.ndarray, measures, num_clbits: int) -> dict:
 
 
 def statevector(circuit: Circuit, *, precision: str = "double", max_fused_qubits: int = 4, staged: bool = True,
-                tile_qubits: int = 0) -> np.ndarray:
+                tile_qubits: int = 0, math: str = "fp32") -> np.ndarray:
     """The final state of a circuit without measurements, as complex128 in
     logical order (index bit q = qubit q). Double precision by default, as
     the reference's `statevector` (python/src/lib.rs:686-718)."""
     ops = circuit.ops()
     with _native.DeviceState(circuit.num_qubits, _precision_bits(precision)) as st:
-        st.apply_ops(ops, _native.options(max_fused_qubits, staged, tile_qubits))
+        st.apply_ops(ops, _native.options(max_fused_qubits, staged, tile_qubits, math=math))
         return st.amplitudes()
 
 
 def run(circuit: Circuit, shots: int = 1024, *, backend: str = "auto", seed: int | None = None,
         precision: str = "single", max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0,
-        state: _native.DeviceState | None = None) -> RunResult:
+        math: str = "fp32", state: _native.DeviceState | None = None) -> RunResult:
     """Sample `shots` shots of `circuit` on the device state vector.
 
     `seed` seeds the uniforms (numpy PCG64; the reference seeds rand_pcg's
@@ -122,7 +122,7 @@ def run(circuit: Circuit, shots: int = 1024, *, backend: str = "auto", seed: int
     _check_backend(backend)
     bits = _precision_bits(precision)
     rng = np.random.Generator(np.random.PCG64(seed))
-    opts = _native.options(max_fused_qubits, staged, tile_qubits)
+    opts = _native.options(max_fused_qubits, staged, tile_qubits, math=math)
     own = state is None
     st = state or _native.DeviceState(circuit.num_qubits, bits)
     try:

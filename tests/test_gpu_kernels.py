@@ -128,3 +128,45 @@ def test_plan_rejects_a_mismatched_state():
     with DeviceState(6, 32) as st, Plan([Op([0], [], np.eye(2))], 7, 32) as plan:
         with pytest.raises(ValueError, match="another state size"):
             st.execute(plan)
+
+
+# Tensor-core stages: fused gates as bf16 hi/lo compensated products with fp32
+# accumulation (about 16 significant bits per product). The bound below is
+# relative to the largest amplitude of the state.
+TC_REL_TOL = 2e-5
+
+
+@pytest.mark.parametrize("n,tile", [(13, 13), (12, 10), (16, 13), (18, 11)])
+def test_tensor_core_stages_match_naive(oracle, n, tile):
+    rng = np.random.Generator(np.random.PCG64(40 + n))
+    initial = random_state(rng, n)
+    for fuse in (3, 4, 5, 6):
+        ops = []
+        for _ in range(30):
+            k = int(rng.integers(1, 4))
+            qs = random_qubits(rng, n, k)
+            m = random_diagonal(rng, k) if rng.random() < 0.25 else random_unitary(rng, k)
+            ops.append(Op(qs, [], m))
+        expected = oracle.naive_apply_ops(initial, ops)
+        with DeviceState(n, 32) as st:
+            st.set_amplitudes(initial)
+            stats = st.apply_ops(ops, options(fuse, True, tile, math="tensor"))
+            got = st.amplitudes()
+        err = max_distance(got, expected) / np.max(np.abs(expected))
+        assert err < TC_REL_TOL, (n, tile, fuse, err, stats)
+
+
+def test_tensor_core_single_wide_gates(oracle):
+    """One dense gate of each tensor-core width (3..6 qubits) on one tile."""
+    rng = np.random.Generator(np.random.PCG64(77))
+    n = 13
+    initial = random_state(rng, n)
+    for k in (3, 4, 5, 6):
+        qubits = random_qubits(rng, n, k)
+        m = random_unitary(rng, k)
+        expected = oracle.naive_apply_ops(initial, [Op(qubits, [], m)])
+        with DeviceState(n, 32) as st:
+            st.set_amplitudes(initial)
+            st.apply_ops([Op(qubits, [], m)], options(6, True, 13, math="tensor"))
+            err = max_distance(st.amplitudes(), expected) / np.max(np.abs(expected))
+        assert err < TC_REL_TOL, (k, qubits, err)
