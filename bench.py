@@ -341,7 +341,8 @@ def run_ours(args, rank: int, world: int):
             "gpu_launches": int(info["passes"]) * args.steps,
             "clocks": clocks.summary(),
             "tuned": {"s": step, "passes": info["passes"], "stages": info["stages"], "kernels": info["kernels"],
-                      "max_fused_qubits": fused, "math": args.math},
+                      "max_fused_qubits": fused, "math": args.math,
+                      "pass_ms": [round(float(x) * 1e3, 3) for x in pass_t[-1]]},
             "plain": {"s": plain_s, "passes": plain_info["passes"], "kernels": plain_info["kernels"]},
             "tuned_over_plain": step / plain_s,
             "max_amp_err_vs_c128": err,

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "program.hpp"
@@ -146,7 +147,231 @@ void append_tc_gate(const HMatrix& m, std::vector<uint8_t>& blob) {
 
 }  // namespace
 
+// Spread the low bits of `x` over the set bits of `mask` (ascending).
+uint32_t spread_bits(uint32_t x, uint32_t mask) {
+  uint32_t out = 0;
+  for (uint32_t bit = 0; mask; mask &= mask - 1, ++bit)
+    if ((x >> bit) & 1) out |= mask & (~mask + 1);
+  return out;
+}
+
+void blob_align(std::vector<uint8_t>& blob) { blob.resize((blob.size() + 15) & ~size_t(15), 0); }
+
+template <class V>
+size_t blob_put(std::vector<uint8_t>& blob, const std::vector<V>& v) {
+  blob_align(blob);
+  const size_t off = blob.size();
+  blob.resize(off + v.size() * sizeof(V));
+  std::memcpy(blob.data() + off, v.data(), v.size() * sizeof(V));
+  return off;
+}
+
+size_t blob_put_c64(std::vector<uint8_t>& blob, const std::vector<C>& v) {
+  std::vector<float> f;
+  for (const C& c : v) {
+    f.push_back(float(c.re));
+    f.push_back(float(c.im));
+  }
+  return blob_put(blob, f);
+}
+
+// Index tables of one gate in a tensor pass, as 32-bit byte offsets into
+// the complex64 tile (element index * 8): the spread of an enumeration index
+// over the tile bits not in `fixed` (64 low + 128 high entries), then the
+// member offsets of the targets (64 entries), or the local part of a
+// diagonal's index (128 + 64 entries, plain indices).
+size_t blob_tables(std::vector<uint8_t>& blob, uint32_t L, uint32_t fixed_mask, const std::vector<int>& tgt_local,
+                   bool diagonal) {
+  const uint32_t free_mask = ((1u << L) - 1u) & ~fixed_mask;
+  // Swizzled positions (tc_swz): XOR-linear, so the kernel combines
+  // entries with XOR.
+  std::vector<uint32_t> t(64 + 128, 0);
+  for (uint32_t x = 0; x < 64; ++x) t[x] = tc_swz(spread_bits(x, free_mask)) * 8;
+  for (uint32_t x = 0; x < 128; ++x) t[64 + x] = tc_swz(spread_bits(x << 6, free_mask)) * 8;
+  if (!diagonal) {
+    for (uint32_t c = 0; c < 64; ++c) {
+      uint32_t o = 0;
+      for (size_t j = 0; j < tgt_local.size(); ++j)
+        if ((c >> j) & 1) o |= 1u << tgt_local[j];
+      t.push_back(c < (1u << tgt_local.size()) ? tc_swz(o) * 8 : 0);
+    }
+  } else {
+    for (uint32_t part = 0; part < 2; ++part)
+      for (uint32_t x = 0; x < (part ? 64u : 128u); ++x) {
+        const uint32_t e = part ? (x << 7) : x;
+        uint32_t idx = 0;
+        for (size_t j = 0; j < tgt_local.size(); ++j)
+          if (tgt_local[j] >= 0 && ((e >> tgt_local[j]) & 1)) idx |= 1u << j;
+        t.push_back(idx);
+      }
+  }
+  return blob_put(blob, t);
+}
+
+// Lower a pass for the tensor-core kernel: every gate's data and tables go
+// into the pass blob, which the kernel keeps in shared memory.
+LoweredPass lower_tensor_pass(const Target& s, const PlannedPass& p, const StageConfig& cfg, StageUpload& up) {
+  LoweredPass lp;
+  TileGeom& geo = lp.geo;
+  geo.L = int(p.tile_bits.size());
+  geo.B = int(cfg.low_bits);
+  geo.num_tiles = uint64_t(1) << (s.n - uint32_t(geo.L));
+  for (size_t j = 0; j < p.tile_bits.size(); ++j) geo.tile_bits[j] = uint8_t(p.tile_bits[j]);
+  std::vector<int> local(s.n, -1);
+  for (size_t j = 0; j < p.tile_bits.size(); ++j) local[p.tile_bits[j]] = int(j);
+  const uint32_t L = uint32_t(geo.L);
+  lp.gate_offset = up.gates.size();
+  blob_align(up.tc);
+  geo.tc_offset = up.tc.size();
+  std::vector<uint8_t> blob;
+  for (const HOp& src : p.ops) {
+    HOp op = src;
+    TileGate g{};
+    // Global controls are tile predicates; local controls of a dense gate
+    // are folded into its matrix (the gate then acts on them too).
+    std::vector<std::pair<uint32_t, bool>> local_controls;
+    for (auto& c : op.controls) {
+      const uint32_t ph = s.layout[c.first];
+      if (local[ph] >= 0) {
+        local_controls.push_back(c);
+      } else {
+        g.gcm |= uint64_t(1) << ph;
+        if (c.second) g.gcv |= uint64_t(1) << ph;
+      }
+    }
+    if (!op.diagonal && !local_controls.empty()) {
+      size_t state = 0;
+      std::vector<uint32_t> qs;
+      for (size_t i = 0; i < local_controls.size(); ++i) {
+        state |= size_t(local_controls[i].second) << i;
+        qs.push_back(local_controls[i].first);
+      }
+      qs.insert(qs.end(), op.targets.begin(), op.targets.end());
+      op.matrix = op.matrix.controlled(local_controls.size(), state);
+      op.targets = qs;
+      local_controls.clear();
+    }
+    uint32_t fixed = 0;
+    for (auto& c : local_controls) {
+      const int l = local[s.layout[c.first]];
+      fixed |= 1u << l;
+      if (c.second) g.lcv |= 1u << l;
+    }
+    const size_t k = op.targets.size();
+    g.k = uint8_t(k);
+    std::vector<int> tl;
+    for (uint32_t q : op.targets) tl.push_back(local[s.layout[q]]);
+    if (op.diagonal) {
+      if (k > QVDG_MAX_DIAGONAL_QUBITS)
+        throw Error(QVDG_ERR_UNSUPPORTED, "diagonal gates on more than 10 qubits are not supported");
+      const std::vector<C> d = op.matrix.diagonal_entries();
+      size_t odd = 0, count = 0;
+      for (size_t i = 0; i < d.size(); ++i)
+        if (!(d[i].re == 1.0 && d[i].im == 0.0)) {
+          odd = i;
+          ++count;
+        }
+      for (size_t j = 0; j < k; ++j) g.tgt[j] = tl[j] >= 0 ? uint8_t(tl[j]) : uint8_t(0x80 | s.layout[op.targets[j]]);
+      if (count <= 1) {
+        // One phase on the elements whose targets read `odd` (CZ, CP, S, T, ...).
+        g.kind = 3;
+        for (size_t j = 0; j < k; ++j) {
+          const bool one = (odd >> j) & 1;
+          if (tl[j] >= 0) {
+            fixed |= 1u << tl[j];
+            if (one) g.lcv |= 1u << tl[j];
+          } else {
+            const uint32_t ph = s.layout[op.targets[j]];
+            g.gcm |= uint64_t(1) << ph;
+            if (one) g.gcv |= uint64_t(1) << ph;
+          }
+        }
+        const C ph = count ? d[odd] : C{1.0, 0.0};
+        g.absorb = (ph.re == -1.0 && ph.im == 0.0) ? 1 : 0;
+        g.mat = uint32_t(blob_put_c64(blob, {ph}));
+        g.tab = uint32_t(blob_tables(blob, L, fixed, {}, false));
+      } else {
+        g.kind = 1;
+        g.mat = uint32_t(blob_put_c64(blob, d));
+        g.tab = uint32_t(blob_tables(blob, L, fixed, tl, true));
+      }
+    } else {
+      if (k > QVDG_MAX_GATE_QUBITS)
+        throw Error(QVDG_ERR_UNSUPPORTED, "dense gates on more than 6 qubits are not supported");
+      for (size_t j = 0; j < k; ++j) {
+        if (tl[j] < 0) throw Error(QVDG_ERR_INVALID, "internal: dense stage gate with a global target");
+        g.tgt[j] = uint8_t(tl[j]);
+        fixed |= 1u << tl[j];
+      }
+      if (k >= 3 && k + 7 <= L) {
+        g.kind = 2;
+        blob_align(blob);
+        g.mat = uint32_t(blob.size());
+        append_tc_gate(op.matrix, blob);
+      } else {
+        g.kind = 0;
+        g.mat = uint32_t(blob_put_c64(blob, op.matrix.a));
+      }
+      g.tab = uint32_t(blob_tables(blob, L, fixed, tl, false));
+    }
+    g.nfixed = uint8_t(__builtin_popcount(fixed));
+    g.lcm = fixed * 8;  // byte units, like the tables
+    g.lcv *= 8;
+    up.gates.push_back(g);
+  }
+  // Runs of one-phase gates right before a tensor-core gate are applied in
+  // that gate's gather; a run at the end of the pass in the final store.
+  if (getenv("QVDG_ABSORB") && getenv("QVDG_ABSORB")[0] == '1') {
+    // kind 3: absorb bit 0 = the phase is -1, bit 1 = applied by a consumer.
+    const size_t first = lp.gate_offset, last = up.gates.size();
+    size_t run = 0;
+    auto mark = [&](size_t end) {
+      for (size_t j = end - run; j < end; ++j) up.gates[j].absorb |= 2;
+    };
+    for (size_t i = first; i < last; ++i) {
+      TileGate& g = up.gates[i];
+      if (g.kind == 3) {
+        ++run;
+      } else if (g.kind == 2 && g.gcm == 0) {  // runs on every tile, so it can carry the run
+        mark(i);
+        g.absorb = uint8_t(run);
+        run = 0;
+      } else {
+        run = 0;
+      }
+    }
+    mark(last);
+    lp.geo.tail_absorb = int(run);
+  }
+  blob_align(blob);
+  up.tc.insert(up.tc.end(), blob.begin(), blob.end());
+  geo.num_gates = int(up.gates.size() - lp.gate_offset);
+  geo.tc_bytes = uint32_t(blob.size());
+  geo.tensor = 1;
+  if (geo.L - geo.B > 10 || geo.L > int(kTcTileBits) || geo.tc_bytes > kTcBlobBytes ||
+      geo.num_gates > kTcMaxGates)
+    throw Error(QVDG_ERR_INVALID, "internal: tensor-core pass does not fit shared memory");
+  return lp;
+}
+
+// Whether the tensor-core kernel can run every gate of a pass: dense gates
+// (with local controls folded in) have at most 2 qubits or fit the
+// tensor-core shape (3 <= k <= L - 7).
+bool tensor_pass_ok(const Target& s, const PlannedPass& p) {
+  const uint32_t L = uint32_t(p.tile_bits.size());
+  if (L < 10 || L > kTcTileBits || p.ops.size() > size_t(kTcMaxGates)) return false;
+  for (const HOp& op : p.ops) {
+    if (op.diagonal) continue;
+    size_t k = op.targets.size();
+    for (auto& c : op.controls)
+      if (std::find(p.tile_bits.begin(), p.tile_bits.end(), s.layout[c.first]) != p.tile_bits.end()) ++k;
+    if (k >= 3 && (k + 7 > L || k > 6)) return false;
+  }
+  return true;
+}
+
 LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig& cfg, StageUpload& up) {
+  if (p.staged && cfg.tensor && cfg.low_bits >= 1 && tensor_pass_ok(s, p)) return lower_tensor_pass(s, p, cfg, up);
   LoweredPass lp;
   lp.staged = p.staged;
   if (!p.staged) {
@@ -209,11 +434,7 @@ LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig&
         g.tgt[j] = uint8_t(l);
         fixed.push_back(uint8_t(l));
       }
-      if (cfg.tensor && tensor_eligible(op, uint32_t(geo.L))) {
-        g.kind = 2;
-        g.mat = uint32_t(up.tc.size() - geo.tc_offset);
-        append_tc_gate(op.matrix, up.tc);
-      } else if (op.targets.size() >= 5) {
+      if (op.targets.size() >= 5) {
         // transposed for the row-parallel kernel
         const size_t D = op.matrix.dim;
         std::vector<C> t(D * D);
@@ -230,10 +451,6 @@ LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig&
     up.gates.push_back(g);
   }
   geo.num_gates = int(up.gates.size() - lp.gate_offset);
-  geo.tc_bytes = uint32_t(up.tc.size() - geo.tc_offset);
-  geo.tensor = geo.tc_bytes > 0 ? 1u : 0u;
-  if (geo.tensor && (geo.L - geo.B > 10 || tc_smem_bytes(geo) > size_t(227 * 1024)))
-    throw Error(QVDG_ERR_INVALID, "internal: tensor-core pass does not fit shared memory");
   return lp;
 }
 

@@ -16,15 +16,18 @@ struct PlannedPass;
 constexpr size_t kMaxStageGates = 256;
 
 // One gate of a stage's program, on tile-local bit positions.
+// Gate kinds: 0 dense on CUDA cores, 1 diagonal, 2 dense on tensor cores,
+// 3 one phase on the elements whose target and control bits hold.
 struct TileGate {
-  uint8_t kind;    // 0 dense, 1 diagonal
+  uint8_t kind;
   uint8_t k;       // targets
   uint8_t nfixed;  // entries of `fixed`
-  uint8_t pad;
+  uint8_t absorb;  // tensor passes: one-phase gates just before this one applied in its gather (kind 2)
+                   // or, for kind 3, 1 when the phase is exactly -1
   uint32_t lcm, lcv;  // local control bits (tile-local positions) and their values
   uint64_t gcm, gcv;  // global control bits (physical positions) and their values
-  uint32_t mat;       // complex-element offset of the matrix / diagonal
-  uint32_t pad2;
+  uint32_t mat;       // complex-element offset of the matrix / diagonal (tensor passes: byte offset in the pass blob)
+  uint32_t tab;       // tensor passes: byte offset of the gate's index tables in the pass blob
   uint8_t tgt[16];    // matrix bit j -> tile-local bit; diagonal global targets: 0x80 | physical bit
   uint8_t fixed[24];  // dense: sorted local targets and controls; diagonal: sorted local controls
 };
@@ -36,7 +39,7 @@ struct TileGeom {
   int32_t num_gates;
   uint32_t tc_bytes;   // bytes of those matrices (kept in shared memory)
   uint32_t tensor;     // 1: launch the tensor-core kernel
-  int32_t pad;
+  int32_t tail_absorb;  // tensor passes: trailing one-phase gates applied in the final store
   uint8_t tile_bits[48];  // ascending physical bits of the tile
 };
 
@@ -75,7 +78,22 @@ size_t tc_smem_bytes(const TileGeom& geo);
 
 // Bytes of one tensor-core gate's matrices (bf16 hi and lo, 2^(k+1) square).
 inline size_t tc_gate_bytes(size_t k) { return size_t(4) << (2 * (k + 1)); }
-// Shared memory the tensor-core kernel may spend on a pass's gate matrices.
-inline size_t tc_budget(uint32_t L) { return size_t(220 * 1024) - (size_t(16) << L); }
+// The tensor-core kernel's tile: 12 local qubits (32 KiB of complex64), two
+// CTAs per SM; each CTA keeps its pass's gate data (at most kTcBlobBytes)
+// and descriptors (at most kTcMaxGates) in shared memory.
+constexpr uint32_t kTcTileBits = 12;
+constexpr size_t kTcBlobBytes = 40 * 1024;
+constexpr int kTcMaxGates = 64;
+inline size_t tc_budget(uint32_t) { return kTcBlobBytes; }
+
+// The tensor-core kernel stores tile element e at position e ^ tc_swizzle(e)
+// in shared memory: the low 4 index bits are XORed with bits 4-7, 8-11 and
+// 12-15, so warps whose lanes step by 16 or 256 elements (group bases of
+// gates on low tile bits) spread over all banks. The map is XOR-linear and
+// an involution.
+__host__ __device__ inline uint32_t tc_swizzle(uint32_t e) { return ((e >> 4) ^ (e >> 8) ^ (e >> 12)) & 15u; }
+__host__ __device__ inline uint32_t tc_swz(uint32_t e) { return e ^ tc_swizzle(e); }
+// The same on byte offsets (element index * 8).
+__host__ __device__ inline uint32_t tc_swz_bytes(uint32_t b) { return tc_swz(b >> 3) << 3; }
 
 }  // namespace qvdg

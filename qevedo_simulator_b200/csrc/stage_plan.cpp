@@ -47,10 +47,21 @@ bool tensor_eligible(const HOp& op, uint32_t L) {
   return !op.diagonal && op.controls.empty() && k >= 3 && k + 7 <= L && k <= 6;
 }
 
+// Upper bound of the shared-memory bytes one op takes in a tensor pass's
+// blob (its matrix or diagonal, and its index tables).
+static size_t tensor_blob_bytes(const HOp& op, uint32_t L) {
+  // tables: 768 bytes of enumeration spreads, plus 256 of member offsets
+  // (dense) or 768 of diagonal index parts; 32 bytes of alignment.
+  if (op.diagonal) return (size_t(8) << op.targets.size()) + 768 + 768 + 32;
+  const size_t k = op.targets.size() + op.controls.size();
+  const size_t data = (k >= 3 && k + 7 <= L) ? tc_gate_bytes(k) : (size_t(8) << (2 * k));
+  return data + 768 + 256 + 32;
+}
+
 StageConfig stage_config(const Target& s, uint32_t requested, bool tensor) {
   StageConfig c{};
   c.tensor = tensor && s.bits == 32;
-  const uint32_t lmax = s.bits == 32 ? 13 : 12;  // 64 KiB tiles
+  const uint32_t lmax = c.tensor ? kTcTileBits : (s.bits == 32 ? 13 : 12);  // 32-64 KiB tiles
   uint32_t L = requested ? std::min<uint32_t>(requested, lmax) : lmax;
   if (!requested && !c.tensor) {
     // Keep at least two tiles per SM on small states.
@@ -131,8 +142,9 @@ std::vector<PlannedPass> plan_stages(const std::vector<HOp>& ops, const std::vec
     p.tile_bits = bits;
     size_t tc_bytes = 0;
     for (HOp& op : fused) {
-      const size_t b = cfg.tensor && tensor_eligible(op, L) ? tc_gate_bytes(op.targets.size()) : 0;
-      if (!p.ops.empty() && (p.ops.size() >= kMaxStageGates || (b > 0 && tc_bytes + b > budget))) {
+      const size_t b = cfg.tensor ? tensor_blob_bytes(op, L) : 0;
+      const size_t max_gates = cfg.tensor ? size_t(kTcMaxGates) : kMaxStageGates;
+      if (!p.ops.empty() && (p.ops.size() >= max_gates || (b > 0 && tc_bytes + b > budget))) {
         passes.push_back(std::move(p));
         p = PlannedPass();
         p.tile_bits = bits;

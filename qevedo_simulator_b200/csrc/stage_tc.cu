@@ -37,8 +37,8 @@ namespace qvdg {
 
 namespace {
 
-constexpr int kTcThreads = 128;
-constexpr uint32_t kTmemCols = 128;  // 2^(L+1) fp32 columns / 128 lanes for L = 13
+constexpr int kTcThreads = 256;
+constexpr uint32_t kTmemCols = 64;  // 2^(L+1) fp32 columns / 128 lanes for L = 12
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -70,14 +70,16 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
+// Waits (suspended in hardware, up to about a millisecond per call) for the
+// barrier phase to complete; returns whether it did.
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase) {
   uint32_t done;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}\n"
       : "=r"(done)
-      : "r"(bar), "r"(phase)
+      : "r"(bar), "r"(phase), "r"(1000000u)
       : "memory");
   return done != 0;
 }
@@ -93,31 +95,77 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// A 16-byte global load issued where it is written (the compiler may not
+// sink it to its first use, so it overlaps the work in between).
+__device__ __forceinline__ float4 ld_early(const float2* p) {
+  float4 v;
+  asm volatile("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Pack 8 floats' bf16 high parts and low parts into two 16-byte vectors.
+// Pack 8 floats' bf16 high parts and low parts into two 16-byte vectors:
+// hi = bf16(x) (round to nearest), lo = bf16(x - hi) with x - hi exact in
+// fp32, so hi + lo keeps about 17 significant bits of x.
 __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
   uint32_t h[4], l[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * i]);
-    const __nv_bfloat16 h1 = __float2bfloat16_rn(x[2 * i + 1]);
-    const __nv_bfloat16 l0 = __float2bfloat16_rn(x[2 * i] - __bfloat162float(h0));
-    const __nv_bfloat16 l1 = __float2bfloat16_rn(x[2 * i + 1] - __bfloat162float(h1));
-    h[i] = uint32_t(__bfloat16_as_ushort(h0)) | (uint32_t(__bfloat16_as_ushort(h1)) << 16);
-    l[i] = uint32_t(__bfloat16_as_ushort(l0)) | (uint32_t(__bfloat16_as_ushort(l1)) << 16);
+    const __nv_bfloat162 hp = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+    h[i] = *reinterpret_cast<const uint32_t*>(&hp);
+    const float h0 = __uint_as_float(h[i] << 16), h1 = __uint_as_float(h[i] & 0xffff0000u);
+    const __nv_bfloat162 lp = __floats2bfloat162_rn(x[2 * i] - h0, x[2 * i + 1] - h1);
+    l[i] = *reinterpret_cast<const uint32_t*>(&lp);
   }
   hi = make_uint4(h[0], h[1], h[2], h[3]);
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// Apply the tile-active one-phase gates sg[a0, a1) to n elements with tile
+// indices e[] (values re[], im[]): a phase of -1 toggles a sign bit, any
+// other phase is one complex multiply.
+template <int N>
+__device__ __forceinline__ void apply_phases(const TileGate* sg, int a0, int a1, uint64_t base,
+                                             const unsigned char* blob, const uint32_t* e, float* re, float* im) {
+  uint32_t sign = 0;
+  for (int a = a0; a < a1; ++a) {
+    const TileGate& p = sg[a];
+    if ((base & p.gcm) != p.gcv) continue;
+    const uint32_t m = p.lcm, v = p.lcv;
+    if (p.absorb & 1) {
+#pragma unroll
+      for (int q = 0; q < N; ++q) sign ^= uint32_t((e[q] & m) == v) << q;
+    } else {
+      const float2 ph = *reinterpret_cast<const float2*>(blob + p.mat);
+#pragma unroll
+      for (int q = 0; q < N; ++q)
+        if ((e[q] & m) == v) {
+          const float r = fmaf(ph.x, re[q], -ph.y * im[q]);
+          im[q] = fmaf(ph.x, im[q], ph.y * re[q]);
+          re[q] = r;
+        }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < N; ++q)
+    if ((sign >> q) & 1) {
+      re[q] = -re[q];
+      im[q] = -im[q];
+    }
+}
+
 // Bounded wait: about two seconds of SM clocks.
 constexpr long long kWaitCycles = 4000000000LL;
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_stage_tc(float2* __restrict__ psi, const TileGeom geo,
+// Per-thread share of one tile in flight: 2^L amplitudes / (2 per 16-byte
+// access) / kTcThreads threads.
+constexpr int kTileVecs = (1 << kTcTileBits) / 2 / kTcThreads;
+
+__global__ void __launch_bounds__(kTcThreads, 2) k_stage_tc(float2* __restrict__ psi, const TileGeom geo,
                                                             const TileGate* __restrict__ gates,
                                                             const float2* __restrict__ mats,
                                                             const uint8_t* __restrict__ tc_blob,
@@ -128,15 +176,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_stage_tc(float2* __restrict__
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_run;
+  __shared__ TileGate sgates[kTcMaxGates];
   const int tid = threadIdx.x, warp = tid >> 5;
   const int L = geo.L, B = geo.B;
   const uint32_t n_el = 1u << L;
+  const uint32_t nvec = n_el / 2;  // 16-byte accesses per tile
   float2* tile = reinterpret_cast<float2*>(smem);
   unsigned char* a_hi = smem + (size_t(8) << L);
   unsigned char* a_lo = a_hi + (size_t(4) << L);
   unsigned char* gmem = a_lo + (size_t(4) << L);  // the pass's gate matrices (bf16 hi, lo)
 
   if (tid < 48) tile_bits[tid] = geo.tile_bits[tid];
+  for (int i = tid; i < geo.num_gates * int(sizeof(TileGate) / 8); i += kTcThreads)
+    reinterpret_cast<uint64_t*>(sgates)[i] = reinterpret_cast<const uint64_t*>(gates)[i];
   if (tid == 0) {
     abort_run = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)));
@@ -174,129 +226,232 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_stage_tc(float2* __restrict__
   const uint32_t barp = smem_addr(&bar);
   const uint32_t lowmask = (1u << B) - 1u;
   uint32_t phase = 0;
+  auto vec_addr = [&](uint64_t base, uint32_t e) -> uint64_t {
+    const uint32_t r = e >> B;
+    return base | hi_lo[r & 31] | hi_hi[r >> nlo] | (e & lowmask);
+  };
 
-  for (uint64_t t = blockIdx.x; t < geo.num_tiles && !abort_run; t += gridDim.x) {
+  // Tile loads run one tile ahead: the next tile's 16-byte vectors are in
+  // flight in registers while this tile is computed.
+  float4 pre[kTileVecs];
+  uint64_t t = blockIdx.x;
+  if (t < geo.num_tiles) {
     const uint64_t base = insert_zeros(t, tile_bits, L);
-    for (uint32_t e = tid * 2; e < n_el; e += kTcThreads * 2) {
-      const uint32_t r = e >> B;
-      const uint64_t a = base | hi_lo[r & 31] | hi_hi[r >> nlo] | (e & lowmask);
-      *reinterpret_cast<float4*>(&tile[e]) = *reinterpret_cast<const float4*>(&psi[a]);
+#pragma unroll
+    for (int i = 0; i < kTileVecs; ++i) {
+      const uint32_t v = uint32_t(i) * kTcThreads + tid;
+      if (v < nvec) pre[i] = ld_early(&psi[vec_addr(base, 2 * v)]);
+    }
+  }
+  for (; t < geo.num_tiles; t += gridDim.x) {
+#pragma unroll
+    for (int i = 0; i < kTileVecs; ++i) {
+      const uint32_t v = uint32_t(i) * kTcThreads + tid;
+      if (v < nvec) {
+        // elements 2v, 2v+1 land at the swizzled pair slot, swapped when the
+        // swizzle flips bit 0
+        const uint32_t hs = tc_swizzle(2 * v);
+        const float4 x = pre[i];
+        reinterpret_cast<float4*>(tile)[v ^ (hs >> 1)] = (hs & 1) ? make_float4(x.z, x.w, x.x, x.y) : x;
+      }
     }
     __syncthreads();
+    const uint64_t base = insert_zeros(t, tile_bits, L);
+    const uint64_t next = t + gridDim.x;
+    if (next < geo.num_tiles) {
+      const uint64_t nbase = insert_zeros(next, tile_bits, L);
+#pragma unroll
+      for (int i = 0; i < kTileVecs; ++i) {
+        const uint32_t v = uint32_t(i) * kTcThreads + tid;
+        if (v < nvec) pre[i] = ld_early(&psi[vec_addr(nbase, 2 * v)]);
+      }
+    }
     for (int gi = 0; gi < geo.num_gates; ++gi) {
-      const TileGate& g = gates[gi];
-      if ((base & g.gcm) != g.gcv) continue;  // global controls: the same for the whole tile
-      if (g.kind == 1) {
-        tile_diag<float>(tile, L, g, mats + g.mat, base);
-      } else if (g.kind == 0) {
-        switch (g.k) {
-          case 1: tile_dense<float, 1>(tile, L, g, mats + g.mat); break;
-          case 2: tile_dense<float, 2>(tile, L, g, mats + g.mat); break;
-          case 3: tile_dense<float, 3>(tile, L, g, mats + g.mat); break;
-          case 4: tile_dense<float, 4>(tile, L, g, mats + g.mat); break;
-          case 5: tile_dense_rows<float, 5>(tile, L, g, mats + g.mat); break;
-          default: tile_dense_rows<float, 6>(tile, L, g, mats + g.mat); break;
+      // Gate scalars (uniform across the CTA); tables and data are in the
+      // shared-memory blob.
+      const TileGate* gp = sgates + gi;
+      if (gp->kind == 3 && (gp->absorb & 2)) continue;  // applied by the next gather or the final store
+      const uint64_t gcm = gp->gcm, gcv = gp->gcv;
+      if ((base & gcm) != gcv) continue;  // global predicate: the same for the whole tile
+      const int kind = gp->kind, k = gp->k;
+      const uint32_t lcv = tc_swz_bytes(gp->lcv);  // swizzled byte units
+      const uint32_t count = 1u << (L - gp->nfixed);
+      const unsigned char* data = gmem + gp->mat;
+      const uint32_t* ebl = reinterpret_cast<const uint32_t*>(gmem + gp->tab);  // byte offsets
+      const uint32_t* ebh = ebl + 64;
+      const uint32_t* aux = ebl + 192;  // member byte offsets, or diagonal index parts
+      unsigned char* tb = reinterpret_cast<unsigned char*>(tile);
+      if (kind == 3) {
+        const float2 ph = *reinterpret_cast<const float2*>(data);
+        for (uint32_t i = tid; i < count; i += kTcThreads) {
+          float2* p = reinterpret_cast<float2*>(tb + (ebl[i & 63] ^ ebh[i >> 6] ^ lcv));
+          const float2 x = *p;
+          *p = make_float2(fmaf(ph.x, x.x, -ph.y * x.y), fmaf(ph.x, x.y, ph.y * x.x));
+        }
+      } else if (kind == 1) {
+        uint32_t dglob = 0;
+        for (int j = 0; j < k; ++j) {
+          const uint32_t tj = gp->tgt[j];
+          if (tj & 0x80) dglob |= uint32_t((base >> (tj & 0x7f)) & 1) << j;
+        }
+        const float2* d = reinterpret_cast<const float2*>(data);
+        for (uint32_t i = tid; i < count; i += kTcThreads) {
+          const uint32_t eb = ebl[i & 63] ^ ebh[i >> 6] ^ lcv;
+          const uint32_t e = tc_swz(eb >> 3);  // logical index for the diagonal
+          const float2 f = d[aux[e & 127] | aux[128 + (e >> 7)] | dglob];
+          float2* p = reinterpret_cast<float2*>(tb + eb);
+          const float2 x = *p;
+          *p = make_float2(fmaf(f.x, x.x, -f.y * x.y), fmaf(f.x, x.y, f.y * x.x));
+        }
+      } else if (kind == 0) {
+        const float2* m = reinterpret_cast<const float2*>(data);
+        if (k == 1) {
+          const float2 m00 = m[0], m01 = m[1], m10 = m[2], m11 = m[3];
+          const uint32_t o1 = aux[1];
+          for (uint32_t i = tid; i < count; i += kTcThreads) {
+            const uint32_t b = ebl[i & 63] ^ ebh[i >> 6] ^ lcv;
+            float2* p0 = reinterpret_cast<float2*>(tb + b);
+            float2* p1 = reinterpret_cast<float2*>(tb + (b ^ o1));
+            const float2 x0 = *p0, x1 = *p1;
+            float2 y0 = make_float2(0.f, 0.f), y1 = make_float2(0.f, 0.f);
+            cmac<float>(y0, m00, x0);
+            cmac<float>(y0, m01, x1);
+            cmac<float>(y1, m10, x0);
+            cmac<float>(y1, m11, x1);
+            *p0 = y0;
+            *p1 = y1;
+          }
+        } else {
+          // k = 2 (wider gates go to the tensor cores)
+          for (uint32_t i = tid; i < count; i += kTcThreads) {
+            const uint32_t b = ebl[i & 63] ^ ebh[i >> 6] ^ lcv;
+            float2 x[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) x[h] = *reinterpret_cast<const float2*>(tb + (b ^ aux[h]));
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              float2 y = make_float2(0.f, 0.f);
+#pragma unroll
+              for (int c = 0; c < 4; ++c) cmac<float>(y, m[r * 4 + c], x[c]);
+              *reinterpret_cast<float2*>(tb + (b ^ aux[r])) = y;
+            }
+          }
         }
       } else {
         // ---- dense gate on the tensor cores
-        const int k = g.k;
         const uint32_t half = 1u << k, kd = 2u << k;
-        const uint32_t sbo = kd * 16;                    // bytes between 8-row core groups
-        const uint32_t block_bytes = 128u * kd * 2u;     // one 128-group block of A (bf16)
-        const uint32_t nblocks = 1u << (L - k - 7);
-        uint8_t tg[8];
-        for (int j = 0; j < k; ++j) tg[j] = g.tgt[j];
-        // Gather: this thread's row in every block.
-        for (uint32_t b = 0; b < nblocks; ++b) {
-          const uint32_t eb = insert_zeros32(b * 128u + tid, g.fixed, k);
-          const uint32_t row = b * block_bytes + (tid >> 3) * sbo + (tid & 7) * 16;
-          for (uint32_t c0 = 0; c0 < half; c0 += 8) {
-            float re[8], im[8];
+        const uint32_t sbo = kd * 16;                 // bytes between 8-row core groups
+        const uint32_t block_bytes = 128u * kd * 2u;  // one 128-group block of A (bf16)
+        const uint32_t groups = count, nblocks = groups >> 7;
+        // Gather: unit = (group, 8 consecutive members); consecutive
+        // threads take consecutive groups.
+        const uint32_t units = groups * (half / 8);
+        const int absorb = gp->absorb;
+#pragma unroll 2
+        for (uint32_t u = tid; u < units; u += kTcThreads) {
+          const uint32_t grp = u & (groups - 1), c0 = (u >> (L - k)) * 8;
+          const uint32_t eb = ebl[grp & 63] ^ ebh[grp >> 6];
+          const uint4 o0 = *reinterpret_cast<const uint4*>(aux + c0);
+          const uint4 o1 = *reinterpret_cast<const uint4*>(aux + c0 + 4);
+          uint32_t e[8] = {eb ^ o0.x, eb ^ o0.y, eb ^ o0.z, eb ^ o0.w, eb ^ o1.x, eb ^ o1.y, eb ^ o1.z, eb ^ o1.w};
+          float re[8], im[8];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              uint32_t off = 0;
-              const uint32_t c = c0 + q;
-              for (int j = 0; j < k; ++j) off |= ((c >> j) & 1u) << tg[j];
-              const float2 v = tile[eb | off];
-              re[q] = v.x;
-              im[q] = v.y;
-            }
-            uint4 h, l;
-            split8(re, h, l);
-            *reinterpret_cast<uint4*>(a_hi + row + (c0 / 8) * 128) = h;
-            *reinterpret_cast<uint4*>(a_lo + row + (c0 / 8) * 128) = l;
-            split8(im, h, l);
-            *reinterpret_cast<uint4*>(a_hi + row + ((half + c0) / 8) * 128) = h;
-            *reinterpret_cast<uint4*>(a_lo + row + ((half + c0) / 8) * 128) = l;
+          for (int q = 0; q < 8; ++q) {
+            const float2 v = *reinterpret_cast<const float2*>(tb + e[q]);
+            re[q] = v.x;
+            im[q] = v.y;
           }
+          if (absorb) {
+            uint32_t le[8];  // logical byte offsets for the phase tests
+#pragma unroll
+            for (int q = 0; q < 8; ++q) le[q] = tc_swz_bytes(e[q]);
+            apply_phases<8>(sgates, gi - absorb, gi, base, gmem, le, re, im);
+          }
+          const uint32_t r = grp & 127;
+          const uint32_t row = (grp >> 7) * block_bytes + (r >> 3) * sbo + (r & 7) * 16;
+          uint4 h, l;
+          split8(re, h, l);
+          *reinterpret_cast<uint4*>(a_hi + row + (c0 / 8) * 128) = h;
+          *reinterpret_cast<uint4*>(a_lo + row + (c0 / 8) * 128) = l;
+          split8(im, h, l);
+          *reinterpret_cast<uint4*>(a_hi + row + ((half + c0) / 8) * 128) = h;
+          *reinterpret_cast<uint4*>(a_lo + row + ((half + c0) / 8) * 128) = l;
         }
         fence_async_shared();
         __syncthreads();
         if (tid == 0) {
           tc_fence_after();
           const uint32_t idesc = umma_idesc(kd);
-          const uint32_t g_hi = smem_addr(gmem + g.mat), g_lo = g_hi + kd * kd * 2;
-          const uint32_t ah = smem_addr(a_hi), al = smem_addr(a_lo);
+          const uint32_t g_hi = smem_addr(data), g_lo = g_hi + kd * kd * 2;
+          // Descriptors differ only in the start-address field (16-byte units).
+          const uint64_t dah = umma_desc(smem_addr(a_hi), 128, sbo), dal = umma_desc(smem_addr(a_lo), 128, sbo);
+          const uint64_t dbh = umma_desc(g_hi, 128, sbo), dbl = umma_desc(g_lo, 128, sbo);
+          const uint32_t ksteps = kd / 16;
           for (uint32_t b = 0; b < nblocks; ++b) {
             const uint32_t d = tmem + b * kd;
+            const uint64_t boff = (b * block_bytes) >> 4;
             uint32_t acc = 0;
+#pragma unroll
             for (int p = 0; p < 3; ++p) {
-              const uint32_t abase = (p == 2 ? al : ah) + b * block_bytes;
-              const uint32_t bbase = p == 1 ? g_lo : g_hi;
-              for (uint32_t s = 0; s < kd / 16; ++s) {
-                umma_bf16(d, umma_desc(abase + s * 256, 128, sbo), umma_desc(bbase + s * 256, 128, sbo), idesc, acc);
+              const uint64_t a0 = (p == 2 ? dal : dah) + boff, b0 = p == 1 ? dbl : dbh;
+              for (uint32_t s = 0; s < ksteps; ++s) {
+                umma_bf16(d, a0 + 16 * s, b0 + 16 * s, idesc, acc);
                 acc = 1;
               }
             }
           }
           umma_commit(barp);
-        }
-        // Bounded wait for the products.
-        const long long t0 = clock64();
-        bool ok = true;
-        while (!mbar_try_wait(barp, phase)) {
-          if (clock64() - t0 > kWaitCycles) {
-            ok = false;
-            break;
+          // Bounded wait for the products by this thread alone (suspended in
+          // hardware); the other warps wait at the barrier below.
+          const long long t0 = clock64();
+          while (!mbar_try_wait(barp, phase)) {
+            if (clock64() - t0 > kWaitCycles) {
+              atomicExch(status, 1);
+              abort_run = 1;
+              break;
+            }
           }
         }
         phase ^= 1u;
-        if (!ok) {
-          atomicExch(status, 1);
-          abort_run = 1;
-        }
         __syncthreads();
         if (abort_run) break;
         tc_fence_after();
-        // Scatter: row tid of each block back to its group in T.
-        for (uint32_t b = 0; b < nblocks; ++b) {
-          const uint32_t eb = insert_zeros32(b * 128u + tid, g.fixed, k);
-          const uint32_t lane_base = tmem + (uint32_t(warp * 32) << 16) + b * kd;
+        // Read-back: warp w reads TMEM lanes 32*(w%4).. of the columns of
+        // work unit w/4 + 2 j, a unit being 16 real and 16 imaginary
+        // columns of one block (or the 16 columns of one block for k = 3).
+        const uint32_t quarter = uint32_t(warp & 3), wg = uint32_t(warp >> 2);
+        const uint32_t chunks = half >= 16 ? half / 16 : 1;
+        const uint32_t nunits = nblocks * chunks;
+        for (uint32_t unit = wg; unit < nunits; unit += kTcThreads / 128) {
+          const uint32_t b = unit / chunks, c0 = (unit % chunks) * 16;
+          const uint32_t grp = b * 128u + quarter * 32u + uint32_t(tid & 31);
+          const uint32_t eb = ebl[grp & 63] ^ ebh[grp >> 6];
+          const uint32_t lane_base = tmem + ((quarter * 32u) << 16) + b * kd;
           if (half == 8) {
-            // 16 columns: 8 real parts then 8 imaginary parts.
             float v[16];
             tmem_ld16(lane_base, v);
+            const uint4 o0 = *reinterpret_cast<const uint4*>(aux);
+            const uint4 o1 = *reinterpret_cast<const uint4*>(aux + 4);
+            const uint32_t o[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
             tmem_wait_ld();
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              uint32_t off = 0;
-              for (int j = 0; j < k; ++j) off |= ((uint32_t(q) >> j) & 1u) << tg[j];
-              tile[eb | off] = make_float2(v[q], v[8 + q]);
-            }
-            continue;
-          }
-          for (uint32_t c0 = 0; c0 < half; c0 += 16) {
+            for (int q = 0; q < 8; ++q) *reinterpret_cast<float2*>(tb + (eb ^ o[q])) = make_float2(v[q], v[8 + q]);
+          } else {
             float re[16], im[16];
             tmem_ld16(lane_base + c0, re);
             tmem_ld16(lane_base + half + c0, im);
+            uint32_t o[16];
+#pragma unroll
+            for (int q = 0; q < 16; q += 4) {
+              const uint4 oo = *reinterpret_cast<const uint4*>(aux + c0 + q);
+              o[q] = oo.x;
+              o[q + 1] = oo.y;
+              o[q + 2] = oo.z;
+              o[q + 3] = oo.w;
+            }
             tmem_wait_ld();
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
-              uint32_t off = 0;
-              const uint32_t c = c0 + q;
-              for (int j = 0; j < k; ++j) off |= ((c >> j) & 1u) << tg[j];
-              tile[eb | off] = make_float2(re[q], im[q]);
-            }
+            for (int q = 0; q < 16; ++q) *reinterpret_cast<float2*>(tb + (eb ^ o[q])) = make_float2(re[q], im[q]);
           }
         }
         tc_fence_before();
@@ -304,10 +459,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_stage_tc(float2* __restrict__
       __syncthreads();
     }
     if (abort_run) break;
-    for (uint32_t e = tid * 2; e < n_el; e += kTcThreads * 2) {
-      const uint32_t r = e >> B;
-      const uint64_t a = base | hi_lo[r & 31] | hi_hi[r >> nlo] | (e & lowmask);
-      *reinterpret_cast<float4*>(&psi[a]) = *reinterpret_cast<const float4*>(&tile[e]);
+    // Store this tile (the next tile's loads are already in flight),
+    // applying the trailing one-phase gates.
+    const int tail0 = geo.num_gates - geo.tail_absorb;
+#pragma unroll
+    for (int i = 0; i < kTileVecs; ++i) {
+      const uint32_t v = uint32_t(i) * kTcThreads + tid;
+      if (v < nvec) {
+        const uint32_t hs = tc_swizzle(2 * v);
+        float4 x = reinterpret_cast<const float4*>(tile)[v ^ (hs >> 1)];
+        if (hs & 1) x = make_float4(x.z, x.w, x.x, x.y);
+        if (geo.tail_absorb) {
+          const uint32_t e[2] = {16 * v, 16 * v + 8};  // byte offsets
+          float re[2] = {x.x, x.z}, im[2] = {x.y, x.w};
+          apply_phases<2>(sgates, tail0, geo.num_gates, base, gmem, e, re, im);
+          x = make_float4(re[0], im[0], re[1], im[1]);
+        }
+        *reinterpret_cast<float4*>(&psi[vec_addr(base, 2 * v)]) = x;
+      }
     }
     __syncthreads();
   }
@@ -323,10 +492,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_stage_tc(float2* __restrict__
 
 size_t tc_smem_bytes(const TileGeom& geo) { return (size_t(16) << geo.L) + geo.tc_bytes; }
 
-// At least 116 KiB of dynamic shared memory: with more than half of the
-// SM's shared memory per CTA, one CTA (and one 128-column TMEM allocation)
-// is resident per SM.
-static size_t tc_launch_smem(const TileGeom& geo) { return std::max(tc_smem_bytes(geo), size_t(116 * 1024)); }
+// Registers limit the kernel to two CTAs per SM (256 threads x 128
+// registers each); two 64-column TMEM allocations always fit.
+static size_t tc_launch_smem(const TileGeom& geo) { return tc_smem_bytes(geo); }
 
 void launch_stage_tc(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev) {
   const size_t smem = tc_launch_smem(lp.geo);
@@ -335,7 +503,7 @@ void launch_stage_tc(StateImpl& s, const LoweredPass& lp, const DeviceUpload& de
     QVDG_CUDA(cudaFuncSetAttribute(k_stage_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     configured = smem;
   }
-  const uint64_t grid = std::min<uint64_t>(lp.geo.num_tiles, uint64_t(s.sms));
+  const uint64_t grid = std::min<uint64_t>(lp.geo.num_tiles, uint64_t(s.sms) * 2);
   k_stage_tc<<<unsigned(grid), kTcThreads, smem, s.stream>>>(static_cast<float2*>(s.amp), lp.geo,
                                                             dev.gates + lp.gate_offset,
                                                             static_cast<const float2*>(dev.mats), dev.tc, s.status);
