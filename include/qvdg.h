@@ -244,6 +244,35 @@ qvdg_status qvdg_set_device(int32_t device);
  * device. */
 qvdg_status qvdg_max_abs_diff(const qvdg_state* a, const qvdg_state* b, double* out);
 
+/* Per-qubit probabilities of a state vector the caller keeps in its own
+ * device memory, computed without allocating anything. No counterpart in
+ * the reference.
+ *
+ * Some callers cannot let this library call cudaMalloc: a program that has
+ * given nearly all of the GPU's memory to its state vector (a 34-qubit
+ * complex64 state alone takes 128 GiB of the 180 GB), or one whose device
+ * memory belongs to another allocator (a framework's caching pool), where
+ * an allocation from here would fail or take memory the pool counts on.
+ * This entry point uses a fixed scratch array of 147,744 bytes, defined
+ * in the library and held on every device that loads it until the process
+ * exits, and allocates no device or pinned host memory.
+ *
+ * `amplitudes`: 2^num_qubits interleaved complex numbers on the current
+ * device (complex64 for precision_bits 32, complex128 for 64), bit q of
+ * the index = qubit q. `stream`: a cudaStream_t (NULL = the default
+ * stream); the call blocks until the results are in host memory.
+ * Outputs: p1[q] = sum of |a_i|^2 over the indices with bit q set
+ * (num_qubits values), *total = sum of all |a_i|^2, both in double
+ * precision; P(q = 1) = p1[q] / *total.
+ *
+ * At most 35 qubits; larger states are refused (QVDG_ERR_UNSUPPORTED).
+ * The first call on a device looks up the scratch array's address on that
+ * device; make that first call before any stream capture. All calls share
+ * the one array, so calls that overlap on the GPU (from several threads or
+ * streams) race: order them, e.g. on one stream. */
+qvdg_status qvdg_bit_probabilities_noalloc(const void* amplitudes, uint32_t num_qubits, uint32_t precision_bits,
+                                           void* stream, double* p1, double* total);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,8 @@ _SIGNATURES = {
     "qvdg_set_pass_timing": (ct.c_int, [_P, ct.c_int32]),
     "qvdg_pass_times": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), ct.POINTER(ct.c_int32),
                                    ct.c_size_t, ct.POINTER(ct.c_size_t)]),
+    "qvdg_bit_probabilities_noalloc": (ct.c_int, [_P, ct.c_uint32, ct.c_uint32, _P, ct.POINTER(ct.c_double),
+                                                  ct.POINTER(ct.c_double)]),
 }
 
 _lib = None
@@ -91,6 +93,18 @@ def check(status: int):
         if status == 2:
             raise MemoryError(msg)
         raise QvdgError(status, msg)
+
+
+def bit_probabilities_noalloc(pointer: int, num_qubits: int, precision_bits: int, stream: int = 0):
+    """(p1, total) of a state vector in the caller's own device memory at
+    `pointer`, computed with the library's fixed scratch array and no
+    allocation (for callers whose device memory is all spoken for). p1[q] is
+    the unnormalised weight of bit q = 1; calls that overlap on the GPU race."""
+    p1 = np.zeros(max(int(num_qubits), 1), dtype=np.float64)
+    total = ct.c_double()
+    check(lib().qvdg_bit_probabilities_noalloc(ct.c_void_p(pointer), int(num_qubits), int(precision_bits),
+                                               ct.c_void_p(stream), as_double_ptr(p1), ct.byref(total)))
+    return p1[:num_qubits], total.value
 
 
 def set_device(device: int):

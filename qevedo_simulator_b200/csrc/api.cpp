@@ -564,4 +564,15 @@ qvdg_status qvdg_max_abs_diff(const qvdg_state* a, const qvdg_state* b, double* 
   });
 }
 
+qvdg_status qvdg_bit_probabilities_noalloc(const void* amplitudes, uint32_t num_qubits, uint32_t precision_bits,
+                                           void* stream, double* p1, double* total) {
+  return guarded([&] {
+    require(amplitudes != nullptr, "null amplitudes");
+    require(p1 != nullptr && total != nullptr, "null output");
+    require(num_qubits >= 1, "num_qubits must be at least 1");
+    require(precision_bits == 32 || precision_bits == 64, "precision_bits must be 32 or 64");
+    bit_probabilities_noalloc(amplitudes, num_qubits, precision_bits, static_cast<cudaStream_t>(stream), p1, total);
+  });
+}
+
 }  // extern "C"

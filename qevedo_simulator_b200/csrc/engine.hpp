@@ -82,6 +82,10 @@ double norm_sqr(StateImpl& s);
 double probability_one(StateImpl& s, uint32_t physical_bit);
 // P(bit = 1) for every physical bit, and the total.
 void bit_probabilities(StateImpl& s, std::vector<double>& p1, double& total);
+// bit_probabilities over a caller's device buffer, with file-scope scratch
+// instead of an allocated workspace (qvdg_bit_probabilities_noalloc).
+void bit_probabilities_noalloc(const void* amplitudes, uint32_t num_qubits, uint32_t precision_bits,
+                               cudaStream_t stream, double* p1, double* total);
 void probabilities(StateImpl& s, double* out_host);
 // Bit-exact restatement of the reference sampler; outcomes are physical
 // indices in chunk order, then mapped to logical with the layout.

@@ -21,9 +21,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "engine.hpp"
+#include "qvdg.h"
 
 namespace qvdg {
 
@@ -583,6 +585,83 @@ void probabilities(StateImpl& s, double* out_host) {
 size_t sample_unordered(StateImpl& s, size_t shots, const double* uniforms_host, uint64_t* out_host) {
   return s.bits == 32 ? sample_t<float>(s, shots, uniforms_host, out_host)
                       : sample_t<double>(s, shots, uniforms_host, out_host);
+}
+
+
+// ---------------------------------------------------------------------------
+// Per-bit probabilities with no allocation (qvdg_bit_probabilities_noalloc).
+//
+// For callers that cannot allocate device memory: the k_bit_probs partials
+// and their column sums live in one file-scope device array instead of the
+// state's workspace. At most kNoAllocMaxBlocks blocks of k_bit_probs, each
+// writing kNoAllocMaxQubits + 1 doubles, plus one row of totals:
+// (512 + 1) * 36 doubles = 147,744 bytes, held on every device that loads
+// this library until the process exits. Every row the kernels read is
+// written earlier in the same call, so nothing needs clearing; calls that
+// overlap on the GPU share the array and race.
+constexpr uint32_t kNoAllocMaxQubits = 35;
+constexpr uint64_t kNoAllocMaxBlocks = 512;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_noalloc_scratch[(kNoAllocMaxBlocks + 1) * (kNoAllocMaxQubits + 1)];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+double* g_noalloc_address[kNoAllocMaxDevices] = {};
+
+// The device address of g_noalloc_scratch on `device` (the current device).
+// In host code g_noalloc_scratch only names the symbol; its address on a
+// device comes from cudaGetSymbolAddress, looked up once per device.
+double* noalloc_scratch(int device) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_address[device] == nullptr) {
+    void* p = nullptr;
+    QVDG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_address[device] = static_cast<double*>(p);
+  }
+  return g_noalloc_address[device];
+}
+
+template <typename T>
+void bit_probs_noalloc_t(const void* amplitudes, uint32_t n, cudaStream_t stream, double* p1, double* total) {
+  int device = 0;
+  QVDG_CUDA(cudaGetDevice(&device));
+  if (device < 0 || device >= kNoAllocMaxDevices)
+    throw Error(QVDG_ERR_UNSUPPORTED, "device index beyond the no-allocation limit of 64 devices");
+  double* d = noalloc_scratch(device);
+  int sms = 0;
+  QVDG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const uint64_t segments = ((uint64_t(1) << n) + 1023) >> 10;
+  uint64_t blocks = 1;
+  while (blocks * 2 <= segments && blocks * 2 <= uint64_t(sms) * 4 && blocks * 2 <= kNoAllocMaxBlocks) blocks *= 2;
+  while (segments / blocks > (uint64_t(1) << kMaxVarBits)) blocks *= 2;
+  if (blocks > kNoAllocMaxBlocks) throw Error(QVDG_ERR_UNSUPPORTED, "state too large for the no-allocation scratch");
+  const uint64_t per_block = segments / blocks;
+  int var_bits = 0;
+  while ((uint64_t(1) << var_bits) < per_block) ++var_bits;
+  const size_t width = size_t(n) + 1;
+  k_bit_probs<T><<<unsigned(blocks), kThreads, 0, stream>>>(static_cast<const cplx_t<T>*>(amplitudes), int(n),
+                                                            per_block, var_bits, d);
+  QVDG_LAUNCH_CHECK();
+  double* sum = d + size_t(blocks) * width;
+  k_sum_columns<<<blocks_for(width, 64), 64, 0, stream>>>(d, int(blocks), int(width), sum);
+  QVDG_LAUNCH_CHECK();
+  QVDG_CUDA(cudaMemcpyAsync(p1, sum, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  QVDG_CUDA(cudaMemcpyAsync(total, sum + n, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  QVDG_CUDA(cudaStreamSynchronize(stream));
+}
+
+}  // namespace
+
+void bit_probabilities_noalloc(const void* amplitudes, uint32_t num_qubits, uint32_t precision_bits,
+                               cudaStream_t stream, double* p1, double* total) {
+  if (num_qubits > kNoAllocMaxQubits)
+    throw Error(QVDG_ERR_UNSUPPORTED, "num_qubits " + std::to_string(num_qubits) +
+                                          " exceeds the no-allocation limit of 35 qubits");
+  if (precision_bits == 32)
+    bit_probs_noalloc_t<float>(amplitudes, num_qubits, stream, p1, total);
+  else
+    bit_probs_noalloc_t<double>(amplitudes, num_qubits, stream, p1, total);
 }
 
 }  // namespace qvdg
