@@ -225,6 +225,67 @@ qvdg_status qvdg_plan_info(const qvdg_plan* plan, qvdg_stats* stats);
  * half of apply_ops, src/simulator.rs:122-147). */
 qvdg_status qvdg_plan_execute(qvdg_state* state, const qvdg_plan* plan, qvdg_stats* stats);
 
+/* ---- Batched layered circuits ------------------------------------------
+ * Many small circuits of uneven width, each a stack of layers: one 2x2 gate
+ * on every qubit, then an optional entangler ladder on (q, q+1) for
+ * q = 0..n-2 in that order (the hardware-efficient ansatz: RY(theta) RZ(phi)
+ * per qubit and a CNOT ladder). Each circuit starts from |0...0> in complex64
+ * and yields <Z_q> = total - 2 P(q = 1) for every qubit, summed in double
+ * precision. The whole batch runs as ONE persistent kernel launch, captured
+ * once in a CUDA graph and replayed by every run. No reference counterpart:
+ * per circuit it equals apply_ops (src/simulator.rs:122-147) followed by
+ * probability_one for each qubit (src/measure.rs:43-65). */
+enum { QVDG_ENTANGLE_NONE = 0, QVDG_ENTANGLE_CX_LADDER = 1, QVDG_ENTANGLE_CZ_LADDER = 2 };
+#define QVDG_BATCH_MAX_QUBITS 24
+
+typedef struct {
+  uint32_t num_qubits;  /* 1..QVDG_BATCH_MAX_QUBITS */
+  uint32_t num_layers;
+  uint32_t entangler;   /* QVDG_ENTANGLE_* */
+  uint32_t reserved;    /* 0 */
+  /* num_layers * num_qubits 2x2 complex128 matrices, layer-major then qubit
+   * (matrix of layer l, qubit q at 8 * (l * num_qubits + q) doubles),
+   * row-major, (re, im) interleaved. */
+  const double* gates;
+} qvdg_layered_circuit;
+
+/* Tile shape of the batched launch: 0, 0 lets the autotuner time candidate
+ * shapes (tile qubits 12-14 x 128-512 threads) on a sample of the batch and
+ * keep the fastest. */
+typedef struct {
+  uint32_t tile_qubits;
+  uint32_t threads;
+} qvdg_batch_options;
+
+typedef struct {
+  uint32_t tile_qubits;  /* shape in use */
+  uint32_t threads;
+  uint32_t ctas;         /* persistent CTAs of the launch */
+  uint32_t candidates;   /* shapes the autotuner timed (0 if given) */
+  uint64_t circuits;
+  uint64_t outputs;      /* sum of num_qubits */
+  double tune_seconds;   /* host time spent autotuning */
+} qvdg_batch_summary;
+
+typedef struct qvdg_batch qvdg_batch;
+
+/* Upload a batch (gate matrices in complex64), pick its tile shape and
+ * capture its launch in a CUDA graph, on the current device. */
+qvdg_status qvdg_batch_create(const qvdg_layered_circuit* circuits, size_t count, const qvdg_batch_options* options,
+                              qvdg_batch** out);
+qvdg_status qvdg_batch_destroy(qvdg_batch* batch);
+/* Replace every gate matrix (same packing as at creation: circuit after
+ * circuit) without re-planning: the graph reads the same device buffer. */
+qvdg_status qvdg_batch_set_gates(qvdg_batch* batch, const double* gates, size_t num_matrices);
+/* Run the batch: `expect_z` receives info.outputs doubles, circuit after
+ * circuit, qubit 0 first; `seconds` (optional) the device time of the launch. */
+qvdg_status qvdg_batch_run(qvdg_batch* batch, double* expect_z, size_t count, double* seconds);
+qvdg_status qvdg_batch_info(const qvdg_batch* batch, qvdg_batch_summary* info);
+/* The autotuner's timings: tile qubits, threads and sample seconds of each
+ * candidate shape (at most `capacity`; `*count` receives the number). */
+qvdg_status qvdg_batch_tuning(const qvdg_batch* batch, uint32_t* tile_qubits, uint32_t* threads, double* seconds,
+                              size_t capacity, size_t* count);
+
 /* Record the device time of every pass of later gate runs on this state
  * (off by default; the reference's timing counters, src/simulator.rs:128-146). */
 qvdg_status qvdg_set_pass_timing(qvdg_state* state, int32_t enabled);

@@ -13,10 +13,10 @@ libqvdgpu.so behind the C ABI of include/qvdg.h; there is no CPU fallback.
 """
 
 from . import library
-from ._native import DeviceState, Plan, QvdgError, options, set_device
+from ._native import Batch, DeviceState, Plan, QvdgError, options, set_device
 from .circuit import Circuit, Gate, Op, gate_op
 from .simulator import RunResult, count_outcomes, run, statevector
 
-__all__ = ["Circuit", "Gate", "Op", "gate_op", "DeviceState", "Plan", "QvdgError", "options", "set_device", "RunResult", "run",
+__all__ = ["Batch", "Circuit", "Gate", "Op", "gate_op", "DeviceState", "Plan", "QvdgError", "options", "set_device", "RunResult", "run",
            "statevector", "count_outcomes", "library"]
 __version__ = "0.1.0"

@@ -43,6 +43,35 @@ class QvdgStats(ct.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class QvdgLayeredCircuit(ct.Structure):
+    _fields_ = [
+        ("num_qubits", ct.c_uint32),
+        ("num_layers", ct.c_uint32),
+        ("entangler", ct.c_uint32),
+        ("reserved", ct.c_uint32),
+        ("gates", ct.POINTER(ct.c_double)),
+    ]
+
+
+class QvdgBatchOptions(ct.Structure):
+    _fields_ = [("tile_qubits", ct.c_uint32), ("threads", ct.c_uint32)]
+
+
+class QvdgBatchSummary(ct.Structure):
+    _fields_ = [
+        ("tile_qubits", ct.c_uint32),
+        ("threads", ct.c_uint32),
+        ("ctas", ct.c_uint32),
+        ("candidates", ct.c_uint32),
+        ("circuits", ct.c_uint64),
+        ("outputs", ct.c_uint64),
+        ("tune_seconds", ct.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class PackedOps:
     """Ops laid out as a contiguous qvdg_op array; owns every buffer the
     structs point into, so it must outlive the call it is passed to."""

@@ -12,7 +12,8 @@ import os
 
 import numpy as np
 
-from ._abi import PackedOps, QvdgOp, QvdgOptions, QvdgStats, as_double_ptr, as_u64_ptr
+from ._abi import (PackedOps, QvdgBatchOptions, QvdgBatchSummary, QvdgLayeredCircuit, QvdgOp, QvdgOptions,
+                   QvdgStats, as_double_ptr, as_u64_ptr)
 
 LIBRARY = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libqvdgpu.so")
 
@@ -57,6 +58,14 @@ _SIGNATURES = {
     "qvdg_set_pass_timing": (ct.c_int, [_P, ct.c_int32]),
     "qvdg_pass_times": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), ct.POINTER(ct.c_int32),
                                    ct.c_size_t, ct.POINTER(ct.c_size_t)]),
+    "qvdg_batch_create": (ct.c_int, [ct.POINTER(QvdgLayeredCircuit), ct.c_size_t, ct.POINTER(QvdgBatchOptions),
+                                     ct.POINTER(_P)]),
+    "qvdg_batch_destroy": (ct.c_int, [_P]),
+    "qvdg_batch_set_gates": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.c_size_t]),
+    "qvdg_batch_run": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.c_size_t, ct.POINTER(ct.c_double)]),
+    "qvdg_batch_info": (ct.c_int, [_P, ct.POINTER(QvdgBatchSummary)]),
+    "qvdg_batch_tuning": (ct.c_int, [_P, ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_double),
+                                     ct.c_size_t, ct.POINTER(ct.c_size_t)]),
     "qvdg_bit_probabilities_noalloc": (ct.c_int, [_P, ct.c_uint32, ct.c_uint32, _P, ct.POINTER(ct.c_double),
                                                   ct.POINTER(ct.c_double)]),
 }
@@ -310,3 +319,87 @@ class Plan:
 
     def __exit__(self, *exc):
         self.close()
+
+
+ENTANGLERS = {"none": 0, "cx": 1, "cz": 2}
+
+
+class Batch:
+    """Many small layered circuits run to <Z_q> in one persistent,
+    graph-captured launch (qvdg_batch). Each circuit is (num_qubits,
+    gates, entangler): `gates` an array of shape (layers, num_qubits, 2, 2)
+    complex, one 2x2 gate per qubit per layer, each layer followed by the
+    entangler ladder ("cx", "cz" or "none") on (q, q+1), q = 0..n-2.
+    `tile_qubits`/`threads` of 0 let the autotuner choose the launch shape."""
+
+    def __init__(self, circuits, tile_qubits: int = 0, threads: int = 0):
+        self._h = ct.c_void_p()
+        arr = (QvdgLayeredCircuit * len(circuits))()
+        self._keep = []
+        self.widths = []
+        for i, (n, gates, ent) in enumerate(circuits):
+            g = np.ascontiguousarray(gates, dtype=np.complex128).reshape(-1)
+            layers = g.size // (4 * n) if n else 0
+            if g.size != layers * 4 * n:
+                raise ValueError("gates must have shape (layers, num_qubits, 2, 2)")
+            flat = g.view(np.float64)
+            self._keep.append(flat)
+            arr[i].num_qubits = int(n)
+            arr[i].num_layers = int(layers)
+            arr[i].entangler = ENTANGLERS[ent] if isinstance(ent, str) else int(ent)
+            arr[i].gates = as_double_ptr(flat)
+            self.widths.append(int(n))
+        opts = QvdgBatchOptions(int(tile_qubits), int(threads))
+        check(lib().qvdg_batch_create(arr, len(circuits), ct.byref(opts), ct.byref(self._h)))
+        self._keep = None
+        self.offsets = np.concatenate([[0], np.cumsum(self.widths)]).astype(np.int64)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().qvdg_batch_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run(self):
+        """(<Z> of every qubit of every circuit as one flat array, device seconds)."""
+        out = np.empty(max(int(self.offsets[-1]), 1), dtype=np.float64)
+        sec = ct.c_double()
+        check(lib().qvdg_batch_run(self._h, as_double_ptr(out), out.size, ct.byref(sec)))
+        return out[:int(self.offsets[-1])], sec.value
+
+    def split(self, flat) -> list:
+        """Per-circuit arrays from run()'s flat output."""
+        return [flat[self.offsets[i]:self.offsets[i + 1]] for i in range(len(self.widths))]
+
+    def set_gates(self, gates_list):
+        """New matrices for every circuit (same shapes as at creation)."""
+        flat = np.concatenate([np.ascontiguousarray(g, dtype=np.complex128).reshape(-1) for g in gates_list])
+        f = flat.view(np.float64)
+        check(lib().qvdg_batch_set_gates(self._h, as_double_ptr(f), flat.size // 4))
+
+    def info(self) -> dict:
+        s = QvdgBatchSummary()
+        check(lib().qvdg_batch_info(self._h, ct.byref(s)))
+        return s.as_dict()
+
+    def tuning(self):
+        """[(tile_qubits, threads, sample seconds)] of every autotuned shape."""
+        count = ct.c_size_t()
+        check(lib().qvdg_batch_tuning(self._h, None, None, None, 0, ct.byref(count)))
+        n = count.value
+        t = (ct.c_uint32 * max(n, 1))()
+        th = (ct.c_uint32 * max(n, 1))()
+        s = (ct.c_double * max(n, 1))()
+        check(lib().qvdg_batch_tuning(self._h, t, th, s, n, ct.byref(count)))
+        return [(t[i], th[i], s[i]) for i in range(n)]

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.hpp"
 #include "engine.hpp"
 #include "host.hpp"
 #include "qvdg.h"
@@ -572,6 +573,39 @@ qvdg_status qvdg_bit_probabilities_noalloc(const void* amplitudes, uint32_t num_
     require(num_qubits >= 1, "num_qubits must be at least 1");
     require(precision_bits == 32 || precision_bits == 64, "precision_bits must be 32 or 64");
     bit_probabilities_noalloc(amplitudes, num_qubits, precision_bits, static_cast<cudaStream_t>(stream), p1, total);
+  });
+}
+
+qvdg_status qvdg_batch_create(const qvdg_layered_circuit* circuits, size_t count, const qvdg_batch_options* options,
+                              qvdg_batch** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output");
+    *out = nullptr;
+    *out = batch_create(circuits, count, options);
+  });
+}
+
+qvdg_status qvdg_batch_destroy(qvdg_batch* batch) {
+  return guarded([&] { batch_destroy(batch); });
+}
+
+qvdg_status qvdg_batch_set_gates(qvdg_batch* batch, const double* gates, size_t num_matrices) {
+  return guarded([&] { batch_set_gates(batch, gates, num_matrices); });
+}
+
+qvdg_status qvdg_batch_run(qvdg_batch* batch, double* expect_z, size_t count, double* seconds) {
+  return guarded([&] { batch_run(batch, expect_z, count, seconds); });
+}
+
+qvdg_status qvdg_batch_info(const qvdg_batch* batch, qvdg_batch_summary* info) {
+  return guarded([&] { batch_info(batch, info); });
+}
+
+qvdg_status qvdg_batch_tuning(const qvdg_batch* batch, uint32_t* tile_qubits, uint32_t* threads, double* seconds,
+                              size_t capacity, size_t* count) {
+  return guarded([&] {
+    const size_t n = batch_tuning(batch, tile_qubits, threads, seconds, capacity);
+    if (count) *count = n;
   });
 }
 

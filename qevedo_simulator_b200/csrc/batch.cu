@@ -1,0 +1,365 @@
+// Batched layered circuits: thousands of small parameterised circuits of
+// uneven width, each layer one 2x2 gate per qubit followed by an optional
+// entangler ladder (CX or CZ on (q, q+1) for q = 0..n-2, in that order), run
+// to <Z_q> for every qubit of every circuit in ONE persistent launch that is
+// captured in a CUDA graph and replayed.
+//
+// There is no batched path in the reference: each circuit there is a run of
+// apply_ops (src/simulator.rs:122-147) on its own StateVector, followed by
+// probability_one per qubit (src/measure.rs:43-65). This file computes the
+// same quantities, <Z_q> = total - 2 * P(q = 1) with sums in f64, for a whole
+// batch at once.
+//
+// Work distribution: circuits are sorted by cost (largest first) and handed
+// out through an atomic counter, so one launch of (SMs x resident CTAs)
+// persistent CTAs keeps every SM busy until the batch drains.
+//
+// A circuit of n <= L qubits lives in shared memory for its whole run (L =
+// tile qubits, 12-14, chosen by the autotuner). A wider circuit lives in a
+// per-CTA slot in HBM and each layer is two tile passes: pass A over tiles of
+// the low L qubits, pass B over tiles of the high n-L qubits plus the low
+// r = 2L - n qubits (so rows of 2^r contiguous amplitudes stay coalesced).
+//
+// Gates are applied in registers, four qubits at a time: a thread loads the
+// 16 amplitudes of a subcube, applies the four 2x2 gates, then the part of
+// the entangler ladder that lands in those qubits (the ladder's gate into the
+// group's first qubit is controlled by a bit outside the subcube, which is
+// constant for it, so it becomes a conditional register swap; the ladder
+// gates inside the group are register renames). Ladder order is preserved:
+// groups run in ascending qubit order and a ladder gate only touches the
+// qubits of its own and the previous group.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "batch.hpp"
+
+namespace qvdg {
+
+namespace {
+
+constexpr int kVec = 16;  // >= max tile qubits + 1 (reduction vector)
+
+// Shared-memory position of tile element e: bits 4-7 are folded into bits
+// 0-3 so that every gate group's warp access touches 16 distinct 8-byte bank
+// pairs (two wavefronts per 32 amplitudes, the minimum).
+__device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 4) & 15u); }
+
+struct TileMap {
+  int kind;   // 0: local = global (in-shared circuits and pass A), 1: pass B
+  int r;      // pass B: low bits kept in the tile
+  int L;      // tile qubits
+  uint32_t tile;
+  __device__ __forceinline__ uint32_t global(uint32_t e) const {
+    if (kind == 0) return (tile << L) | e;
+    const uint32_t low = e & ((1u << r) - 1u);
+    return low | (tile << r) | ((e >> r) << L);
+  }
+};
+
+__device__ __forceinline__ float2 cfma2(float2 m0, float2 x0, float2 m1, float2 x1) {
+  float2 o;
+  o.x = fmaf(m0.x, x0.x, fmaf(-m0.y, x0.y, fmaf(m1.x, x1.x, -m1.y * x1.y)));
+  o.y = fmaf(m0.x, x0.y, fmaf(m0.y, x0.x, fmaf(m1.x, x1.y, m1.y * x1.x)));
+  return o;
+}
+
+// Apply the gates of local qubits q..q+G-1 (and their ladder part) to every
+// subcube of the 2^nb-element tile. `mats` holds 4 complex entries per local
+// qubit (m00, m01, m10, m11). `qglob` = global qubit of local bit q.
+template <int G>
+__device__ void apply_group(float2* __restrict__ tile, int nb, int q, const float2* __restrict__ mats,
+                            int entangler, int qglob, const TileMap& map) {
+  constexpr int S = 1 << G;
+  const uint32_t subcubes = 1u << (nb - G);
+  const uint32_t low_mask = (1u << q) - 1u;
+  for (uint32_t b = threadIdx.x; b < subcubes; b += blockDim.x) {
+    const uint32_t base = ((b & ~low_mask) << G) | (b & low_mask);
+    float2 a[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) a[j] = tile[swz(base | (uint32_t(j) << q))];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const float2 m00 = mats[4 * (q + g) + 0], m01 = mats[4 * (q + g) + 1];
+      const float2 m10 = mats[4 * (q + g) + 2], m11 = mats[4 * (q + g) + 3];
+#pragma unroll
+      for (int j = 0; j < S; ++j) {
+        if (j & (1 << g)) continue;
+        const float2 x0 = a[j], x1 = a[j | (1 << g)];
+        a[j] = cfma2(m00, x0, m01, x1);
+        a[j | (1 << g)] = cfma2(m10, x0, m11, x1);
+      }
+    }
+    if (entangler != QVDG_ENTANGLE_NONE) {
+      const bool ctrl = qglob > 0 && ((map.global(base) >> (qglob - 1)) & 1u);
+      if (entangler == QVDG_ENTANGLE_CX_LADDER) {
+        // cx(qglob-1, qglob): flip local bit 0 where the outside control is 1.
+#pragma unroll
+        for (int j = 0; j < S; j += 2) {
+          const float2 t0 = a[j], t1 = a[j + 1];
+          a[j] = ctrl ? t1 : t0;
+          a[j + 1] = ctrl ? t0 : t1;
+        }
+        // cx(q+g, q+g+1) inside the group, in ladder order.
+#pragma unroll
+        for (int g = 0; g + 1 < G; ++g) {
+#pragma unroll
+          for (int j = 0; j < S; ++j) {
+            if (!(j & (1 << g)) || (j & (2 << g))) continue;
+            const float2 t = a[j];
+            a[j] = a[j | (2 << g)];
+            a[j | (2 << g)] = t;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 1; j < S; j += 2)
+          if (ctrl) a[j] = make_float2(-a[j].x, -a[j].y);
+#pragma unroll
+        for (int g = 0; g + 1 < G; ++g) {
+#pragma unroll
+          for (int j = 0; j < S; ++j)
+            if ((j & (1 << g)) && (j & (2 << g))) a[j] = make_float2(-a[j].x, -a[j].y);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < S; ++j) tile[swz(base | (uint32_t(j) << q))] = a[j];
+  }
+}
+
+// Gates of local qubits [q0, q1) in groups of up to four, ascending.
+__device__ void apply_range(float2* tile, int nb, int q0, int q1, const float2* mats, int entangler, int qglob0,
+                            const TileMap& map) {
+  for (int q = q0; q < q1; q += 4) {
+    const int G = min(4, q1 - q);
+    const int qg = qglob0 + (q - q0);
+    if (G == 4)
+      apply_group<4>(tile, nb, q, mats, entangler, qg, map);
+    else if (G == 3)
+      apply_group<3>(tile, nb, q, mats, entangler, qg, map);
+    else if (G == 2)
+      apply_group<2>(tile, nb, q, mats, entangler, qg, map);
+    else
+      apply_group<1>(tile, nb, q, mats, entangler, qg, map);
+    __syncthreads();
+  }
+}
+
+// Deterministic block sum of kVec doubles per thread into out[0..kVec)
+// (valid in every thread after the call).
+__device__ void block_sum_vec(double (&v)[kVec], double* red /* [32 * kVec] */, double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+#pragma unroll
+  for (int i = 0; i < kVec; ++i) {
+    double x = v[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    v[i] = x;
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int i = 0; i < kVec; ++i) red[warp * kVec + i] = v[i];
+  __syncthreads();
+  if (threadIdx.x < kVec) {
+    double t = 0.0;
+    for (int w = 0; w < warps; ++w) t += red[w * kVec + threadIdx.x];
+    out[threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+// Adds the tile's probability sums to the CTA's per-qubit accumulators
+// acc[0] = total, acc[1 + q] = sum over global index bit q set. Thread i
+// visits elements i, i + T, i + 2T, ...: the local bits below log2(T) are
+// fixed per thread and the others vary.
+__device__ void reduce_tile(const float2* tile, int nb, const TileMap& map, int n, double* red, double* tmp,
+                            double* acc) {
+  double v[kVec];
+#pragma unroll
+  for (int i = 0; i < kVec; ++i) v[i] = 0.0;
+  const uint32_t count = 1u << nb;
+  const int tbits = 31 - __clz(blockDim.x);
+  for (uint32_t e = threadIdx.x; e < count; e += blockDim.x) {
+    const float2 a = tile[swz(e)];
+    const double p = __dadd_rn(__dmul_rn(double(a.x), double(a.x)), __dmul_rn(double(a.y), double(a.y)));
+    v[0] += p;
+#pragma unroll
+    for (int bit = 0; bit < kVec - 1; ++bit)
+      if (bit >= tbits && bit < nb && ((e >> bit) & 1u)) v[1 + bit] += p;
+  }
+#pragma unroll
+  for (int bit = 0; bit < kVec - 1; ++bit)
+    if (bit < tbits && bit < nb && ((threadIdx.x >> bit) & 1u)) v[1 + bit] = v[0];
+  block_sum_vec(v, red, tmp);
+  if (threadIdx.x == 0) {
+    // Local bit -> global qubit; the tile's fixed bits take the whole total.
+    const uint32_t g0 = map.global(0);
+    uint32_t local_global = 0;
+    for (int bit = 0; bit < nb; ++bit) {
+      const uint32_t gq = 31 - __clz(map.global(1u << bit) ^ g0);
+      local_global |= 1u << gq;
+      acc[1 + gq] += tmp[1 + bit];
+    }
+    for (int q = 0; q < n; ++q)
+      if (!((local_global >> q) & 1u) && ((g0 >> q) & 1u)) acc[1 + q] += tmp[0];
+    acc[0] += tmp[0];
+  }
+  __syncthreads();
+}
+
+// Tile <-> slot copies in 16-byte units (element pairs 2u, 2u+1, which are
+// adjacent in the slot because every tile keeps at least global bit 0, and
+// adjacent in shared memory because swz only flips bit 0 of the pair's
+// position when bit 4 of e is set). Four units per thread are in flight.
+constexpr int kCopyUnroll = 4;
+
+__device__ __forceinline__ void put_pair(float2* tile, uint32_t e, float4 v) {
+  const uint32_t p = swz(e);
+  float4* dst = reinterpret_cast<float4*>(tile + (p & ~1u));
+  *dst = (p & 1u) ? make_float4(v.z, v.w, v.x, v.y) : v;
+}
+
+__device__ __forceinline__ float4 get_pair(const float2* tile, uint32_t e) {
+  const uint32_t p = swz(e);
+  const float4 v = *reinterpret_cast<const float4*>(tile + (p & ~1u));
+  return (p & 1u) ? make_float4(v.z, v.w, v.x, v.y) : v;
+}
+
+__device__ void load_tile(float2* tile, const float2* __restrict__ slot, const TileMap& map) {
+  const uint32_t units = 1u << (map.L - 1);
+  for (uint32_t u0 = threadIdx.x; u0 < units; u0 += kCopyUnroll * blockDim.x) {
+    float4 v[kCopyUnroll];
+#pragma unroll
+    for (int k = 0; k < kCopyUnroll; ++k) {
+      const uint32_t u = u0 + k * blockDim.x;
+      if (u < units) v[k] = __ldcs(reinterpret_cast<const float4*>(slot + map.global(2 * u)));
+    }
+#pragma unroll
+    for (int k = 0; k < kCopyUnroll; ++k) {
+      const uint32_t u = u0 + k * blockDim.x;
+      if (u < units) put_pair(tile, 2 * u, v[k]);
+    }
+  }
+}
+
+__device__ void store_tile(const float2* tile, float2* __restrict__ slot, const TileMap& map) {
+  const uint32_t units = 1u << (map.L - 1);
+  for (uint32_t u = threadIdx.x; u < units; u += blockDim.x)
+    __stcs(reinterpret_cast<float4*>(slot + map.global(2 * u)), get_pair(tile, 2 * u));
+}
+
+__device__ void load_mats(float2* smem_mats, const float2* gates, int first_global, int count, int local0) {
+  for (int i = threadIdx.x; i < 4 * count; i += blockDim.x)
+    smem_mats[4 * local0 + i] = gates[4 * first_global + i];
+}
+
+__global__ void __launch_bounds__(512) k_batch(const BatchCircuit* __restrict__ circuits,
+                                               const uint32_t* __restrict__ order, uint32_t count,
+                                               const float2* __restrict__ gates, float2* __restrict__ slots,
+                                               uint64_t slot_elems, double* __restrict__ out,
+                                               uint32_t* __restrict__ queue, int L) {
+  extern __shared__ float2 tile[];
+  __shared__ float2 mats[4 * kBatchMaxQubits];
+  __shared__ double red[32 * kVec];
+  __shared__ double tmp[kVec];
+  __shared__ double acc[1 + kBatchMaxQubits];
+  __shared__ uint32_t item;
+  float2* slot = slots + uint64_t(blockIdx.x) * slot_elems;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(queue, 1u);
+    __syncthreads();
+    const uint32_t it = item;
+    if (it >= count) break;
+    const BatchCircuit c = circuits[order[it]];
+    const int n = int(c.num_qubits);
+    if (threadIdx.x <= kBatchMaxQubits) acc[threadIdx.x] = 0.0;
+    if (n <= L) {
+      // Whole state in shared memory.
+      const uint32_t size = 1u << n;
+      for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) tile[swz(e)] = make_float2(e == 0 ? 1.f : 0.f, 0.f);
+      const TileMap map{0, 0, L, 0};
+      for (uint32_t l = 0; l < c.num_layers; ++l) {
+        __syncthreads();
+        load_mats(mats, gates + 4 * c.gates, int(l) * n, n, 0);
+        __syncthreads();
+        apply_range(tile, n, 0, n, mats, int(c.entangler), 0, map);
+      }
+      __syncthreads();
+      reduce_tile(tile, n, map, n, red, tmp, acc);
+    } else {
+      // Two tile passes per layer over the slot in HBM.
+      const int r = 2 * L - n;
+      const uint32_t tiles = 1u << (n - L);
+      const uint32_t tsize = 1u << L;
+      for (uint32_t l = 0; l < c.num_layers; ++l) {
+        const bool last = l + 1 == c.num_layers;
+        __syncthreads();
+        load_mats(mats, gates + 4 * c.gates, int(l) * n, n, 0);
+        __syncthreads();
+        for (uint32_t t = 0; t < tiles; ++t) {  // pass A: low L qubits
+          const TileMap map{0, 0, L, t};
+          if (l == 0) {
+            for (uint32_t e = threadIdx.x; e < tsize; e += blockDim.x)
+              tile[swz(e)] = make_float2((t == 0 && e == 0) ? 1.f : 0.f, 0.f);
+          } else {
+            load_tile(tile, slot, map);
+          }
+          __syncthreads();
+          apply_range(tile, L, 0, L, mats, int(c.entangler), 0, map);
+          store_tile(tile, slot, map);
+          __syncthreads();
+        }
+        for (uint32_t t = 0; t < tiles; ++t) {  // pass B: high n-L qubits
+          const TileMap map{1, r, L, t};
+          load_tile(tile, slot, map);
+          __syncthreads();
+          // Local bits r..L-1 are global qubits L..n-1 (matrices at local index).
+          apply_range(tile, L, r, L, mats + 4 * (L - r), int(c.entangler), L, map);
+          if (last) {
+            reduce_tile(tile, L, map, n, red, tmp, acc);
+          } else {
+            store_tile(tile, slot, map);
+            __syncthreads();
+          }
+        }
+      }
+    }
+    if (threadIdx.x < uint32_t(n)) out[c.out + threadIdx.x] = acc[0] - 2.0 * acc[1 + threadIdx.x];
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+int batch_kernel_occupancy(int threads, int tile_qubits) {
+  int blocks = 0;
+  const size_t smem = sizeof(float2) << tile_qubits;
+  // Allow the largest tile once, so that launches (also under stream
+  // capture) need no attribute change.
+  if (cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(float2) << 14)) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_batch, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return blocks;
+}
+
+void launch_batch(const BatchLaunch& b, cudaStream_t stream) {
+  const size_t smem = sizeof(float2) << b.tile_qubits;
+  QVDG_CUDA(cudaMemsetAsync(b.queue, 0, sizeof(uint32_t), stream));
+  k_batch<<<b.ctas, b.threads, smem, stream>>>(b.circuits, b.order, b.count, b.gates, b.slots, b.slot_elems, b.out,
+                                               b.queue, b.tile_qubits);
+  QVDG_LAUNCH_CHECK();
+}
+
+}  // namespace qvdg

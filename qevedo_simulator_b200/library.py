@@ -19,7 +19,7 @@ import math
 
 import numpy as np
 
-from .circuit import Circuit
+from .circuit import Circuit, Gate
 
 HALF_PI = math.pi / 2.0
 
@@ -184,6 +184,31 @@ def hea_circuit(width: int, layers: int, seed: int) -> Circuit:
         for q in range(width - 1):
             c.cx(q, q + 1)
     return c
+
+
+def hea_layers(width: int, layers: int, seed: int) -> np.ndarray:
+    """The per-qubit gates of hea_circuit(width, layers, seed) as an array of
+    shape (layers, width, 2, 2): RZ(phi) @ RY(theta) (RY applied first), from
+    the same angle draws."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = np.empty((layers, width, 2, 2), dtype=np.complex128)
+    for layer in range(layers):
+        angles = rng.random(2 * width) * math.tau
+        for q in range(width):
+            rz = Gate("rz", (float(angles[2 * q + 1]),)).matrix()
+            out[layer, q] = rz @ Gate("ry", (float(angles[2 * q]),)).matrix()
+    return out
+
+
+def hea_batch(count: int, seed: int, widths=(10, 22), layers=(4, 12)) -> list:
+    """`count` hardware-efficient ansatz specs (width, layers, seed) with width
+    and layer count uniform in the given inclusive ranges; hea_circuit and
+    hea_layers rebuild each one from its spec."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = rng.integers(widths[0], widths[1] + 1, size=count)
+    l = rng.integers(layers[0], layers[1] + 1, size=count)
+    s = rng.integers(0, 2**62, size=count)
+    return [(int(a), int(b), int(c)) for a, b, c in zip(w, l, s)]
 
 
 def haar_su2(rng: np.random.Generator) -> np.ndarray:

@@ -45,3 +45,24 @@ def test_host_only_calls_need_no_device():
     assert "precision" in lib.qvdg_last_error().decode()
     assert lib.qvdg_state_destroy(None) == 0
     assert lib.qvdg_norm_sqr(None, None) == 1
+
+
+def test_batch_validation_needs_no_device():
+    """Invalid batches are refused before any device work."""
+    import numpy as np
+
+    from qevedo_simulator_b200._abi import QvdgLayeredCircuit, as_double_ptr
+
+    lib = _native.lib()
+    g = np.zeros(8 * 25, dtype=np.float64)
+    arr = (QvdgLayeredCircuit * 1)()
+    arr[0].num_qubits, arr[0].num_layers, arr[0].entangler = 25, 1, 1
+    arr[0].gates = as_double_ptr(g)
+    h = ct.c_void_p()
+    assert lib.qvdg_batch_create(arr, 1, None, ct.byref(h)) == 1
+    assert "num_qubits" in lib.qvdg_last_error().decode()
+    arr[0].num_qubits, arr[0].entangler = 3, 9
+    assert lib.qvdg_batch_create(arr, 1, None, ct.byref(h)) == 1
+    assert "entangler" in lib.qvdg_last_error().decode()
+    assert lib.qvdg_batch_create(arr, 0, None, ct.byref(h)) == 1
+    assert lib.qvdg_batch_destroy(None) == 0
