@@ -377,6 +377,7 @@ bool tensor_pass_ok(const Target& s, const PlannedPass& p) {
 
 LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig& cfg, StageUpload& up) {
   if (p.staged && cfg.tensor && cfg.low_bits >= 1 && tensor_pass_ok(s, p)) return lower_tensor_pass(s, p, cfg, up);
+  if (p.staged && cfg.reg && cfg.low_bits >= 1 && register_pass_ok(s, p)) return lower_register_pass(s, p, cfg, up);
   LoweredPass lp;
   lp.staged = p.staged;
   if (!p.staged) {
@@ -464,7 +465,9 @@ void launch_pass(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev) {
     launch_plain_gate(s, lp.plain, dev.mats);
     return;
   }
-  if (lp.geo.tensor)
+  if (lp.geo.tensor == 2)
+    launch_stage_reg(s, lp, dev);
+  else if (lp.geo.tensor == 1)
     launch_stage_tc(s, lp, dev);
   else if (s.bits == 32)
     stage_launch<float>(s, lp, dev);

@@ -35,6 +35,7 @@ struct StageConfig {
   uint32_t tile_bits;  // L
   uint32_t low_bits;   // B
   bool tensor;         // fused 3-6 qubit gates on the tensor cores
+  bool reg;            // CUDA-core stages gate by gate in registers (unfused)
 };
 
 struct Target;

@@ -38,7 +38,7 @@ struct TileGeom {
   int32_t L, B;
   int32_t num_gates;
   uint32_t tc_bytes;   // bytes of those matrices (kept in shared memory)
-  uint32_t tensor;     // 1: launch the tensor-core kernel
+  uint32_t tensor;     // 1: tensor-core kernel, 2: register-blocked kernel, 0: k_stage
   int32_t tail_absorb;  // tensor passes: trailing one-phase gates applied in the final store
   uint8_t tile_bits[48];  // ascending physical bits of the tile
 };
@@ -74,6 +74,11 @@ struct Target;
 LoweredPass lower_pass(const Target& t, const PlannedPass& p, const StageConfig& cfg, StageUpload& up);
 void launch_pass(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
 void launch_stage_tc(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
+// Register-blocked CUDA-core stages (stage_reg.cu): gates unfused, four tile
+// bits per register pass.
+bool register_pass_ok(const Target& s, const PlannedPass& p);
+LoweredPass lower_register_pass(const Target& s, const PlannedPass& p, const StageConfig& cfg, StageUpload& up);
+void launch_stage_reg(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
 size_t tc_smem_bytes(const TileGeom& geo);
 
 // Bytes of one tensor-core gate's matrices (bf16 hi and lo, 2^(k+1) square).

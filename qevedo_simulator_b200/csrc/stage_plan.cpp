@@ -61,6 +61,7 @@ static size_t tensor_blob_bytes(const HOp& op, uint32_t L) {
 StageConfig stage_config(const Target& s, uint32_t requested, bool tensor) {
   StageConfig c{};
   c.tensor = tensor && s.bits == 32;
+  c.reg = !c.tensor;
   const uint32_t lmax = c.tensor ? kTcTileBits : (s.bits == 32 ? 13 : 12);  // 32-64 KiB tiles
   uint32_t L = requested ? std::min<uint32_t>(requested, lmax) : lmax;
   if (!requested && !c.tensor) {
@@ -131,7 +132,9 @@ std::vector<PlannedPass> plan_stages(const std::vector<HOp>& ops, const std::vec
     // Fuse only ops whose qubits are all local: a fused matrix on a global
     // control or diagonal target would make it a global target
     // (src/blocking.rs:265-267).
-    std::vector<HOp> fused = fuse_where(stage_ops, max_fused, [&](const HOp& op) {
+    // The register-blocked kernel applies gates one by one (fusing would
+    // only add arithmetic there); runs on one qubit still merge.
+    std::vector<HOp> fused = fuse_where(stage_ops, cfg.reg ? 1 : max_fused, [&](const HOp& op) {
       for (uint32_t q : op.qubits())
         if (!local(q)) return false;
       return true;
@@ -244,7 +247,7 @@ void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_s
   QVDG_CUDA(cudaEventRecord(s.ev_stop, s.stream));
   QVDG_CUDA(cudaStreamSynchronize(s.stream));
   bool tensor = false;
-  for (const LoweredPass& lp : p.passes) tensor = tensor || (lp.staged && lp.geo.tensor);
+  for (const LoweredPass& lp : p.passes) tensor = tensor || (lp.staged && lp.geo.tensor == 1);
   if (tensor) {
     int flag = 0;
     QVDG_CUDA(cudaMemcpy(&flag, s.status, sizeof(int), cudaMemcpyDeviceToHost));
