@@ -225,6 +225,43 @@ qvdg_status qvdg_plan_info(const qvdg_plan* plan, qvdg_stats* stats);
  * half of apply_ops, src/simulator.rs:122-147). */
 qvdg_status qvdg_plan_execute(qvdg_state* state, const qvdg_plan* plan, qvdg_stats* stats);
 
+/* ---- Learned cost model ------------------------------------------------
+ * No reference counterpart: the reference plans with fixed greedy rules
+ * (src/fusion.rs, src/blocking.rs). Here a small MLP predicts each pass's
+ * device time from QVDG_PASS_FEATURES features the planner computes per
+ * pass, so a caller can compare candidate plans before running any. */
+#define QVDG_PASS_FEATURES 32
+
+/* Features of every pass the planner builds for `ops` on a `num_qubits`
+ * state under `options` (host only: no device work). `out` receives at most
+ * `capacity` rows of QVDG_PASS_FEATURES floats; `*num_passes` the number of
+ * passes. */
+qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                               const qvdg_options* options, float* out, size_t capacity, size_t* num_passes);
+
+/* An MLP with two hidden ReLU layers of `hidden` units and one linear
+ * output, trained and evaluated by this library's own CUDA kernels (fp32,
+ * on the current device). Parameters, in order: W1 (hidden x inputs), b1,
+ * W2 (hidden x hidden), b2, W3 (1 x hidden), b3. */
+typedef struct qvdg_mlp qvdg_mlp;
+qvdg_status qvdg_mlp_create(uint32_t inputs, uint32_t hidden, uint64_t seed, qvdg_mlp** out);
+qvdg_status qvdg_mlp_destroy(qvdg_mlp* mlp);
+/* Number of parameters; get/set copy all of them (host arrays). */
+qvdg_status qvdg_mlp_num_params(const qvdg_mlp* mlp, size_t* count);
+qvdg_status qvdg_mlp_get_params(const qvdg_mlp* mlp, float* params, size_t count);
+qvdg_status qvdg_mlp_set_params(qvdg_mlp* mlp, const float* params, size_t count);
+/* y[i] = f(x[i]) for `rows` rows of `inputs` floats. */
+qvdg_status qvdg_mlp_forward(qvdg_mlp* mlp, const float* x, size_t rows, float* y);
+/* Mean squared error of f(x) against `target` and its gradient with respect
+ * to every parameter (`grads`: num_params floats, may be NULL). */
+qvdg_status qvdg_mlp_gradients(qvdg_mlp* mlp, const float* x, const float* target, size_t rows, float* loss,
+                               float* grads);
+/* `epochs` passes of Adam (learning rate `lr`) over mini-batches of `batch`
+ * rows in a fixed shuffled order (`seed`); `loss` receives the final
+ * full-data mean squared error. */
+qvdg_status qvdg_mlp_train(qvdg_mlp* mlp, const float* x, const float* target, size_t rows, uint32_t epochs,
+                           uint32_t batch, float lr, uint64_t seed, float* loss);
+
 /* ---- Batched layered circuits ------------------------------------------
  * Many small circuits of uneven width, each a stack of layers: one 2x2 gate
  * on every qubit, then an optional entangler ladder on (q, q+1) for

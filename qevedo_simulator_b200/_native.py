@@ -66,6 +66,19 @@ _SIGNATURES = {
     "qvdg_batch_info": (ct.c_int, [_P, ct.POINTER(QvdgBatchSummary)]),
     "qvdg_batch_tuning": (ct.c_int, [_P, ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_double),
                                      ct.c_size_t, ct.POINTER(ct.c_size_t)]),
+    "qvdg_plan_features": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(QvdgOp), ct.c_size_t,
+                                      ct.POINTER(QvdgOptions), ct.POINTER(ct.c_float), ct.c_size_t,
+                                      ct.POINTER(ct.c_size_t)]),
+    "qvdg_mlp_create": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.c_uint64, ct.POINTER(_P)]),
+    "qvdg_mlp_destroy": (ct.c_int, [_P]),
+    "qvdg_mlp_num_params": (ct.c_int, [_P, ct.POINTER(ct.c_size_t)]),
+    "qvdg_mlp_get_params": (ct.c_int, [_P, ct.POINTER(ct.c_float), ct.c_size_t]),
+    "qvdg_mlp_set_params": (ct.c_int, [_P, ct.POINTER(ct.c_float), ct.c_size_t]),
+    "qvdg_mlp_forward": (ct.c_int, [_P, ct.POINTER(ct.c_float), ct.c_size_t, ct.POINTER(ct.c_float)]),
+    "qvdg_mlp_gradients": (ct.c_int, [_P, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float), ct.c_size_t,
+                                      ct.POINTER(ct.c_float), ct.POINTER(ct.c_float)]),
+    "qvdg_mlp_train": (ct.c_int, [_P, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float), ct.c_size_t, ct.c_uint32,
+                                  ct.c_uint32, ct.c_float, ct.c_uint64, ct.POINTER(ct.c_float)]),
     "qvdg_bit_probabilities_noalloc": (ct.c_int, [_P, ct.c_uint32, ct.c_uint32, _P, ct.POINTER(ct.c_double),
                                                   ct.POINTER(ct.c_double)]),
 }

@@ -576,6 +576,90 @@ qvdg_status qvdg_bit_probabilities_noalloc(const void* amplitudes, uint32_t num_
   });
 }
 
+qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                               const qvdg_options* options, float* out, size_t capacity, size_t* num_passes) {
+  return guarded([&] {
+    require(precision_bits == 32 || precision_bits == 64, "precision must be 32 or 64 bits");
+    require(num_qubits >= 1 && num_qubits <= 40, "a state needs 1 to 40 qubits");
+    qvdg_options opt;
+    qvdg_default_options(&opt);
+    if (options) opt = *options;
+    Target t;
+    t.n = num_qubits;
+    t.bits = int(precision_bits);
+    for (uint32_t q = 0; q < num_qubits; ++q) t.layout.push_back(q);
+    const Program prog = build_program(t, lower_ops(ops, num_ops, num_qubits), opt);
+    const size_t rows = prog.passes.size();
+    if (num_passes) *num_passes = rows;
+    if (out) std::memcpy(out, prog.features.data(), std::min(rows, capacity) * kPassFeatures * sizeof(float));
+  });
+}
+
+qvdg_status qvdg_mlp_create(uint32_t inputs, uint32_t hidden, uint64_t seed, qvdg_mlp** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output handle");
+    *out = nullptr;
+    require(inputs >= 1 && inputs <= 1024 && hidden >= 1 && hidden <= 1024, "inputs and hidden must be 1..1024");
+    *out = mlp_create(inputs, hidden, seed);
+  });
+}
+
+qvdg_status qvdg_mlp_destroy(qvdg_mlp* mlp) {
+  return guarded([&] { mlp_destroy(mlp); });
+}
+
+qvdg_status qvdg_mlp_num_params(const qvdg_mlp* mlp, size_t* count) {
+  return guarded([&] {
+    require(mlp != nullptr && count != nullptr, "null argument");
+    *count = mlp_num_params(mlp);
+  });
+}
+
+qvdg_status qvdg_mlp_get_params(const qvdg_mlp* mlp, float* params, size_t count) {
+  return guarded([&] {
+    require(mlp != nullptr && params != nullptr, "null argument");
+    require(count == mlp_num_params(mlp), "expected " + std::to_string(mlp_num_params(mlp)) + " parameters");
+    mlp_get_params(mlp, params);
+  });
+}
+
+qvdg_status qvdg_mlp_set_params(qvdg_mlp* mlp, const float* params, size_t count) {
+  return guarded([&] {
+    require(mlp != nullptr && params != nullptr, "null argument");
+    require(count == mlp_num_params(mlp), "expected " + std::to_string(mlp_num_params(mlp)) + " parameters");
+    mlp_set_params(mlp, params);
+  });
+}
+
+qvdg_status qvdg_mlp_forward(qvdg_mlp* mlp, const float* x, size_t rows, float* y) {
+  return guarded([&] {
+    require(mlp != nullptr && x != nullptr && y != nullptr, "null argument");
+    require(rows >= 1 && rows <= (size_t(1) << 24), "rows must be 1..2^24");
+    mlp_forward(mlp, x, rows, y);
+  });
+}
+
+qvdg_status qvdg_mlp_gradients(qvdg_mlp* mlp, const float* x, const float* target, size_t rows, float* loss,
+                               float* grads) {
+  return guarded([&] {
+    require(mlp != nullptr && x != nullptr && target != nullptr, "null argument");
+    require(rows >= 1 && rows <= (size_t(1) << 24), "rows must be 1..2^24");
+    const float l = mlp_gradients(mlp, x, target, rows, grads);
+    if (loss) *loss = l;
+  });
+}
+
+qvdg_status qvdg_mlp_train(qvdg_mlp* mlp, const float* x, const float* target, size_t rows, uint32_t epochs,
+                           uint32_t batch, float lr, uint64_t seed, float* loss) {
+  return guarded([&] {
+    require(mlp != nullptr && x != nullptr && target != nullptr, "null argument");
+    require(rows >= 1 && rows <= (size_t(1) << 24), "rows must be 1..2^24");
+    require(batch >= 1 && batch <= 65535, "batch must be 1..65535");
+    const float l = mlp_train(mlp, x, target, rows, epochs, batch, lr, seed);
+    if (loss) *loss = l;
+  });
+}
+
 qvdg_status qvdg_batch_create(const qvdg_layered_circuit* circuits, size_t count, const qvdg_batch_options* options,
                               qvdg_batch** out) {
   return guarded([&] {

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "qvdg.h"
 
 namespace qvdg {
 
@@ -98,5 +99,16 @@ double max_abs_diff(StateImpl& a, StateImpl& b);
 // Ascending stable LSD radix sort of `count` 64-bit keys in place (`tmp` has
 // room for `count` keys). `work` provides temporary device memory.
 void radix_sort_u64(uint64_t* keys, uint64_t* tmp, size_t count, DeviceScratch& work, cudaStream_t stream);
+
+// ---- mlp.cu (learned cost model network)
+qvdg_mlp* mlp_create(uint32_t inputs, uint32_t hidden, uint64_t seed);
+void mlp_destroy(qvdg_mlp* m);
+size_t mlp_num_params(const qvdg_mlp* m);
+void mlp_get_params(const qvdg_mlp* m, float* out);
+void mlp_set_params(qvdg_mlp* m, const float* in);
+void mlp_forward(qvdg_mlp* m, const float* x, size_t rows, float* y);
+float mlp_gradients(qvdg_mlp* m, const float* x, const float* t, size_t rows, float* grads);
+float mlp_train(qvdg_mlp* m, const float* x, const float* t, size_t rows, uint32_t epochs, uint32_t batch, float lr,
+                uint64_t seed);
 
 }  // namespace qvdg

@@ -20,6 +20,10 @@ struct Target {
   std::vector<uint32_t> layout;
 };
 
+// Per-pass features for the learned cost model (cost_features.cpp): the
+// kind of pass, its gates by type and width, where they sit, tile shape.
+constexpr int kPassFeatures = 32;
+
 struct Program {
   Target target;
   StageConfig cfg{};
@@ -28,7 +32,10 @@ struct Program {
   StageUpload upload;              // host copy of the gate programs and matrices
   uint64_t gates = 0, kernels = 0, stages = 0;
   double bytes = 0.0;
+  std::vector<float> features;  // kPassFeatures per pass
 };
+
+void pass_features(const Target& t, const PlannedPass& p, const LoweredPass& lp, const StageUpload& up, float* f);
 
 Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt);
 

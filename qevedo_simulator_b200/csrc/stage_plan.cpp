@@ -191,6 +191,8 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
   const double state_bytes = double(uint64_t(t.bits == 32 ? 8 : 16) << t.n);
   for (const PlannedPass& p : passes) {
     prog.passes.push_back(lower_pass(t, p, prog.cfg, prog.upload));
+    prog.features.resize(prog.features.size() + kPassFeatures);
+    pass_features(t, p, prog.passes.back(), prog.upload, prog.features.data() + prog.features.size() - kPassFeatures);
     prog.kernels += p.ops.size();
     double b = 2.0 * state_bytes;
     if (p.staged)

@@ -19,7 +19,7 @@ import math
 
 import numpy as np
 
-from .circuit import Circuit, Gate
+from .circuit import Circuit, Gate, Op
 
 HALF_PI = math.pi / 2.0
 
@@ -222,37 +222,37 @@ def haar_su2(rng: np.random.Generator) -> np.ndarray:
 ISWAP = np.array([[1, 0, 0, 0], [0, 0, 1j, 0], [0, 1j, 0, 0], [0, 0, 0, 1]], dtype=np.complex128)
 
 
-def mixed_circuit(n: int, depth: int, seed: int, p_distance: float = 0.3) -> Circuit:
-    """Cost-model training circuits: per layer, Haar-random SU(2) on every
-    qubit, then pair gates (CZ, CX or iSWAP) on pairs at geometric qubit
-    distance (parameter `p_distance`), a diagonal phase gate and a gate with
-    1-3 controls."""
+def mixed_ops(n: int, depth: int, seed: int, p_distance: float = 0.3) -> list:
+    """Cost-model training circuits as ops: per layer, a Haar-random SU(2) on
+    every qubit; then pair gates (CZ, CX or iSWAP, uniformly) on disjoint
+    pairs at geometric qubit distance (success probability `p_distance`); a
+    diagonal phase gate; and an X with 1 to 3 controls (an op with separate
+    controls, as the reference's Op allows, src/fusion.rs:17-23)."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    c = Circuit(n)
+    ops = []
+    x = np.array([[0, 1], [1, 0]], dtype=np.complex128)
+    z = np.diag([1, -1]).astype(np.complex128)
     for _ in range(depth):
         for q in range(n):
-            c.unitary(haar_su2(rng), [q])
-        free = list(rng.permutation(n))
+            ops.append(Op([q], [], haar_su2(rng)))
+        free = [int(v) for v in rng.permutation(n)]
         while len(free) >= 2:
-            a = int(free.pop())
-            d = int(rng.geometric(p_distance))
-            b = (a + d) % n
+            a = free.pop()
+            b = (a + int(rng.geometric(p_distance))) % n
             if b not in free:
                 continue
             free.remove(b)
             kind = int(rng.integers(0, 3))
             if kind == 0:
-                c.cz(a, b)
+                ops.append(Op([b], [(a, True)], z))
             elif kind == 1:
-                c.cx(a, b)
+                ops.append(Op([b], [(a, True)], x))
             else:
-                c.unitary(ISWAP, [a, b])
+                ops.append(Op([a, b], [], ISWAP))
         q = int(rng.integers(0, n))
-        c.p(float(rng.random()) * math.tau, q)
-        controls = int(rng.integers(1, 3))
-        picks = [int(x) for x in rng.choice(n, size=controls + 1, replace=False)]
-        if controls == 1:
-            c.cx(picks[0], picks[1])
-        else:
-            c.ccx(picks[0], picks[1], picks[2])
-    return c
+        phase = float(rng.random()) * math.tau
+        ops.append(Op([q], [], np.diag([1, complex(math.cos(phase), math.sin(phase))])))
+        controls = int(rng.integers(1, 4))
+        picks = [int(v) for v in rng.choice(n, size=controls + 1, replace=False)]
+        ops.append(Op([picks[-1]], [(c, True) for c in picks[:-1]], x))
+    return ops
