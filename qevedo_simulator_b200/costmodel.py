@@ -219,3 +219,107 @@ def choose_measured(model: CostModel, ops, num_qubits: int, state: DeviceState, 
     if t_default <= t_pick:
         return "default", default_options(), t_default, t_default
     return name, opts, t_pick, t_default
+
+
+def _spec(seed: int, qubits, depth):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return int(rng.choice(qubits)), int(rng.integers(depth[0], depth[1] + 1))
+
+
+def evaluate(model: CostModel, op_lists, num_qubits: int, all_candidates: bool = True) -> list:
+    """Per circuit: the greedy default's, the model's and (optionally) every
+    candidate's measured seconds."""
+    rows = []
+    with DeviceState(num_qubits, 32) as st:
+        for ops in op_lists:
+            name, opts, pred = model.choose(ops, num_qubits)
+            row = {"pick": name, "predicted_s": pred}
+            row["pick_s"], _ = measure_plan(ops, num_qubits, opts, st)
+            row["default_s"], _ = measure_plan(ops, num_qubits, default_options(), st)
+            if all_candidates:
+                row["candidates_s"] = {nm: measure_plan(ops, num_qubits, o, st)[0] for nm, o in candidates()}
+            rows.append(row)
+    return rows
+
+
+def main(argv=None):
+    """Train the cost model on the engine's own timings and evaluate it:
+
+        python -m qevedo_simulator_b200.costmodel --circuits 160 --out PATH
+
+    Training circuits are library.mixed_ops at the --train-qubits sizes with
+    depths in --depth; evaluation circuits are held out (other seeds) at
+    --eval-qubits (every candidate measured) and --big-qubits (greedy default
+    against the model's pick only)."""
+    import argparse
+    import json
+    import time
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train-qubits", type=int, nargs="+", default=[24, 25])
+    ap.add_argument("--circuits", type=int, default=160)
+    ap.add_argument("--depth", type=int, nargs=2, default=[10, 40])
+    ap.add_argument("--eval-qubits", type=int, default=28)
+    ap.add_argument("--eval-circuits", type=int, default=6)
+    ap.add_argument("--big-qubits", type=int, default=33)
+    ap.add_argument("--big-circuits", type=int, default=2)
+    ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--out", default=MODEL_PATH)
+    ap.add_argument("--report", default=None)
+    a = ap.parse_args(argv)
+    t0 = time.time()
+    by_n = {}
+    for i in range(a.circuits):
+        n, d = _spec(1000 + i, a.train_qubits, a.depth)
+        by_n.setdefault(n, []).append(library_mixed(n, d, 1000 + i))
+    xs, ts = [], []
+    for n, lists in sorted(by_n.items()):
+        x, t = collect(lists, n, repeats=1)
+        xs.append(x)
+        ts.append(t)
+    x, t = np.concatenate(xs), np.concatenate(ts)
+    collect_s = time.time() - t0
+    # Hold out every tenth row to report the fit.
+    idx = np.arange(len(t))
+    test = idx % 10 == 0
+    model = CostModel(MLP(seed=7))
+    t1 = time.time()
+    loss = model.fit(x[~test], t[~test], epochs=a.epochs, batch=256, lr=1e-3, seed=11)
+    train_s = time.time() - t1
+    pred = model.mlp.forward(x[test])
+    err = np.abs(pred - t[test])
+    report = {
+        "training_circuits": a.circuits, "train_qubits": a.train_qubits, "depth": a.depth,
+        "pass_rows": int(len(t)), "collect_s": collect_s, "train_s": train_s, "train_loss": loss,
+        "heldout_rows": int(test.sum()), "heldout_median_abs_log_err": float(np.median(err)),
+        "heldout_p90_abs_log_err": float(np.quantile(err, 0.9)),
+    }
+    model.save(a.out, train_loss=loss)
+    ev = [library_mixed(a.eval_qubits, d, 5000 + i)
+          for i, d in enumerate(np.linspace(a.depth[0], a.depth[1], a.eval_circuits).astype(int))]
+    report["eval"] = {"qubits": a.eval_qubits, "circuits": evaluate(model, ev, a.eval_qubits)}
+    if a.big_circuits:
+        big = [library_mixed(a.big_qubits, 10, 7000 + i) for i in range(a.big_circuits)]
+        report["big"] = {"qubits": a.big_qubits, "circuits": evaluate(model, big, a.big_qubits, all_candidates=False)}
+    for key in ("eval", "big"):
+        if key in report:
+            rows = report[key]["circuits"]
+            report[key]["default_total_s"] = float(sum(r["default_s"] for r in rows))
+            report[key]["pick_total_s"] = float(sum(r["pick_s"] for r in rows))
+            if rows and "candidates_s" in rows[0]:
+                report[key]["best_total_s"] = float(sum(min(r["candidates_s"].values()) for r in rows))
+    text = json.dumps(report, indent=1)
+    print(text)
+    if a.report:
+        with open(a.report, "w") as f:
+            f.write(text)
+
+
+def library_mixed(n: int, depth: int, seed: int):
+    from . import library
+
+    return library.mixed_ops(n, depth, seed)
+
+
+if __name__ == "__main__":
+    main()
