@@ -11,8 +11,11 @@ from |0...0>. Synthetic: the circuit comes from a fixed seed.
 Our arm ("ours"): a step is one run of the circuit through a plan executed
 on the device (the state reset to |0...0> between steps, outside the timed
 work), timed with CUDA events on the library's stream. `value` is seconds per
-circuit (tuned path); the plain path (one pass per fused gate), the per-pass
-HBM roofline, the amplitude error against a complex128 run, the end-to-end
+circuit on the tuned path: the plan the learned cost model picks among the
+candidates (plain per-gate passes at fusion 2-5, staged CUDA-core and
+tensor-core stages), judged by measurement against the greedy default; every
+candidate's measured time is in the line. The plain path (one pass per fused
+4-qubit gate), the HBM roofline of the dominant kernel, the amplitude error against a complex128 run, the end-to-end
 time of the public `run()` call (host planning, uploads from pinned memory,
 1000 shots, outcomes back to the host) and the CPU baseline are reported
 beside it. With N GPUs each rank runs its own circuit (replicas; the state
@@ -223,6 +226,27 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def choose_tuned(ops, n: int, st, fixed=None):
+    """The tuned plan: the learned cost model's pick among the candidate plans
+    (plain per-gate passes at fusion 2-5, staged CUDA-core, staged tensor-core),
+    judged by measurement against the greedy default. Returns (name, options,
+    {candidate: measured seconds}) -- every candidate is measured once so the
+    line shows what the choice was between."""
+    from qevedo_simulator_b200 import costmodel, options
+
+    if fixed is not None:
+        return fixed[0], fixed[1], {}
+    model = costmodel.CostModel.load()
+    name, opts, _ = model.choose(ops, n)
+    measured = {}
+    for nm, o in costmodel.candidates():
+        measured[nm] = costmodel.measure_plan(ops, n, o, st, repeats=1)[0]
+    default = measured["staged-cuda"]
+    if measured[name] > default:  # the greedy default judges the pick
+        name, opts = "staged-cuda", costmodel.default_options()
+    return name, opts, measured
+
+
 def run_ours(args, rank: int, world: int):
     import torch
 
@@ -241,10 +265,14 @@ def run_ours(args, rank: int, world: int):
     n, depth = args.qubits, DEPTH
     circuit = build_circuit(n, depth)
     ops = circuit.ops()
-    fused = args.fusion
-    tuned = Plan(ops, n, 32, options(fused, staged=True, math=args.math))
-    plain = Plan(ops, n, 32, options(4, staged=False))
     st = DeviceState(n, 32)
+    fixed = None
+    if args.plan:
+        f, staged, math_ = args.plan
+        fixed = (f"fixed-{f}-{staged}-{math_}", options(int(f), staged=staged == "staged", math=math_))
+    tuned_name, tuned_opts, candidates = choose_tuned(ops, n, st, fixed)
+    tuned = Plan(ops, n, 32, tuned_opts)
+    plain = Plan(ops, n, 32, options(4, staged=False))
     st.set_pass_timing(True)
 
     def barrier():
@@ -278,27 +306,35 @@ def run_ours(args, rank: int, world: int):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         step = float(t.item())
     info = tuned.info()
-    # Plain path (one pass per fused gate, the reference's region_bits=None).
+    # Plain path (one pass per fused 4-qubit gate, the reference's region_bits=None).
     plain_times = []
     for _ in range(max(1, min(2, args.steps))):
         st.zero()
         plain_times.append(st.execute(plain)["gate_seconds"])
     plain_s = float(np.mean(plain_times))
     plain_info = plain.info()
-    # Roofline of the dominant kernel: the staged tile pass.
+    # Roofline of the dominant kernel of the tuned plan (the pass kind with
+    # the most device time): algorithmic bytes per launch / mean launch time.
     sec = np.concatenate(pass_t)
     byt = np.concatenate(pass_b)
     kind = np.concatenate(pass_k)
     peaks = measured_peaks()
-    staged_sec = sec[kind == 1]
-    staged_bytes = byt[kind == 1]
-    avg = float(staged_sec.mean()) if staged_sec.size else float(sec.mean())
-    per_launch = float(staged_bytes.mean()) if staged_bytes.size else float(byt.mean())
-    achieved = per_launch / avg / 1e9
+    dom = 1 if sec[kind == 1].sum() >= sec[kind == 0].sum() else 0
+    dsec, dbyt = sec[kind == dom], byt[kind == dom]
+    avg = float(dsec.mean())
+    per_launch = float(dbyt.mean())
+    achieved = float(dbyt.sum() / dsec.sum() / 1e9)
+    if dom == 0:
+        kernel = "k_dense<float,K,...> (plain fused-gate pass)"
+    elif tuned_opts.math == 1:
+        kernel = "k_stage_tc (tensor-core stage)"
+    else:
+        kernel = "k_stage_reg<float> (register-blocked stage)"
+    traffic = args.traffic
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": args.traffic,
-                "kernel": "k_stage_tc" if args.math == "tensor" else "k_stage<float>",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": kernel,
                 "peak_source": peaks["source"], "bytes_per_launch": per_launch, "avg_launch_s": avg,
+                "launches_per_step": int(dsec.size // max(1, args.steps)),
                 "whole_run_gbs": info["bytes"] / step / 1e9}
     # Accuracy: tuned complex64 against a complex128 run of the same circuit.
     err = None
@@ -311,10 +347,12 @@ def run_ours(args, rank: int, world: int):
     # End to end through the public API: plan on the host, upload gate data
     # from pinned memory, run, sample SHOTS shots, outcomes back to the host.
     e2e = []
+    staged = bool(tuned_opts.staged)
+    math_name = "tensor" if tuned_opts.math == 1 else "fp32"
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        res = run(circuit.copy().measure_all(), SHOTS, seed=7 + i, max_fused_qubits=fused, math=args.math,
-                  state=st)
+        run(circuit.copy().measure_all(), SHOTS, seed=7 + i, max_fused_qubits=int(tuned_opts.max_fused_qubits),
+            staged=staged, math=math_name, state=st)
         if i >= args.warmup:
             e2e.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e))
@@ -340,8 +378,11 @@ def run_ours(args, rank: int, world: int):
                     "call": f"qevedo_simulator_b200.run(circuit, shots={SHOTS}) on a reused device state"},
             "gpu_launches": int(info["passes"]) * args.steps,
             "clocks": clocks.summary(),
-            "tuned": {"s": step, "passes": info["passes"], "stages": info["stages"], "kernels": info["kernels"],
-                      "max_fused_qubits": fused, "math": args.math,
+            "tuned": {"s": step, "plan": tuned_name, "passes": info["passes"], "stages": info["stages"],
+                      "kernels": info["kernels"], "max_fused_qubits": int(tuned_opts.max_fused_qubits),
+                      "staged": staged, "math": math_name,
+                      "chosen_by": "learned cost model, judged against the greedy default" if fixed is None
+                      else "--plan", "candidates_s": {k: round(v, 5) for k, v in candidates.items()},
                       "pass_ms": [round(float(x) * 1e3, 3) for x in pass_t[-1]]},
             "plain": {"s": plain_s, "passes": plain_info["passes"], "kernels": plain_info["kernels"]},
             "tuned_over_plain": step / plain_s,
@@ -370,13 +411,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--qubits", type=int, default=30)
-    ap.add_argument("--fusion", type=int, default=5)
-    ap.add_argument("--math", choices=["tensor", "fp32"], default="tensor")
+    ap.add_argument("--plan", nargs=3, metavar=("FUSION", "plain|staged", "fp32|tensor"), default=None,
+                    help="run this plan instead of the learned planner's choice")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-check", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0)
     ap.add_argument("--traffic", type=float, default=None,
-                    help="DRAM bytes per stage launch from an ncu capture (reported as roofline.traffic)")
+                    help="DRAM bytes per launch of the dominant kernel from an ncu capture (roofline.traffic)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

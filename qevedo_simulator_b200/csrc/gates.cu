@@ -85,6 +85,106 @@ __global__ void __launch_bounds__(kThreads) k_dense(cplx_t<T>* __restrict__ psi,
   }
 }
 
+// Dense gates with targets among the low index bits: each thread's group is
+// then a short contiguous run and a warp's loads stride by the run length.
+// Instead, a block stages a tile of 2^13 amplitudes -- index bits 0..Lb-1
+// (contiguous runs of 2^Lb) plus the targets above them -- in shared memory
+// with coalesced 16-byte accesses, applies the gate to the tile's 2^(13-K)
+// groups there (two per thread, so each matrix entry read serves both) and
+// stores the tile back.
+constexpr int kTileBits = 13;
+
+struct DenseTileGeom {
+  uint64_t tiles;
+  int32_t lb;             // contiguous low bits of the tile
+  int32_t nhigh;          // targets at or above lb
+  uint8_t high[8];        // physical positions of those targets (ascending)
+  uint8_t fixed_tile[8];  // tile-local positions of all targets (ascending)
+  uint16_t offsets[64];   // tile-local offset of group member h (matrix index order)
+};
+
+// Shared-memory position of tile element e (bits 4-7 folded into 1-3; bit 0
+// kept so 16-byte element pairs stay together).
+__device__ __forceinline__ uint32_t dswz(uint32_t e) { return e ^ ((e >> 4) & 14u); }
+
+template <int K>
+__global__ void __launch_bounds__(kThreads) k_dense_tile(float2* __restrict__ psi, const DenseTileGeom g,
+                                                         const float2* __restrict__ mat) {
+  constexpr int D = 1 << K;
+  constexpr uint32_t kTile = 1u << kTileBits;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tile = reinterpret_cast<float2*>(smem_raw);
+  float2* sm = tile + kTile;
+  __shared__ uint8_t fixed[8];
+  __shared__ uint16_t off[64];
+  for (int i = threadIdx.x; i < D * D; i += blockDim.x) sm[i] = mat[i];
+  if (threadIdx.x < 8) fixed[threadIdx.x] = g.fixed_tile[threadIdx.x];
+  if (threadIdx.x < 64) off[threadIdx.x] = g.offsets[threadIdx.x];
+  __syncthreads();
+  const uint32_t lowmask = (1u << g.lb) - 1u;
+  for (uint64_t t = blockIdx.x; t < g.tiles; t += gridDim.x) {
+    // Tile t: its bits above lb, with zeros at the high targets, give the
+    // base index; element e adds its low bits and the high targets.
+    uint64_t base = t << g.lb;
+    for (int i = 0; i < g.nhigh; ++i) {
+      const uint32_t p = g.high[i];
+      base = ((base >> p) << (p + 1)) | (base & ((uint64_t(1) << p) - 1));
+    }
+    auto global_of = [&](uint32_t e) -> uint64_t {
+      uint64_t x = base | (e & lowmask);
+      uint32_t h = e >> g.lb;
+      for (int i = 0; i < g.nhigh; ++i) x |= uint64_t((h >> i) & 1u) << g.high[i];
+      return x;
+    };
+    // Every 16-byte copy of the tile in flight at once (cp.async).
+    for (uint32_t u = threadIdx.x; u < kTile / 2; u += blockDim.x) {
+      const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(tile + dswz(2 * u)));
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(psi + global_of(2 * u)) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    constexpr uint32_t kGroups = kTile >> K;
+    for (uint32_t q = threadIdx.x; q < kGroups / 2; q += blockDim.x) {
+      uint32_t b[2];
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        uint32_t x = q + s * (kGroups / 2);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          const uint32_t p = fixed[i];
+          x = ((x >> p) << (p + 1)) | (x & ((1u << p) - 1u));
+        }
+        b[s] = x;
+      }
+      float2 x[2][D];
+#pragma unroll
+      for (int h = 0; h < D; ++h) {
+        x[0][h] = tile[dswz(b[0] | off[h])];
+        x[1][h] = tile[dswz(b[1] | off[h])];
+      }
+#pragma unroll 1
+      for (int r = 0; r < D; ++r) {
+        float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int c = 0; c < D; c += 2) {
+          const float4 m = *reinterpret_cast<const float4*>(sm + r * D + c);
+          const float2 m0 = make_float2(m.x, m.y), m1 = make_float2(m.z, m.w);
+          cmac<float>(a0, m0, x[0][c]);
+          cmac<float>(a1, m0, x[1][c]);
+          cmac<float>(a0, m1, x[0][c + 1]);
+          cmac<float>(a1, m1, x[1][c + 1]);
+        }
+        tile[dswz(b[0] | off[r])] = a0;
+        tile[dswz(b[1] | off[r])] = a1;
+      }
+    }
+    __syncthreads();
+    for (uint32_t u = threadIdx.x; u < kTile / 2; u += blockDim.x)
+      *reinterpret_cast<float4*>(psi + global_of(2 * u)) = *reinterpret_cast<const float4*>(tile + dswz(2 * u));
+    __syncthreads();
+  }
+}
+
 struct DiagGeom {
   uint64_t n_iter;         // amplitudes in the controlled subspace
   uint64_t control_value;
@@ -265,6 +365,68 @@ void plain_gate(StateImpl& s, const PlainGate& pg, const void* matrices) {
     g.offsets[h] = o;
   }
   const bool bit0_free = fixed.empty() || fixed[0] != 0;
+  // complex64, no controls, targets (nearly) all among bits 0-3 -- each
+  // group one short contiguous run -- and a state of at least one tile:
+  // stage tiles through shared memory (coalesced) instead. With fewer low
+  // targets the direct kernel's accesses are coalesced enough and it is faster.
+  int low_targets = 0;
+  for (uint32_t t : pg.targets) low_targets += t < 4 ? 1 : 0;
+  if (sizeof(T) == 4 && c == 0 && k >= 2 && k <= 4 && low_targets >= std::min(k, 3) &&
+      s.n >= uint32_t(kTileBits) + 1) {
+    DenseTileGeom tg{};
+    int lb = kTileBits, nhigh = 0;
+    for (int iter = 0; iter < 8; ++iter) {
+      nhigh = 0;
+      for (uint32_t t : pg.targets) nhigh += t >= uint32_t(lb) ? 1 : 0;
+      const int next = kTileBits - nhigh;
+      if (next == lb) break;
+      lb = next;
+    }
+    std::vector<uint32_t> high;
+    for (uint32_t t : pg.targets)
+      if (t >= uint32_t(lb)) high.push_back(t);
+    std::sort(high.begin(), high.end());
+    if (int(high.size()) == nhigh && lb + nhigh == kTileBits) {
+      tg.lb = lb;
+      tg.nhigh = nhigh;
+      tg.tiles = uint64_t(1) << (s.n - kTileBits);
+      for (int i = 0; i < nhigh; ++i) tg.high[i] = uint8_t(high[i]);
+      auto local = [&](uint32_t t) -> uint32_t {
+        if (t < uint32_t(lb)) return t;
+        return uint32_t(lb) + uint32_t(std::find(high.begin(), high.end(), t) - high.begin());
+      };
+      std::vector<uint8_t> ft;
+      for (uint32_t t : pg.targets) ft.push_back(uint8_t(local(t)));
+      std::sort(ft.begin(), ft.end());
+      for (size_t i = 0; i < ft.size(); ++i) tg.fixed_tile[i] = ft[i];
+      for (int h = 0; h < (1 << k); ++h) {
+        uint32_t o = 0;
+        for (int j = 0; j < k; ++j) o |= uint32_t((h >> j) & 1) << local(pg.targets[j]);
+        tg.offsets[h] = uint16_t(o);
+      }
+      const size_t bytes = (size_t(1) << kTileBits) * sizeof(float2) + (size_t(1) << (2 * k)) * sizeof(float2);
+      const unsigned grid = unsigned(std::min<uint64_t>(tg.tiles, uint64_t(s.sms) * 3));
+      auto* psi = static_cast<float2*>(s.amp);
+      auto* m = reinterpret_cast<const float2*>(mat);
+      static bool configured[5] = {false, false, false, false, false};
+      if (!configured[k]) {
+        const void* fn = k == 2 ? reinterpret_cast<const void*>(k_dense_tile<2>)
+                                : (k == 3 ? reinterpret_cast<const void*>(k_dense_tile<3>)
+                                          : reinterpret_cast<const void*>(k_dense_tile<4>));
+        QVDG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+        configured[k] = true;
+      }
+      switch (k) {
+        case 2:
+          k_dense_tile<2><<<grid, kThreads, bytes, s.stream>>>(psi, tg, m);
+          break;
+        case 3: k_dense_tile<3><<<grid, kThreads, bytes, s.stream>>>(psi, tg, m); break;
+        default: k_dense_tile<4><<<grid, kThreads, bytes, s.stream>>>(psi, tg, m); break;
+      }
+      QVDG_LAUNCH_CHECK();
+      return;
+    }
+  }
   switch (k) {
     case 1: return dense_pick<T, 1>(s, g, mat, bit0_free);
     case 2: return dense_pick<T, 2>(s, g, mat, bit0_free);

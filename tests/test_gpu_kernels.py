@@ -80,6 +80,25 @@ def test_staged_gate_with_global_controls_and_diagonals(oracle, bits):
                 assert max_distance(st.amplitudes(), expected) < TOL[bits] * 10, (case, tile)
 
 
+@pytest.mark.parametrize("n", [13, 14, 16])
+def test_dense_gates_on_low_bits_through_tiles(oracle, n):
+    """Plain dense gates with targets among bits 0-3 (staged through
+    shared-memory tiles) on every kind of target layout, against the naive
+    oracle; controlled ones keep the direct path."""
+    rng = np.random.Generator(np.random.PCG64(n))
+    initial = random_state(rng, n)
+    layouts = [[0, 1, 2, 3], [0, 1, 5, 7], [3, 0], [1, n - 1], [0, n - 3, n - 2, n - 1], [2, 11, 12],
+               [n - 1, 0, 6, 2], [1, 2, 3], [3, 1, n - 1, 2], [2, 0, 1, 9]]
+    for qubits in layouts:
+        for controls in ([], [(4 if 4 not in qubits else 8, True)]):
+            m = random_unitary(rng, len(qubits))
+            expected = oracle.naive_apply_ops(initial, [Op(qubits, controls, m)])
+            with DeviceState(n, 32) as st:
+                st.set_amplitudes(initial)
+                st.apply_ops([Op(qubits, controls, m)], options(4, staged=False))
+                assert max_distance(st.amplitudes(), expected) < TOL[32] * 4, (qubits, controls)
+
+
 def test_invalid_input_is_rejected():
     with DeviceState(4, 32) as st:
         with pytest.raises(ValueError, match="out of range"):
