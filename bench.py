@@ -226,6 +226,18 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(value: float, dist, device: str = "cuda") -> float:
+    """The largest `value` over all ranks (every rank gets it); the value
+    itself with no process group."""
+    if dist is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def choose_tuned(ops, n: int, st, fixed=None):
     """The tuned plan: the learned cost model's pick among the candidate plans
     (plain per-gate passes at fusion 2-5, staged CUDA-core, staged tensor-core),
@@ -300,11 +312,7 @@ def run_ours(args, rank: int, world: int):
     torch.cuda.synchronize()
     barrier()
     wall = time.perf_counter() - wall0
-    step = float(np.mean(times))
-    if dist is not None:
-        t = torch.tensor([step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step = float(t.item())
+    step = max_over_ranks(float(np.mean(times)), dist)
     info = tuned.info()
     # Plain path (one pass per fused 4-qubit gate, the reference's region_bits=None).
     plain_times = []
@@ -355,13 +363,9 @@ def run_ours(args, rank: int, world: int):
             staged=staged, math=math_name, state=st)
         if i >= args.warmup:
             e2e.append(time.perf_counter() - t0)
-    e2e_s = float(np.mean(e2e))
+    e2e_s = max_over_ranks(float(np.mean(e2e)), dist)
     h2d = tuned_upload_bytes(ops) + 8 * SHOTS
     d2h = 8 * SHOTS + 16
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         cpu = cpu_baseline(ops, n, layer_prefix_ops(circuit, n), budget_s=args.cpu_budget)
