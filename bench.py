@@ -402,6 +402,118 @@ def run_ours(args, rank: int, world: int):
         dist.destroy_process_group()
 
 
+def timed_plan(st, plan, initial=None, repeats: int = 2):
+    """(best device seconds, per-pass seconds, per-pass bytes) of a plan; the
+    state is reset (or loaded with `initial`) outside the timed work."""
+    best, sec, byt = float("inf"), None, None
+    st.set_pass_timing(True)
+    for _ in range(repeats):
+        if initial is None:
+            st.zero()
+        else:
+            st.set_amplitudes(initial)
+        s = st.execute(plan)
+        if s["gate_seconds"] < best:
+            best = s["gate_seconds"]
+            sec, byt, _ = st.pass_times()
+    st.set_pass_timing(False)
+    return best, sec, byt
+
+
+def run_qft(args):
+    """QFT on n qubits (complex64) from a normalised i.i.d. complex Gaussian
+    state (seeded); every candidate plan and the learned pick timed, per-pass
+    HBM GB/s, error against a complex128 run of the same circuit."""
+    from qevedo_simulator_b200 import DeviceState, Plan, costmodel, library
+
+    n = args.qubits
+    psi0 = library.gaussian_state(n, SEED)
+    ops = library.qft(n).ops()
+    model = costmodel.CostModel.load()
+    pick, pick_opts, _ = model.choose(ops, n)
+    out = {"metric": "QFT seconds and per-pass HBM GB/s", "workload": f"QFT {n} qubits complex64 from a seeded "
+           "normalised complex Gaussian state (textbook H + controlled phases, no final swaps)", "unit": "s",
+           "higher_is_better": False, "pick": pick, "plans": {}}
+    peak = measured_peaks()["hbm_gbs"]
+    with DeviceState(n, 64) as ref:
+        ref.set_amplitudes(psi0)
+        ref.apply_ops(ops, costmodel.options(4, staged=False))
+        with DeviceState(n, 32) as st:
+            for name, opts in costmodel.candidates():
+                if name not in ("plain-f4", "staged-cuda", "staged-tensor-f4", pick):
+                    continue
+                with Plan(ops, n, 32, opts) as plan:
+                    t, sec, byt = timed_plan(st, plan, psi0)
+                    gbs = byt / sec / 1e9
+                    out["plans"][name] = {"s": t, "passes": int(sec.size), "pass_gbs_mean": float(gbs.mean()),
+                                          "pass_gbs_min": float(gbs.min()), "frac_of_measured_hbm":
+                                          float(byt.sum() / sec.sum() / 1e9 / peak),
+                                          "max_amp_err_vs_c128": ref.max_abs_diff(st)}
+    out["value"] = out["plans"][pick]["s"]
+    out["plain_s"] = out["plans"]["plain-f4"]["s"]
+    print(json.dumps(out), flush=True)
+
+
+def grid_circuit_31():
+    """The 4x8 grid circuit with every gate on qubit 31 removed (31 is prime,
+    so the 31-qubit grid is 4x8 minus its last qubit)."""
+    from qevedo_simulator_b200 import Circuit, library
+
+    full = library.random_grid_circuit(4, 8, DEPTH, SEED)
+    c = Circuit(31)
+    for ins in full._instructions:
+        if ins[0] == "gate" and 31 not in ins[2]:
+            c._instructions.append(ins)
+    return c
+
+
+def run_precision(args):
+    """The precision form: grid circuits at 32 qubits complex64 (tensor-core
+    stages, 5-6 qubit fused matrices as bf16x3 products with fp32
+    accumulation) and 31 qubits complex128, 1M shots each; the error of
+    every complex64 path against an FP64 run at 28 qubits."""
+    from qevedo_simulator_b200 import DeviceState, Plan, library, options
+
+    out = {"metric": "precision form: seconds, 1M-shot sampling seconds, error vs FP64", "unit": "s",
+           "higher_is_better": False, "runs": {}}
+    # Error at 28 qubits (4x7 grid).
+    c28 = library.random_grid_circuit(4, 7, DEPTH, SEED)
+    with DeviceState(28, 64) as ref:
+        ref.apply_ops(c28.ops(), options(4, staged=False))
+        errs = {}
+        for name, opts in [("tensor-f5", options(5, True, math="tensor")), ("tensor-f4", options(4, True,
+                           math="tensor")), ("fp32-staged", options(4, True)), ("fp32-plain", options(4, False))]:
+            with DeviceState(28, 32) as st:
+                st.apply_ops(c28.ops(), opts)
+                errs[name] = ref.max_abs_diff(st)
+        out["max_amp_err_vs_fp64_28q"] = errs
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    u = rng.random(1_000_000)
+    for label, circuit, bits, plans in [
+            ("32q-c64", library.random_grid_circuit(4, 8, DEPTH, SEED), 32,
+             [("tensor-f5", options(5, True, math="tensor")), ("plain-f4", options(4, False))]),
+            ("31q-c128", grid_circuit_31(), 64,
+             [("staged-fp64", options(4, True)), ("plain-f4", options(4, False))])]:
+        n = circuit.num_qubits
+        ops = circuit.ops()
+        run = {}
+        with DeviceState(n, bits) as st:
+            for name, opts in plans:
+                with Plan(ops, n, bits, opts) as plan:
+                    t, sec, _ = timed_plan(st, plan, None, repeats=1)
+                    run[name] = {"s": t, "passes": int(sec.size)}
+            st.zero()
+            st.apply_ops(ops, plans[0][1])
+            t0 = time.perf_counter()
+            shots = st.sample_unordered(u)
+            run["sample_1M_s"] = time.perf_counter() - t0
+            run["norm_sqr"] = st.norm_sqr()
+            run["shots"] = int(shots.size)
+        out["runs"][label] = run
+    out["value"] = out["runs"]["32q-c64"]["tensor-f5"]["s"]
+    print(json.dumps(out), flush=True)
+
+
 def tuned_upload_bytes(ops) -> int:
     """Upper bound of the gate-program and matrix bytes a plan uploads per
     run (complex64 matrices plus a 96-byte descriptor per op)."""
@@ -415,6 +527,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--workload", choices=["grid", "qft", "precision"], default="grid",
+                    help="grid: the 30-qubit random-circuit benchmark (the bench line); qft and precision: the "
+                         "other configurations, one JSON line each")
     ap.add_argument("--plan", nargs=3, metavar=("FUSION", "plain|staged", "fp32|tensor"), default=None,
                     help="run this plan instead of the learned planner's choice")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -427,6 +542,12 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "qft":
+        if rank == 0:
+            run_qft(args)
+    elif args.workload == "precision":
+        if rank == 0:
+            run_precision(args)
     else:
         run_ours(args, rank, world)
 
