@@ -71,7 +71,7 @@ enum { QVDG_PLANNER_GREEDY = 0, QVDG_PLANNER_LEARNED = 1 };
  * real matrix products on the tensor cores, operands split into bf16 high and
  * low parts with fp32 accumulation (hi*hi + hi*lo + lo*hi, about 16
  * significant bits per product; diagonal and 1-2 qubit gates stay fp32). */
-enum { QVDG_MATH_FP32 = 0, QVDG_MATH_TENSOR = 1 };
+enum { QVDG_MATH_FP32 = 0, QVDG_MATH_TENSOR = 1, QVDG_MATH_GATES = 2 };
 
 /* Simulator options. Reference: simulator::Options, src/simulator.rs:37-66
  * (defaults max_fused_qubits = 4, region_bits = Some(14)). */
@@ -88,7 +88,9 @@ typedef struct {
   uint32_t tile_qubits;
   /* QVDG_PLANNER_GREEDY or QVDG_PLANNER_LEARNED. */
   uint32_t planner;
-  /* QVDG_MATH_FP32 or QVDG_MATH_TENSOR. */
+  /* QVDG_MATH_FP32, QVDG_MATH_TENSOR, or QVDG_MATH_GATES: plain passes
+   * (staged = 0) apply a fused group of 4-5 qubits member gate by member
+   * gate in registers instead of as its product matrix. */
   uint32_t math;
 } qvdg_options;
 

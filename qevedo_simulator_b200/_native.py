@@ -134,14 +134,15 @@ def set_device(device: int):
     check(lib().qvdg_set_device(int(device)))
 
 
-MATH = {"fp32": 0, "tensor": 1}
+MATH = {"fp32": 0, "tensor": 1, "gates": 2}
 
 
 def options(max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0, planner: int = 0,
             math: str = "fp32") -> QvdgOptions:
     """Simulator options (the reference's Options, src/simulator.rs:37-66).
     `math="tensor"` runs the staged path's fused 3-6 qubit gates on the
-    tensor cores (complex64 states only)."""
+    tensor cores (complex64 states only); `math="gates"` makes plain passes
+    apply a fused 4-5 qubit group gate by gate in registers."""
     o = QvdgOptions()
     o.max_fused_qubits = int(max_fused_qubits)
     o.staged = 1 if staged else 0

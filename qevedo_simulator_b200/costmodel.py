@@ -43,6 +43,8 @@ def candidates() -> list:
     out = []
     for f in (2, 3, 4, 5):
         out.append((f"plain-f{f}", options(f, staged=False)))
+    for f in (4, 5):
+        out.append((f"plain-gates-f{f}", options(f, staged=False, math="gates")))
     out.append(("staged-cuda", options(4, staged=True)))
     for f in (4, 5):
         out.append((f"staged-tensor-f{f}", options(f, staged=True, math="tensor")))

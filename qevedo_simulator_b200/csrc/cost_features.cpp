@@ -35,6 +35,37 @@ void pass_features(const Target& t, const PlannedPass& p, const LoweredPass& lp,
   f[0] = 1.f;
   f[1] = float(t.n) / 32.f;
   f[30] = t.bits == 64 ? 1.f : 0.f;
+  if (lp.block) {
+    // A plain pass applying a fused group member by member (f[31] = 1).
+    f[2] = 1.f;
+    f[31] = 1.f;
+    f[6] = float(p.block_qubits.size()) / 6.f;
+    f[12] = 1.f;
+    f[14] = float(p.ops.size()) / 64.f;
+    uint32_t lo = 64, hi = 0, low4 = 0;
+    for (uint32_t q : p.block_qubits) {
+      const uint32_t ph = t.layout[q];
+      lo = std::min(lo, ph);
+      hi = std::max(hi, ph);
+      if (ph < 4) ++low4;
+    }
+    f[9] = float(lo) / 32.f;
+    f[10] = float(hi) / 32.f;
+    f[11] = float(low4) / 6.f;
+    int d1 = 0, diag = 0, realish = 0;
+    for (const HOp& op : p.ops) {
+      if (op.diagonal) {
+        ++diag;
+      } else {
+        ++d1;
+        if (real_like(op.matrix)) ++realish;
+      }
+    }
+    f[15] = float(d1) / 64.f;
+    f[18] = float(diag) / 64.f;
+    f[29] = float(realish) / 64.f;
+    return;
+  }
   if (!lp.staged) {
     const HOp& op = p.ops[0];
     f[2] = 1.f;

@@ -141,27 +141,34 @@ void grow(const std::vector<HOp>& ops, std::vector<bool>& done, size_t seed, std
 
 }  // namespace
 
-std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
-                            const std::function<bool(const HOp&)>& fusable) {
+std::vector<FusedGroup> fuse_groups(const std::vector<HOp>& ops, size_t max_qubits,
+                                    const std::function<bool(const HOp&)>& fusable) {
   const std::function<size_t(const HOp&)> width = [&](const HOp& op) {
     return fusable(op) ? op.width() : SIZE_MAX;
   };
   std::vector<bool> done(ops.size(), false);
-  std::vector<HOp> fused;
+  std::vector<FusedGroup> groups;
   for (size_t seed = 0; seed < ops.size(); ++seed) {
     if (done[seed]) continue;
     done[seed] = true;
-    std::vector<size_t> members{seed};
-    std::vector<uint32_t> qubits = ops[seed].qubits();
+    FusedGroup g;
+    g.members = {seed};
+    g.qubits = ops[seed].qubits();
     if (width(ops[seed]) <= max_qubits) {
-      grow(ops, done, seed, members, qubits, max_qubits, true, width);
-      grow(ops, done, seed, members, qubits, max_qubits, false, width);
+      grow(ops, done, seed, g.members, g.qubits, max_qubits, true, width);
+      grow(ops, done, seed, g.members, g.qubits, max_qubits, false, width);
     }
-    if (members.size() == 1) {
-      fused.push_back(ops[seed]);
-      continue;
-    }
-    std::sort(qubits.begin(), qubits.end());
+    std::sort(g.qubits.begin(), g.qubits.end());
+    groups.push_back(std::move(g));
+  }
+  return groups;
+}
+
+HOp fuse_group(const std::vector<HOp>& ops, const FusedGroup& g) {
+  const std::vector<size_t>& members = g.members;
+  const std::vector<uint32_t>& qubits = g.qubits;
+  if (members.size() == 1) return ops[members[0]];
+  {
     HMatrix m = HMatrix::identity(qubits.size());
     for (size_t i : members) {
       std::vector<uint32_t> oq;
@@ -173,8 +180,14 @@ std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
     f.targets = qubits;
     f.matrix = std::move(m);
     f.diagonal = f.matrix.is_diagonal();
-    fused.push_back(std::move(f));
+    return f;
   }
+}
+
+std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
+                            const std::function<bool(const HOp&)>& fusable) {
+  std::vector<HOp> fused;
+  for (const FusedGroup& g : fuse_groups(ops, max_qubits, fusable)) fused.push_back(fuse_group(ops, g));
   return fused;
 }
 

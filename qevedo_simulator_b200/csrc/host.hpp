@@ -51,6 +51,21 @@ struct HOp {
   void full(std::vector<uint32_t>& qs, HMatrix& m) const;
 };
 
+// A fused group: its member ops (indices, program order) and their qubits
+// (ascending).
+struct FusedGroup {
+  std::vector<size_t> members;
+  std::vector<uint32_t> qubits;
+};
+
+// The groups of the greedy fusion below (src/fusion.rs:63-170).
+std::vector<FusedGroup> fuse_groups(const std::vector<HOp>& ops, size_t max_qubits,
+                                    const std::function<bool(const HOp&)>& fusable);
+
+// The group's ops as one op (the product matrix on its qubits; a group of one
+// op is that op, controls kept).
+HOp fuse_group(const std::vector<HOp>& ops, const FusedGroup& g);
+
 // Greedy fusion; ops with !fusable(op) are never merged and block their qubits.
 std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
                             const std::function<bool(const HOp&)>& fusable);

@@ -376,6 +376,7 @@ bool tensor_pass_ok(const Target& s, const PlannedPass& p) {
 }
 
 LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig& cfg, StageUpload& up) {
+  if (p.block) return lower_block_pass(s, p, up);
   if (p.staged && cfg.tensor && cfg.low_bits >= 1 && tensor_pass_ok(s, p)) return lower_tensor_pass(s, p, cfg, up);
   if (p.staged && cfg.reg && cfg.low_bits >= 1 && register_pass_ok(s, p)) return lower_register_pass(s, p, cfg, up);
   LoweredPass lp;
@@ -461,6 +462,10 @@ LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig&
 }
 
 void launch_pass(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev) {
+  if (lp.block) {
+    launch_block(s, lp, dev);
+    return;
+  }
   if (!lp.staged) {
     launch_plain_gate(s, lp.plain, dev.mats);
     return;

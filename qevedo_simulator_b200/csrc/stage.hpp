@@ -28,7 +28,9 @@ namespace qvdg {
 struct PlannedPass {
   bool staged = true;
   std::vector<uint32_t> tile_bits;  // physical bits of the tile, ascending
-  std::vector<HOp> ops;             // fused ops of the stage (logical qubits)
+  std::vector<HOp> ops;             // fused ops of the stage (logical qubits); block: the group's member ops
+  bool block = false;               // one plain pass applying a fused group's member gates in registers
+  std::vector<uint32_t> block_qubits;  // block: the group's logical qubits
 };
 
 struct StageConfig {

@@ -45,6 +45,7 @@ struct TileGeom {
 
 struct LoweredPass {
   bool staged = true;
+  bool block = false;  // plain pass of k_block (geo.L = group qubits, geo.tile_bits = their physical bits)
   TileGeom geo{};
   size_t gate_offset = 0;  // first TileGate of this pass in the upload
   PlainGate plain;         // when !staged
@@ -74,6 +75,10 @@ struct Target;
 LoweredPass lower_pass(const Target& t, const PlannedPass& p, const StageConfig& cfg, StageUpload& up);
 void launch_pass(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
 void launch_stage_tc(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
+// Plain passes applying a fused group gate by gate in registers (block.cu).
+bool block_pass_ok(const Target& t, const std::vector<HOp>& members, const std::vector<uint32_t>& qubits);
+LoweredPass lower_block_pass(const Target& t, const PlannedPass& p, StageUpload& up);
+void launch_block(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
 // Register-blocked CUDA-core stages (stage_reg.cu): gates unfused, four tile
 // bits per register pass.
 bool register_pass_ok(const Target& s, const PlannedPass& p);

@@ -180,11 +180,25 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
   if (opt.staged) {
     passes = plan_stages(ops, t.layout, t.n, prog.cfg, max_fused);
   } else {
-    // One pass per fused op (src/simulator.rs:136-143).
-    for (HOp& op : fuse(ops, max_fused)) {
+    // One pass per fused op (src/simulator.rs:136-143). With the gates math,
+    // an eligible group is applied member by member in registers instead of
+    // as its product matrix.
+    const bool gates = opt.math == QVDG_MATH_GATES;
+    for (const FusedGroup& g : fuse_groups(ops, max_fused, [](const HOp&) { return true; })) {
       PlannedPass p;
       p.staged = false;
-      p.ops.push_back(std::move(op));
+      if (gates) {
+        std::vector<HOp> members;
+        for (size_t i : g.members) members.push_back(ops[i]);
+        if (block_pass_ok(t, members, g.qubits)) {
+          p.block = true;
+          p.block_qubits = g.qubits;
+          p.ops = std::move(members);
+          passes.push_back(std::move(p));
+          continue;
+        }
+      }
+      p.ops.push_back(fuse_group(ops, g));
       passes.push_back(std::move(p));
     }
   }
@@ -193,11 +207,11 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     prog.passes.push_back(lower_pass(t, p, prog.cfg, prog.upload));
     prog.features.resize(prog.features.size() + kPassFeatures);
     pass_features(t, p, prog.passes.back(), prog.upload, prog.features.data() + prog.features.size() - kPassFeatures);
-    prog.kernels += p.ops.size();
+    prog.kernels += p.block ? 1 : p.ops.size();
     double b = 2.0 * state_bytes;
     if (p.staged)
       ++prog.stages;
-    else
+    else if (!p.block)
       b /= double(uint64_t(1) << p.ops[0].controls.size());
     prog.pass_bytes.push_back(b);
     prog.bytes += b;

@@ -217,3 +217,30 @@ def test_tensor_core_circuits(oracle, kind):
             st.apply_ops(c.ops(), options(fuse, True, 0, math="tensor"))
             err = max_distance(st.amplitudes(), expected) / np.max(np.abs(expected))
         assert err < TC_CIRCUIT_TOL, (kind, fuse, err)
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+@pytest.mark.parametrize("kind", ["grid", "mixed", "qft", "gates"])
+def test_plain_passes_applying_groups_gate_by_gate(oracle, bits, kind):
+    """math="gates": each fused 4-5 qubit group runs as one pass that applies
+    its member gates in registers (merged diagonals as one phase vector or
+    sign mask, controls as pair masks); groups that do not qualify keep the
+    product-matrix kernel. Same results as the naive oracle."""
+    from qevedo_simulator_b200 import library
+
+    n = 15
+    if kind == "grid":
+        ops = library.random_grid_circuit(3, 5, 12, seed=4).ops()
+    elif kind == "mixed":
+        ops = library.mixed_ops(n, 8, seed=6)
+    elif kind == "qft":
+        ops = library.qft(n).ops()
+    else:
+        ops = library.random_gate_circuit(n, 150, seed=12).ops()
+    initial = random_state(np.random.Generator(np.random.PCG64(21)), n)
+    expected = oracle.naive_apply_ops(initial, ops)
+    for fuse in (4, 5):
+        with DeviceState(n, bits) as st:
+            st.set_amplitudes(initial)
+            stats = st.apply_ops(ops, options(fuse, staged=False, math="gates"))
+            assert max_distance(st.amplitudes(), expected) < TOL[bits] * 50, (kind, fuse, stats)
