@@ -190,6 +190,27 @@ qvdg_status qvdg_reset(qvdg_state* state, uint32_t qubit, double uniform);
 qvdg_status qvdg_sample_unordered(const qvdg_state* state, size_t shots, const double* uniforms,
                                   uint64_t* out, size_t* count);
 
+/* Sample `shots` outcomes as qvdg_sample_unordered does (same uniforms, same
+ * outcomes) and count them by classical key on the device: bit c of a key
+ * is the OR of the values measured into classical bit c over the
+ * (measure_qubits[i], measure_clbits[i]) pairs, as the reference's keyed
+ * counting builds it (classical bits 0..63; at most 64 distinct pairs). Distinct keys come back ascending
+ * with their counts (at most `capacity`; `*num_keys` receives how many
+ * there are). Reference: count_outcomes and counts_from_keys,
+ * src/simulator.rs:187-230 (the formatting of keys as bitstrings stays with
+ * the caller). */
+qvdg_status qvdg_sample_counts(const qvdg_state* state, size_t shots, const double* uniforms,
+                               const uint32_t* measure_qubits, const uint32_t* measure_clbits, size_t num_measures,
+                               uint64_t* keys, uint64_t* counts, size_t capacity, size_t* num_keys);
+
+/* <psi|P|psi> for the Pauli string P = product of paulis[i] ('X', 'Y', 'Z' or
+ * 'I') on qubits[i], summed in double precision (not normalised by the
+ * norm). Reference: the state-vector branch of the Qiskit Estimator,
+ * python/python/qevedo/simulator/qiskit.py:584-590 (expectation of a
+ * SparsePauliOp term by term). */
+qvdg_status qvdg_expect_pauli(const qvdg_state* state, const uint32_t* qubits, const char* paulis, size_t count,
+                              double* out);
+
 /* Exchange physical bit positions pairwise in one pass and relabel the
  * logical qubits that lived there. Reference: StateVector::swap_physical,
  * src/state.rs:212-268 (any bit positions are allowed here). */

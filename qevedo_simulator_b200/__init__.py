@@ -15,8 +15,8 @@ libqvdgpu.so behind the C ABI of include/qvdg.h; there is no CPU fallback.
 from . import library
 from ._native import Batch, DeviceState, Plan, QvdgError, options, set_device
 from .circuit import Circuit, Gate, Op, gate_op
-from .simulator import RunResult, count_outcomes, run, statevector
+from .simulator import RunResult, count_outcomes, estimate, run, statevector
 
 __all__ = ["Batch", "Circuit", "Gate", "Op", "gate_op", "DeviceState", "Plan", "QvdgError", "options", "set_device", "RunResult", "run",
-           "statevector", "count_outcomes", "library"]
+           "statevector", "count_outcomes", "estimate", "library"]
 __version__ = "0.1.0"

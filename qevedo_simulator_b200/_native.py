@@ -66,6 +66,10 @@ _SIGNATURES = {
     "qvdg_batch_info": (ct.c_int, [_P, ct.POINTER(QvdgBatchSummary)]),
     "qvdg_batch_tuning": (ct.c_int, [_P, ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_double),
                                      ct.c_size_t, ct.POINTER(ct.c_size_t)]),
+    "qvdg_sample_counts": (ct.c_int, [_P, ct.c_size_t, ct.POINTER(ct.c_double), ct.POINTER(ct.c_uint32),
+                                      ct.POINTER(ct.c_uint32), ct.c_size_t, ct.POINTER(ct.c_uint64),
+                                      ct.POINTER(ct.c_uint64), ct.c_size_t, ct.POINTER(ct.c_size_t)]),
+    "qvdg_expect_pauli": (ct.c_int, [_P, ct.POINTER(ct.c_uint32), ct.c_char_p, ct.c_size_t, ct.POINTER(ct.c_double)]),
     "qvdg_plan_features": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(QvdgOp), ct.c_size_t,
                                       ct.POINTER(QvdgOptions), ct.POINTER(ct.c_float), ct.c_size_t,
                                       ct.POINTER(ct.c_size_t)]),
@@ -265,6 +269,36 @@ class DeviceState:
         count = ct.c_size_t()
         check(lib().qvdg_sample_unordered(self._h, u.size, as_double_ptr(u), as_u64_ptr(out), ct.byref(count)))
         return out[:count.value]
+
+    def sample_counts(self, uniforms, measures):
+        """(keys, counts): distinct classical keys (ascending; bit c = the value
+        measured into classical bit c) of the shots sampled with `uniforms`,
+        for `measures` = [(qubit, clbit), ...] with clbits 0..63."""
+        u = np.ascontiguousarray(uniforms, dtype=np.float64)
+        q = np.array([m[0] for m in measures] or [0], dtype=np.uint32)
+        c = np.array([m[1] for m in measures] or [0], dtype=np.uint32)
+        n = ct.c_size_t()
+        args = (self._h, u.size, as_double_ptr(u), q.ctypes.data_as(ct.POINTER(ct.c_uint32)),
+                c.ctypes.data_as(ct.POINTER(ct.c_uint32)), len(measures))
+        check(lib().qvdg_sample_counts(*args, None, None, 0, ct.byref(n)))
+        keys = np.zeros(max(n.value, 1), dtype=np.uint64)
+        counts = np.zeros(max(n.value, 1), dtype=np.uint64)
+        check(lib().qvdg_sample_counts(*args, as_u64_ptr(keys), as_u64_ptr(counts), keys.size, ct.byref(n)))
+        return keys[:n.value], counts[:n.value]
+
+    def expect_pauli(self, label) -> float:
+        """<psi|P|psi> for a Pauli label in Qiskit order (rightmost letter =
+        qubit 0), or for [(qubit, letter), ...]."""
+        if isinstance(label, str):
+            pairs = [(i, ch) for i, ch in enumerate(reversed(label)) if ch.upper() != "I"]
+        else:
+            pairs = list(label)
+        q = np.array([p[0] for p in pairs] or [0], dtype=np.uint32)
+        letters = "".join(p[1] for p in pairs).encode()
+        v = ct.c_double()
+        check(lib().qvdg_expect_pauli(self._h, q.ctypes.data_as(ct.POINTER(ct.c_uint32)), letters, len(pairs),
+                                      ct.byref(v)))
+        return v.value
 
     def execute(self, plan: "Plan") -> dict:
         stats = QvdgStats()

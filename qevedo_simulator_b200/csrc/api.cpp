@@ -576,6 +576,54 @@ qvdg_status qvdg_bit_probabilities_noalloc(const void* amplitudes, uint32_t num_
   });
 }
 
+qvdg_status qvdg_sample_counts(const qvdg_state* st, size_t shots, const double* uniforms,
+                               const uint32_t* measure_qubits, const uint32_t* measure_clbits, size_t num_measures,
+                               uint64_t* keys, uint64_t* counts, size_t capacity, size_t* num_keys) {
+  return guarded([&] {
+    StateImpl& s = const_cast<StateImpl&>(impl(st));
+    require(shots == 0 || uniforms != nullptr, "null uniforms");
+    require(num_measures == 0 || (measure_qubits != nullptr && measure_clbits != nullptr), "null measurements");
+    for (size_t i = 0; i < num_measures; ++i) {
+      require(measure_qubits[i] < s.n, "measured qubit out of range");
+      require(measure_clbits[i] < 64, "classical bits beyond 63 are not supported by device counting");
+    }
+    for (size_t i = 0; i < shots; ++i) require(uniforms[i] >= 0.0 && uniforms[i] < 1.0, "uniforms must be in [0, 1)");
+    std::vector<uint64_t> k, c;
+    sample_counts(s, shots, uniforms, measure_qubits, measure_clbits, num_measures, k, c);
+    if (num_keys) *num_keys = k.size();
+    if (keys && counts)
+      for (size_t i = 0; i < std::min(capacity, k.size()); ++i) {
+        keys[i] = k[i];
+        counts[i] = c[i];
+      }
+  });
+}
+
+qvdg_status qvdg_expect_pauli(const qvdg_state* st, const uint32_t* qubits, const char* paulis, size_t count,
+                              double* out) {
+  return guarded([&] {
+    StateImpl& s = const_cast<StateImpl&>(impl(st));
+    require(out != nullptr, "null output");
+    require(count == 0 || (qubits != nullptr && paulis != nullptr), "null Pauli string");
+    uint64_t x = 0, z = 0, seen = 0;
+    int ny = 0;
+    for (size_t i = 0; i < count; ++i) {
+      require(qubits[i] < s.n, "qubit out of range");
+      const uint64_t bit = uint64_t(1) << s.layout[qubits[i]];
+      require(!(seen & bit), "a Pauli string names a qubit twice");
+      seen |= bit;
+      switch (paulis[i]) {
+        case 'X': case 'x': x |= bit; break;
+        case 'Z': case 'z': z |= bit; break;
+        case 'Y': case 'y': x |= bit; z |= bit; ++ny; break;
+        case 'I': case 'i': break;
+        default: throw Error(QVDG_ERR_INVALID, std::string("unknown Pauli `") + paulis[i] + "`");
+      }
+    }
+    *out = expect_pauli(s, x, z, ny);
+  });
+}
+
 qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
                                const qvdg_options* options, float* out, size_t capacity, size_t* num_passes) {
   return guarded([&] {

@@ -83,6 +83,12 @@ double norm_sqr(StateImpl& s);
 double probability_one(StateImpl& s, uint32_t physical_bit);
 // P(bit = 1) for every physical bit, and the total.
 void bit_probabilities(StateImpl& s, std::vector<double>& p1, double& total);
+// Sample and count by classical key (clbits < 64; logical measured qubits);
+// keys ascending.
+size_t sample_counts(StateImpl& s, size_t shots, const double* uniforms_host, const uint32_t* qubits,
+                     const uint32_t* clbits, size_t nm, std::vector<uint64_t>& keys, std::vector<uint64_t>& counts);
+// <psi|P|psi> for X/Y bits x, Z/Y bits z (physical) and ny Y factors.
+double expect_pauli(StateImpl& s, uint64_t x, uint64_t z, int ny);
 // bit_probabilities over a caller's device buffer, with file-scope scratch
 // instead of an allocated workspace (qvdg_bit_probabilities_noalloc).
 void bit_probabilities_noalloc(const void* amplitudes, uint32_t num_qubits, uint32_t precision_bits,

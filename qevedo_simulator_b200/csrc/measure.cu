@@ -447,9 +447,12 @@ void probabilities_t(StateImpl& s, double* out_host) {
   }
 }
 
+// The sampler's outcomes (logical indices) left in the workspace at *out_dev;
+// returns their number. The workspace's `keys` and `tmp` regions (shots
+// entries each) are free afterwards and returned for reuse.
 template <typename T>
-size_t sample_t(StateImpl& s, size_t shots, const double* uniforms_host, uint64_t* out_host) {
-  if (shots == 0) return 0;
+size_t sample_device_t(StateImpl& s, size_t shots, const double* uniforms_host, uint64_t** out_dev,
+                       uint64_t** keys_dev, uint64_t** tmp_dev) {
   const uint64_t len = s.size();
   // CHUNK_BLOCKS (4096) blocks of LANES amplitudes (8 for f32, 4 for f64).
   const uint64_t chunk_len = sizeof(T) == 4 ? 32768 : 16384;
@@ -520,9 +523,110 @@ size_t sample_t(StateImpl& s, size_t shots, const double* uniforms_host, uint64_
     k_remap<<<blocks_for(found, kThreads), kThreads, 0, s.stream>>>(out, found, tables, nt);
     QVDG_LAUNCH_CHECK();
   }
+  *out_dev = out;
+  *keys_dev = keys;
+  *tmp_dev = tmp;
+  return found;
+}
+
+template <typename T>
+size_t sample_t(StateImpl& s, size_t shots, const double* uniforms_host, uint64_t* out_host) {
+  if (shots == 0) return 0;
+  uint64_t *out = nullptr, *keys = nullptr, *tmp = nullptr;
+  const size_t found = sample_device_t<T>(s, shots, uniforms_host, &out, &keys, &tmp);
   if (found > 0) QVDG_CUDA(cudaMemcpyAsync(out_host, out, found * 8, cudaMemcpyDeviceToHost, s.stream));
   QVDG_CUDA(cudaStreamSynchronize(s.stream));
   return found;
+}
+
+// Classical keys of outcomes: bit c of key i = bit q of outcome i for each
+// (q, c) measurement (count_outcomes, src/simulator.rs:187-230).
+struct MeasureMap {
+  uint8_t q[64], c[64];
+  int32_t n;
+};
+
+__global__ void k_outcome_keys(const uint64_t* __restrict__ out, size_t found, const MeasureMap m,
+                               uint64_t* __restrict__ keys) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= found) return;
+  const uint64_t o = out[i];
+  uint64_t k = 0;
+  for (int j = 0; j < m.n; ++j) k |= ((o >> m.q[j]) & 1ull) << m.c[j];
+  keys[i] = k;
+}
+
+template <typename T>
+size_t counts_t(StateImpl& s, size_t shots, const double* uniforms_host, const MeasureMap& m,
+                std::vector<uint64_t>& keys_out, std::vector<uint64_t>& counts_out) {
+  keys_out.clear();
+  counts_out.clear();
+  if (shots == 0) return 0;
+  uint64_t *out = nullptr, *keys = nullptr, *tmp = nullptr;
+  const size_t found = sample_device_t<T>(s, shots, uniforms_host, &out, &keys, &tmp);
+  if (found == 0) return 0;
+  k_outcome_keys<<<blocks_for(found, kThreads), kThreads, 0, s.stream>>>(out, found, m, keys);
+  QVDG_LAUNCH_CHECK();
+  radix_sort_u64(keys, tmp, found, s.work2, s.stream);
+  std::vector<uint64_t> sorted(found);
+  QVDG_CUDA(cudaMemcpyAsync(sorted.data(), keys, found * 8, cudaMemcpyDeviceToHost, s.stream));
+  QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  for (size_t i = 0; i < found;) {
+    size_t j = i + 1;
+    while (j < found && sorted[j] == sorted[i]) ++j;
+    keys_out.push_back(sorted[i]);
+    counts_out.push_back(j - i);
+    i = j;
+  }
+  return found;
+}
+
+// <psi|P|psi> for a Pauli string with X/Y on the bits of x, Z/Y on the bits of
+// z (physical): P|j> = i^nY (-1)^popc(j & z) |j ^ x>, so the value is
+// i^nY * sum_j conj(psi[j ^ x]) psi[j] (-1)^popc(j & z). Per-block partial
+// sums (re, im) in double precision, summed in order.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_pauli(const cplx_t<T>* __restrict__ psi, uint64_t len, uint64_t x,
+                                                    uint64_t z, double* __restrict__ partials) {
+  __shared__ double red[32];
+  double re = 0.0, im = 0.0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < len; j += stride) {
+    const cplx_t<T> a = psi[j], b = psi[j ^ x];
+    // conj(b) * a
+    const double pr = double(b.x) * double(a.x) + double(b.y) * double(a.y);
+    const double pi = double(b.x) * double(a.y) - double(b.y) * double(a.x);
+    const double sgn = (__popcll(j & z) & 1) ? -1.0 : 1.0;
+    re += sgn * pr;
+    im += sgn * pi;
+  }
+  const double tr = block_sum(re, red);
+  __syncthreads();
+  const double ti = block_sum(im, red);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = tr;
+    partials[2 * blockIdx.x + 1] = ti;
+  }
+}
+
+template <typename T>
+double pauli_t(StateImpl& s, uint64_t x, uint64_t z, int ny) {
+  const unsigned blocks = unsigned(umin64(uint64_t(s.sms) * 8, std::max<uint64_t>(1, s.size() / kThreads)));
+  double* d = static_cast<double*>(s.work.get((2 * size_t(blocks) + 2) * sizeof(double)));
+  k_pauli<T><<<blocks, kThreads, 0, s.stream>>>(static_cast<const cplx_t<T>*>(s.amp), s.size(), x, z, d);
+  QVDG_LAUNCH_CHECK();
+  k_sum_columns<<<1, 32, 0, s.stream>>>(d, int(blocks), 2, d + 2 * blocks);
+  QVDG_LAUNCH_CHECK();
+  double* h = static_cast<double*>(s.host.get(2 * sizeof(double)));
+  QVDG_CUDA(cudaMemcpyAsync(h, d + 2 * blocks, 2 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+  QVDG_CUDA(cudaStreamSynchronize(s.stream));
+  const double re = h[0], im = h[1];
+  switch (ny & 3) {
+    case 0: return re;
+    case 1: return -im;
+    case 2: return -re;
+    default: return im;
+  }
 }
 
 }  // namespace
@@ -580,6 +684,27 @@ void probabilities(StateImpl& s, double* out_host) {
     probabilities_t<float>(s, out_host);
   else
     probabilities_t<double>(s, out_host);
+}
+
+size_t sample_counts(StateImpl& s, size_t shots, const double* uniforms_host, const uint32_t* qubits,
+                     const uint32_t* clbits, size_t nm, std::vector<uint64_t>& keys, std::vector<uint64_t>& counts) {
+  MeasureMap m{};
+  // Every pair ORs its bit into the key, as the reference's keyed counting
+  // does (src/simulator.rs:204-210); pairs repeated exactly are kept once.
+  for (size_t i = 0; i < nm && m.n < 64; ++i) {
+    bool dup = false;
+    for (int j = 0; j < m.n; ++j) dup = dup || (m.q[j] == qubits[i] && m.c[j] == clbits[i]);
+    if (dup) continue;
+    m.q[m.n] = uint8_t(qubits[i]);
+    m.c[m.n] = uint8_t(clbits[i]);
+    ++m.n;
+  }
+  return s.bits == 32 ? counts_t<float>(s, shots, uniforms_host, m, keys, counts)
+                      : counts_t<double>(s, shots, uniforms_host, m, keys, counts);
+}
+
+double expect_pauli(StateImpl& s, uint64_t x, uint64_t z, int ny) {
+  return s.bits == 32 ? pauli_t<float>(s, x, z, ny) : pauli_t<double>(s, x, z, ny);
 }
 
 size_t sample_unordered(StateImpl& s, size_t shots, const double* uniforms_host, uint64_t* out_host) {

@@ -138,8 +138,16 @@ def run(circuit: Circuit, shots: int = 1024, *, backend: str = "auto", seed: int
             result.stats = stats
             t0 = time.perf_counter()
             measures = [(i[1], i[2]) for i in circuit._instructions[split:] if i[0] == "measure"]
-            outcomes = st.sample_unordered(uniforms(rng, shots))
-            result.counts = count_outcomes(outcomes, measures, circuit.num_clbits)
+            if circuit.num_clbits <= 64:
+                # Keys built, sorted and counted on the device; only the
+                # distinct keys come back to be formatted.
+                keys, cnt = st.sample_counts(uniforms(rng, shots), measures)
+                result.counts = {bitstring([(int(k) >> c) & 1 for c in range(circuit.num_clbits)]): int(n)
+                                 for k, n in zip(keys, cnt)}
+                result.counts = dict(sorted(result.counts.items()))
+            else:
+                outcomes = st.sample_unordered(uniforms(rng, shots))
+                result.counts = count_outcomes(outcomes, measures, circuit.num_clbits)
             result.measure_seconds = time.perf_counter() - t0
             return result
         counts = {}
@@ -176,3 +184,21 @@ def run(circuit: Circuit, shots: int = 1024, *, backend: str = "auto", seed: int
     finally:
         if own:
             st.close()
+
+
+def estimate(circuit: Circuit, observable, *, precision: str = "double") -> float:
+    """<psi|O|psi> of the circuit's final state for O = sum of coeff * Pauli
+    string, given as {label: coeff} or [(label, coeff), ...] with Qiskit
+    labels (rightmost letter = qubit 0); each term is one device reduction.
+    The reference's Qiskit Estimator computes the same from its state vector
+    (python/python/qevedo/simulator/qiskit.py:584-590)."""
+    terms = observable.items() if isinstance(observable, dict) else observable
+    ops = circuit.ops()
+    with _native.DeviceState(circuit.num_qubits, _precision_bits(precision)) as st:
+        st.apply_ops(ops, _native.options(4, staged=False))
+        total = 0.0
+        for label, coeff in terms:
+            if len(label) != circuit.num_qubits:
+                raise ValueError(f"label `{label}` does not have {circuit.num_qubits} letters")
+            total += float(np.real(coeff)) * st.expect_pauli(label)
+        return total

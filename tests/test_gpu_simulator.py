@@ -229,3 +229,60 @@ def test_measure_and_reset_match_the_oracle(oracle):
                 assert max_distance(st.amplitudes(), o.amplitudes()) < 1e-6
                 st.reset(0, u)
                 assert st.probability_one(0) < 1e-12
+
+
+def test_device_counts_match_host_counting():
+    """qvdg_sample_counts: keys built, sorted and counted on the device equal
+    the host's count_outcomes of the same samples (count_outcomes,
+    src/simulator.rs:187-230), duplicate classical bits included (their
+    bits OR together, as in the reference's keyed counting)."""
+    from qevedo_simulator_b200 import library
+    from qevedo_simulator_b200.simulator import count_outcomes
+
+    rng = np.random.Generator(np.random.PCG64(3))
+    for n, measures, nclbits in [(10, [(q, q) for q in range(10)], 10), (12, [(0, 3), (5, 0), (11, 1)], 4),
+                                 (9, [(1, 0), (2, 0), (8, 2)], 3), (14, [], 2)]:
+        c = library.random_grid_circuit(*library.grid_shape(n), 6, seed=n)
+        with DeviceState(n, 32) as st:
+            st.apply_ops(c.ops(), options(4, True))
+            u = rng.random(20000)
+            outcomes = st.sample_unordered(u)
+            keys, counts = st.sample_counts(u, measures)
+        host = count_outcomes(outcomes, measures, nclbits)
+        dev = {"".join("1" if (int(k) >> b) & 1 else "0" for b in reversed(range(nclbits))): int(v)
+               for k, v in zip(keys, counts)}
+        assert dev == host and sum(dev.values()) == 20000
+        assert list(keys) == sorted(keys)
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_pauli_expectations_match_numpy(bits):
+    rng = np.random.Generator(np.random.PCG64(bits))
+    n = 9
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    mats = {"I": np.eye(2), "X": np.array([[0, 1], [1, 0]]), "Y": np.array([[0, -1j], [1j, 0]]),
+            "Z": np.diag([1, -1])}
+    with DeviceState(n, bits) as st:
+        st.set_amplitudes(psi)
+        st.swap_physical([(0, 5), (2, 7)])  # logical qubits stay where they are
+        for _ in range(25):
+            label = "".join(rng.choice(list("IXYZ"), size=n))
+            op = np.array([[1.0]])
+            for ch in label:  # leftmost letter = highest qubit
+                op = np.kron(op, mats[ch])
+            expected = float(np.real(np.vdot(psi, op @ psi)))
+            got = st.expect_pauli(label)
+            assert abs(got - expected) < (1e-12 if bits == 64 else 2e-6), (label, got, expected)
+        with pytest.raises(ValueError, match="twice"):
+            st.expect_pauli([(1, "X"), (1, "Z")])
+
+
+def test_estimate_sums_pauli_terms(oracle):
+    from qevedo_simulator_b200 import estimate, library
+
+    c = library.random_grid_circuit(3, 3, 6, seed=2)
+    psi = oracle.naive_statevector(c.ops(), 9)
+    z0 = np.where(np.arange(1 << 9) & 1, -1.0, 1.0)
+    expected = 0.5 * float(np.sum(np.abs(psi) ** 2 * z0)) + 2.0
+    assert estimate(c, {"IIIIIIIIZ": 0.5, "IIIIIIIII": 2.0}) == pytest.approx(expected, abs=1e-12)
