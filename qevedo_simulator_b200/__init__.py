@@ -12,11 +12,11 @@ libqvdgpu.so behind the C ABI of include/qvdg.h; there is no CPU fallback.
     ['00', '11']
 """
 
-from . import library
+from . import library, qasm
 from ._native import Batch, DeviceState, Plan, QvdgError, options, set_device
 from .circuit import Circuit, Gate, Op, gate_op
 from .simulator import RunResult, count_outcomes, estimate, run, statevector
 
 __all__ = ["Batch", "Circuit", "Gate", "Op", "gate_op", "DeviceState", "Plan", "QvdgError", "options", "set_device", "RunResult", "run",
-           "statevector", "count_outcomes", "estimate", "library"]
+           "statevector", "count_outcomes", "estimate", "library", "qasm"]
 __version__ = "0.1.0"

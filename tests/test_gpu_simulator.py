@@ -286,3 +286,26 @@ def test_estimate_sums_pauli_terms(oracle):
     z0 = np.where(np.arange(1 << 9) & 1, -1.0, 1.0)
     expected = 0.5 * float(np.sum(np.abs(psi) ** 2 * z0)) + 2.0
     assert estimate(c, {"IIIIIIIIZ": 0.5, "IIIIIIIII": 2.0}) == pytest.approx(expected, abs=1e-12)
+
+
+def test_qasm_teleportation_with_feedback_runs():
+    """An OpenQASM 3 teleportation (Pauli corrections as classical feedback,
+    run shot by shot on the device): qubit 2 ends in the state RY(0.9)|0>."""
+    from qevedo_simulator_b200 import qasm
+
+    program = """OPENQASM 3.0;
+        include "stdgates.inc";
+        qubit[3] q;
+        bit[3] c;
+        ry(0.9) q[0];
+        h q[1]; cx q[1], q[2];
+        cx q[0], q[1]; h q[0];
+        c[0] = measure q[0];
+        c[1] = measure q[1];
+        if (c[1]) x q[2];
+        if (c[0]) z q[2];
+        c[2] = measure q[2];"""
+    c = qasm.parse(program)
+    r = run(c, 4000, seed=11)
+    ones = sum(v for k, v in r.counts.items() if k[0] == "1")
+    assert abs(ones / 4000 - math.sin(0.45) ** 2) < 0.03
