@@ -45,10 +45,10 @@ namespace {
 
 constexpr int kVec = 16;  // >= max tile qubits + 1 (reduction vector)
 
-// Shared-memory position of tile element e: bits 4-7 are folded into bits
-// 0-3 so that every gate group's warp access touches 16 distinct 8-byte bank
-// pairs (two wavefronts per 32 amplitudes, the minimum).
-__device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 4) & 15u); }
+// Shared-memory position of tile element e: bits 5-7 are folded into bits
+// 1-3 so that gate groups above the lowest four bits reach all banks; bit 0
+// is kept, so element pairs 2v, 2v+1 stay one 16-byte slot (cp.async).
+__device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 4) & 14u); }
 
 struct TileMap {
   int kind;   // 0: local = global (in-shared circuits and pass A), 1: pass B
@@ -213,40 +213,26 @@ __device__ void reduce_tile(const float2* tile, int nb, const TileMap& map, int 
   __syncthreads();
 }
 
-// Tile <-> slot copies in 16-byte units (element pairs 2u, 2u+1, which are
-// adjacent in the slot because every tile keeps at least global bit 0, and
-// adjacent in shared memory because swz only flips bit 0 of the pair's
-// position when bit 4 of e is set). Four units per thread are in flight.
-constexpr int kCopyUnroll = 4;
-
-__device__ __forceinline__ void put_pair(float2* tile, uint32_t e, float4 v) {
-  const uint32_t p = swz(e);
-  float4* dst = reinterpret_cast<float4*>(tile + (p & ~1u));
-  *dst = (p & 1u) ? make_float4(v.z, v.w, v.x, v.y) : v;
-}
-
+// Tile <-> slot copies in 16-byte units (element pairs 2u, 2u+1: adjacent in
+// the slot because every tile keeps global bit 0, and one aligned slot in
+// shared memory because swz keeps bit 0).
 __device__ __forceinline__ float4 get_pair(const float2* tile, uint32_t e) {
-  const uint32_t p = swz(e);
-  const float4 v = *reinterpret_cast<const float4*>(tile + (p & ~1u));
-  return (p & 1u) ? make_float4(v.z, v.w, v.x, v.y) : v;
+  return *reinterpret_cast<const float4*>(tile + swz(e));
 }
 
-__device__ void load_tile(float2* tile, const float2* __restrict__ slot, const TileMap& map) {
+// The tile's 16-byte copies issued asynchronously (cp.async) into `tile`,
+// as one commit group.
+__device__ void issue_tile(float2* tile, const float2* __restrict__ slot, const TileMap& map) {
   const uint32_t units = 1u << (map.L - 1);
-  for (uint32_t u0 = threadIdx.x; u0 < units; u0 += kCopyUnroll * blockDim.x) {
-    float4 v[kCopyUnroll];
-#pragma unroll
-    for (int k = 0; k < kCopyUnroll; ++k) {
-      const uint32_t u = u0 + k * blockDim.x;
-      if (u < units) v[k] = __ldcs(reinterpret_cast<const float4*>(slot + map.global(2 * u)));
-    }
-#pragma unroll
-    for (int k = 0; k < kCopyUnroll; ++k) {
-      const uint32_t u = u0 + k * blockDim.x;
-      if (u < units) put_pair(tile, 2 * u, v[k]);
-    }
+  for (uint32_t u = threadIdx.x; u < units; u += blockDim.x) {
+    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(tile + swz(2 * u)));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(slot + map.global(2 * u)) : "memory");
   }
+  asm volatile("cp.async.commit_group;" ::: "memory");
 }
+
+__device__ __forceinline__ void commit_empty() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ void store_tile(const float2* tile, float2* __restrict__ slot, const TileMap& map) {
   const uint32_t units = 1u << (map.L - 1);
@@ -293,41 +279,62 @@ __global__ void __launch_bounds__(512) k_batch(const BatchCircuit* __restrict__ 
       __syncthreads();
       reduce_tile(tile, n, map, n, red, tmp, acc);
     } else {
-      // Two tile passes per layer over the slot in HBM.
-      const int r = 2 * L - n;
-      const uint32_t tiles = 1u << (n - L);
-      const uint32_t tsize = 1u << L;
+      // Two tile passes per layer over the slot in HBM, on tiles of
+      // Lw = L - 1 qubits: the CTA's shared tile holds two of them, so the
+      // next tile's copies fly (cp.async) while the current one is computed.
+      const int Lw = L - 1;
+      const int r = 2 * Lw - n;
+      const uint32_t tiles = 1u << (n - Lw);
+      const uint32_t tsize = 1u << Lw;
+      float2* buf[2] = {tile, tile + tsize};
       for (uint32_t l = 0; l < c.num_layers; ++l) {
         const bool last = l + 1 == c.num_layers;
         __syncthreads();
         load_mats(mats, gates + 4 * c.gates, int(l) * n, n, 0);
         __syncthreads();
-        for (uint32_t t = 0; t < tiles; ++t) {  // pass A: low L qubits
-          const TileMap map{0, 0, L, t};
+        // pass A: low Lw qubits
+        if (l > 0) issue_tile(buf[0], slot, TileMap{0, 0, Lw, 0});
+        for (uint32_t t = 0; t < tiles; ++t) {
+          const TileMap map{0, 0, Lw, t};
+          float2* cur = (t & 1u) ? buf[1] : buf[0];
           if (l == 0) {
             for (uint32_t e = threadIdx.x; e < tsize; e += blockDim.x)
-              tile[swz(e)] = make_float2((t == 0 && e == 0) ? 1.f : 0.f, 0.f);
+              cur[swz(e)] = make_float2((t == 0 && e == 0) ? 1.f : 0.f, 0.f);
           } else {
-            load_tile(tile, slot, map);
+            if (t + 1 < tiles)
+              issue_tile((t & 1u) ? buf[0] : buf[1], slot, TileMap{0, 0, Lw, t + 1});
+            else
+              commit_empty();
+            wait_prev();
           }
           __syncthreads();
-          apply_range(tile, L, 0, L, mats, int(c.entangler), 0, map);
-          store_tile(tile, slot, map);
+          apply_range(cur, Lw, 0, Lw, mats, int(c.entangler), 0, map);
+          store_tile(cur, slot, map);
+          __threadfence_block();
           __syncthreads();
         }
-        for (uint32_t t = 0; t < tiles; ++t) {  // pass B: high n-L qubits
-          const TileMap map{1, r, L, t};
-          load_tile(tile, slot, map);
+        // pass B: high n-Lw qubits (reads what pass A stored, after the barrier)
+        issue_tile(buf[0], slot, TileMap{1, r, Lw, 0});
+        for (uint32_t t = 0; t < tiles; ++t) {
+          const TileMap map{1, r, Lw, t};
+          float2* cur = (t & 1u) ? buf[1] : buf[0];
+          if (t + 1 < tiles)
+            issue_tile((t & 1u) ? buf[0] : buf[1], slot, TileMap{1, r, Lw, t + 1});
+          else
+            commit_empty();
+          wait_prev();
           __syncthreads();
-          // Local bits r..L-1 are global qubits L..n-1 (matrices at local index).
-          apply_range(tile, L, r, L, mats + 4 * (L - r), int(c.entangler), L, map);
+          // Local bits r..Lw-1 are global qubits Lw..n-1 (matrices at local index).
+          apply_range(cur, Lw, r, Lw, mats + 4 * (Lw - r), int(c.entangler), Lw, map);
           if (last) {
-            reduce_tile(tile, L, map, n, red, tmp, acc);
+            reduce_tile(cur, Lw, map, n, red, tmp, acc);
           } else {
-            store_tile(tile, slot, map);
+            store_tile(cur, slot, map);
+            __threadfence_block();
             __syncthreads();
           }
         }
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
       }
     }
     if (threadIdx.x < uint32_t(n)) out[c.out + threadIdx.x] = acc[0] - 2.0 * acc[1 + threadIdx.x];

@@ -47,9 +47,10 @@ void require(bool ok, const std::string& message) {
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Whether a tile shape can run every circuit: wide circuits need the pass-B
-// tile (high n-L qubits plus r >= 1 low ones) to fit, n <= 2L - 1.
-bool shape_fits(uint32_t max_qubits, int L) { return max_qubits <= uint32_t(L) || max_qubits <= uint32_t(2 * L - 1); }
+// Whether a tile shape can run every circuit: wide circuits (n > L) run on
+// tiles of L - 1 qubits and need the pass-B tile (high n-L+1 qubits plus
+// r >= 1 low ones) to fit, n <= 2(L - 1) - 1.
+bool shape_fits(uint32_t max_qubits, int L) { return max_qubits <= uint32_t(L) || max_qubits <= uint32_t(2 * L - 3); }
 
 uint64_t slot_elems_for(uint32_t max_qubits, int L) {
   return max_qubits > uint32_t(L) ? (uint64_t(1) << max_qubits) : 0;

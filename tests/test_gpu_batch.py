@@ -52,10 +52,12 @@ def test_small_batch_matches_the_naive_oracle(oracle):
 
 @pytest.mark.parametrize("tile,threads", [(12, 128), (13, 256), (14, 512)])
 def test_wide_circuits_match_the_per_circuit_path(tile, threads):
-    """Circuits wider than the tile run in HBM slots (two tile passes per
-    layer); compared with complex128 runs of the same circuits through
-    apply_ops on single states."""
-    specs = [(15, 3, 1), (17, 4, 2), (18, 2, 3), (20, 3, 4), (22, 2, 5), (tile + 1, 3, 6), (min(2 * tile - 2, 24), 2, 7)]
+    """Circuits wider than the tile run in HBM slots (two double-buffered
+    tile passes per layer on tiles of L - 1 qubits); compared with
+    complex128 runs of the same circuits through apply_ops on single
+    states."""
+    specs = [(15, 3, 1), (17, 4, 2), (18, 2, 3), (20, 3, 4), (min(22, 2 * tile - 3), 2, 5), (tile + 1, 3, 6),
+             (min(2 * tile - 3, 24), 2, 7)]
     circuits, expected = [], []
     for i, (w, layers, seed) in enumerate(specs):
         ent = "cz" if i == 2 else "cx"
