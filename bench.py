@@ -42,6 +42,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "30q random-circuit s & HBM GB/s vs peak, tuned vs plain GPU at <=1e-6 amp err"
+# DRAM bytes (read + write) per amplitude of one plain fused-gate pass
+# (k_dense<float,4,2,1>), from an ncu capture at 26 qubits: 536.9 MB read +
+# 476.7 MB written per launch over 2^26 amplitudes; a full-size launch
+# scales by its amplitude count.
+DENSE_TRAFFIC_BYTES_PER_AMP = (536.9e6 + 476.7e6) / 2 ** 26
 ROWS, COLS, DEPTH, SEED = 5, 6, 20, 2024
 SHOTS = 1000
 
@@ -339,9 +344,13 @@ def run_ours(args, rank: int, world: int):
     else:
         kernel = "k_stage_reg<float> (register-blocked stage)"
     traffic = args.traffic
+    if traffic is None and dom == 0:
+        traffic = DENSE_TRAFFIC_BYTES_PER_AMP * 2 ** n
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": kernel,
                 "peak_source": peaks["source"], "bytes_per_launch": per_launch, "avg_launch_s": avg,
+                "traffic_source": "ncu capture of the same kernel at 26 qubits, scaled by amplitudes"
+                if args.traffic is None and dom == 0 else ("--traffic" if args.traffic else None),
                 "launches_per_step": int(dsec.size // max(1, args.steps)),
                 "whole_run_gbs": info["bytes"] / step / 1e9}
     # Accuracy: tuned complex64 against a complex128 run of the same circuit.
