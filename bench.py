@@ -42,11 +42,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "30q random-circuit s & HBM GB/s vs peak, tuned vs plain GPU at <=1e-6 amp err"
-# DRAM bytes (read + write) per amplitude of one plain fused-gate pass
-# (k_dense<float,4,2,1>), from an ncu capture at 26 qubits: 536.9 MB read +
-# 476.7 MB written per launch over 2^26 amplitudes; a full-size launch
-# scales by its amplitude count.
-DENSE_TRAFFIC_BYTES_PER_AMP = (536.9e6 + 476.7e6) / 2 ** 26
+# DRAM bytes (read + write) per amplitude of one plain fused-gate pass, from
+# ncu captures at 26 qubits (2^26 amplitudes per launch; a full-size launch
+# scales by its amplitude count), by pass kind: 0 k_dense<float,4,2,1>
+# (536.9 MB read + 476.7 MB written), 2 k_dense_tc<6,0> (537.0 + 476.9 MB).
+TRAFFIC_BYTES_PER_AMP = {0: (536.9e6 + 476.7e6) / 2 ** 26, 2: (537.0e6 + 476.9e6) / 2 ** 26}
+KERNEL_OF_KIND = {0: "k_dense<float,K,...> (plain fused-gate pass, CUDA cores)",
+                  2: "k_dense_tc<K,...> (plain fused-gate pass, tensor cores)"}
 ROWS, COLS, DEPTH, SEED = 5, 6, 20, 2024
 SHOTS = 1000
 
@@ -245,7 +247,8 @@ def max_over_ranks(value: float, dist, device: str = "cuda") -> float:
 
 def choose_tuned(ops, n: int, st, fixed=None):
     """The tuned plan: the learned cost model's pick among the candidate plans
-    (plain per-gate passes at fusion 2-5, staged CUDA-core, staged tensor-core),
+    (plain per-gate passes at fusion 2-6 on the CUDA or the tensor cores,
+    staged CUDA-core, staged tensor-core),
     judged by measurement against the greedy default. Returns (name, options,
     {candidate: measured seconds}) -- every candidate is measured once so the
     line shows what the choice was between."""
@@ -332,25 +335,25 @@ def run_ours(args, rank: int, world: int):
     byt = np.concatenate(pass_b)
     kind = np.concatenate(pass_k)
     peaks = measured_peaks()
-    dom = 1 if sec[kind == 1].sum() >= sec[kind == 0].sum() else 0
+    dom = max((0, 1, 2), key=lambda k: sec[kind == k].sum())
     dsec, dbyt = sec[kind == dom], byt[kind == dom]
     avg = float(dsec.mean())
     per_launch = float(dbyt.mean())
     achieved = float(dbyt.sum() / dsec.sum() / 1e9)
-    if dom == 0:
-        kernel = "k_dense<float,K,...> (plain fused-gate pass)"
+    if dom != 1:
+        kernel = KERNEL_OF_KIND[dom]
     elif tuned_opts.math == 1:
         kernel = "k_stage_tc (tensor-core stage)"
     else:
         kernel = "k_stage_reg<float> (register-blocked stage)"
     traffic = args.traffic
-    if traffic is None and dom == 0:
-        traffic = DENSE_TRAFFIC_BYTES_PER_AMP * 2 ** n
+    if traffic is None and dom != 1:
+        traffic = TRAFFIC_BYTES_PER_AMP[dom] * 2 ** n
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": kernel,
                 "peak_source": peaks["source"], "bytes_per_launch": per_launch, "avg_launch_s": avg,
                 "traffic_source": "ncu capture of the same kernel at 26 qubits, scaled by amplitudes"
-                if args.traffic is None and dom == 0 else ("--traffic" if args.traffic else None),
+                if args.traffic is None and dom != 1 else ("--traffic" if args.traffic else None),
                 "launches_per_step": int(dsec.size // max(1, args.steps)),
                 "whole_run_gbs": info["bytes"] / step / 1e9}
     # Accuracy: tuned complex64 against a complex128 run of the same circuit.
@@ -365,7 +368,7 @@ def run_ours(args, rank: int, world: int):
     # from pinned memory, run, sample SHOTS shots, outcomes back to the host.
     e2e = []
     staged = bool(tuned_opts.staged)
-    math_name = "tensor" if tuned_opts.math == 1 else "fp32"
+    math_name = {0: "fp32", 1: "tensor", 2: "gates"}[int(tuned_opts.math)]
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         run(circuit.copy().measure_all(), SHOTS, seed=7 + i, max_fused_qubits=int(tuned_opts.max_fused_qubits),

@@ -88,9 +88,12 @@ typedef struct {
   uint32_t tile_qubits;
   /* QVDG_PLANNER_GREEDY or QVDG_PLANNER_LEARNED. */
   uint32_t planner;
-  /* QVDG_MATH_FP32, QVDG_MATH_TENSOR, or QVDG_MATH_GATES: plain passes
-   * (staged = 0) apply a fused group of 4-5 qubits member gate by member
-   * gate in registers instead of as its product matrix. */
+  /* QVDG_MATH_FP32: every gate on the CUDA cores. QVDG_MATH_TENSOR
+   * (complex64 only): fused dense gates of 3-6 qubits in staged tiles, or of
+   * 4-6 qubits in plain passes (staged = 0), run on the tensor cores as
+   * split-bf16 products (hi*hi + hi*lo + lo*hi) accumulated in fp32.
+   * QVDG_MATH_GATES: plain passes apply a fused group of 4-5 qubits member
+   * gate by member gate in registers instead of as its product matrix. */
   uint32_t math;
 } qvdg_options;
 
@@ -351,7 +354,8 @@ qvdg_status qvdg_batch_tuning(const qvdg_batch* batch, uint32_t* tile_qubits, ui
 qvdg_status qvdg_set_pass_timing(qvdg_state* state, int32_t enabled);
 
 /* Per-pass device seconds, algorithmic bytes and kind (1 staged tile pass,
- * 0 single-gate pass) of the last gate run; `*count` receives the number of
+ * 0 single-gate pass, 2 single-gate pass on the tensor cores) of the last
+ * gate run; `*count` receives the number of
  * passes, at most `capacity` entries are written. */
 qvdg_status qvdg_pass_times(const qvdg_state* state, double* seconds, double* bytes, int32_t* staged,
                             size_t capacity, size_t* count);

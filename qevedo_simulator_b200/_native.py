@@ -144,8 +144,9 @@ MATH = {"fp32": 0, "tensor": 1, "gates": 2}
 def options(max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0, planner: int = 0,
             math: str = "fp32") -> QvdgOptions:
     """Simulator options (the reference's Options, src/simulator.rs:37-66).
-    `math="tensor"` runs the staged path's fused 3-6 qubit gates on the
-    tensor cores (complex64 states only); `math="gates"` makes plain passes
+    `math="tensor"` runs fused dense gates on the tensor cores (complex64
+    states only): 3-6 qubit gates inside staged tiles, 4-6 qubit gates as
+    plain passes; `math="gates"` makes plain passes
     apply a fused 4-5 qubit group gate by gate in registers."""
     o = QvdgOptions()
     o.max_fused_qubits = int(max_fused_qubits)
@@ -309,7 +310,9 @@ class DeviceState:
         check(lib().qvdg_set_pass_timing(self._h, 1 if enabled else 0))
 
     def pass_times(self):
-        """(seconds, bytes, staged) per pass of the last gate run."""
+        """(seconds, bytes, kind) per pass of the last gate run; kind 1 is a
+        staged tile pass, 0 a single-gate pass, 2 a single-gate pass on the
+        tensor cores."""
         count = ct.c_size_t()
         check(lib().qvdg_pass_times(self._h, None, None, None, 0, ct.byref(count)))
         n = count.value

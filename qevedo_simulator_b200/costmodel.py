@@ -1,7 +1,7 @@
 """Learned cost model: an MLP that predicts each planned pass's device time,
-used to choose among candidate plans (plain one-pass-per-gate, staged on the
-CUDA cores, staged on the tensor cores; fusion widths 2-6) before running
-any of them.
+used to choose among candidate plans (plain one-pass-per-gate on the CUDA
+cores or the tensor cores, staged on the CUDA cores, staged on the tensor
+cores; fusion widths 2-6) before running any of them.
 
 There is no learned planner in the reference: it plans with fixed greedy
 rules (fusion in src/fusion.rs:63-170, stages in src/blocking.rs:151-302,
@@ -45,6 +45,8 @@ def candidates() -> list:
         out.append((f"plain-f{f}", options(f, staged=False)))
     for f in (4, 5):
         out.append((f"plain-gates-f{f}", options(f, staged=False, math="gates")))
+    for f in (4, 5, 6):
+        out.append((f"plain-tensor-f{f}", options(f, staged=False, math="tensor")))
     out.append(("staged-cuda", options(4, staged=True)))
     for f in (4, 5):
         out.append((f"staged-tensor-f{f}", options(f, staged=True, math="tensor")))

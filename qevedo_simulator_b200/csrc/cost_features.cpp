@@ -83,6 +83,9 @@ void pass_features(const Target& t, const PlannedPass& p, const LoweredPass& lp,
     f[10] = float(hi) / 32.f;
     f[11] = float(low4) / 6.f;
     f[12] = float(std::ldexp(1.0, -int(op.controls.size())));
+    // On the tensor-core plain pass: one tensor-core gate of its width (the
+    // staged tensor passes' per-width counts).
+    if (lp.plain.tensor) f[op.targets.size() == 4 ? 22 : 23] = 1.f / 16.f;
     return;
   }
   const int kind = int(lp.geo.tensor);  // 2 register, 1 tensor, 0 shared-memory

@@ -33,6 +33,8 @@ struct PlainGate {
   std::vector<uint32_t> targets;                      // physical, matrix bit j = targets[j]
   std::vector<std::pair<uint32_t, bool>> controls;    // physical
   size_t matrix_offset = 0;  // element offset (complex) of its matrix / diagonal in the upload
+  bool tensor = false;       // dense, on the tensor-core plain pass (targets ascending)
+  size_t tc_offset = 0;      // tensor: byte offset of its bf16 matrices in the tensor-core blob
 };
 
 struct StateImpl {
@@ -53,7 +55,7 @@ struct StateImpl {
   bool record_passes = false;
   std::vector<cudaEvent_t> pass_events;
   std::vector<double> pass_seconds, pass_bytes;
-  std::vector<int> pass_kinds;  // 1 staged tile pass, 0 plain gate pass
+  std::vector<int> pass_kinds;  // 1 staged tile pass, 0 plain gate pass, 2 plain pass on the tensor cores
 
   size_t elem_bytes() const { return bits == 32 ? 8 : 16; }
   uint64_t size() const { return uint64_t(1) << n; }

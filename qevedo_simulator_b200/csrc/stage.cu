@@ -11,6 +11,7 @@
 #include <cstring>
 
 #include "program.hpp"
+#include "dense_tc.hpp"
 #include "stage.hpp"
 #include "stage_kernel.hpp"
 #include "tile_ops.cuh"
@@ -391,6 +392,28 @@ LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig&
       if (op.targets.size() > QVDG_MAX_DIAGONAL_QUBITS)
         throw Error(QVDG_ERR_UNSUPPORTED, "diagonal gates on more than 10 qubits are not supported");
       g.matrix_offset = up.push_matrix(op.matrix.diagonal_entries());
+    } else if (cfg.plain_tensor && dense_tc_ok(s.n, s.bits, g.targets, g.controls.size())) {
+      // Targets ascending, the matrix permuted to match: new index bit i is
+      // old bit order[i].
+      const size_t k = g.targets.size(), D = op.matrix.dim;
+      std::vector<size_t> order(k);
+      for (size_t i = 0; i < k; ++i) order[i] = i;
+      std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return g.targets[a] < g.targets[b]; });
+      std::vector<uint32_t> sorted(k);
+      for (size_t i = 0; i < k; ++i) sorted[i] = g.targets[order[i]];
+      auto old_index = [&](size_t h) {
+        size_t o = 0;
+        for (size_t i = 0; i < k; ++i) o |= ((h >> i) & 1) << order[i];
+        return o;
+      };
+      HMatrix m(D);
+      for (size_t r = 0; r < D; ++r)
+        for (size_t c = 0; c < D; ++c) m.at(r, c) = op.matrix.at(old_index(r), old_index(c));
+      g.targets = sorted;
+      g.tensor = true;
+      blob_align(up.tc);
+      g.tc_offset = up.tc.size();
+      append_tc_gate(m, up.tc);
     } else {
       if (op.targets.size() > QVDG_MAX_GATE_QUBITS)
         throw Error(QVDG_ERR_UNSUPPORTED, "dense gates on more than 6 qubits are not supported");
@@ -467,7 +490,10 @@ void launch_pass(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev) {
     return;
   }
   if (!lp.staged) {
-    launch_plain_gate(s, lp.plain, dev.mats);
+    if (lp.plain.tensor)
+      launch_dense_tc(s, lp.plain, dev.tc);
+    else
+      launch_plain_gate(s, lp.plain, dev.mats);
     return;
   }
   if (lp.geo.tensor == 2)

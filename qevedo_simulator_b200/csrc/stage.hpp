@@ -38,6 +38,7 @@ struct StageConfig {
   uint32_t low_bits;   // B
   bool tensor;         // fused 3-6 qubit gates on the tensor cores
   bool reg;            // CUDA-core stages gate by gate in registers (unfused)
+  bool plain_tensor;   // plain passes: fused 4-6 qubit dense gates on the tensor cores
 };
 
 struct Target;

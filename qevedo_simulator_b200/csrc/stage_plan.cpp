@@ -176,6 +176,7 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
   prog.gates = ops.size();
   const size_t max_fused = std::max<uint32_t>(opt.max_fused_qubits, 1);
   prog.cfg = stage_config(t, opt.tile_qubits, opt.staged && opt.math == QVDG_MATH_TENSOR);
+  prog.cfg.plain_tensor = !opt.staged && opt.math == QVDG_MATH_TENSOR && t.bits == 32;
   std::vector<PlannedPass> passes;
   if (opt.staged) {
     passes = plan_stages(ops, t.layout, t.n, prog.cfg, max_fused);
@@ -263,13 +264,14 @@ void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_s
   QVDG_CUDA(cudaEventRecord(s.ev_stop, s.stream));
   QVDG_CUDA(cudaStreamSynchronize(s.stream));
   bool tensor = false;
-  for (const LoweredPass& lp : p.passes) tensor = tensor || (lp.staged && lp.geo.tensor == 1);
+  for (const LoweredPass& lp : p.passes)
+    tensor = tensor || (lp.staged ? lp.geo.tensor == 1 : lp.plain.tensor);
   if (tensor) {
     int flag = 0;
     QVDG_CUDA(cudaMemcpy(&flag, s.status, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) {
       QVDG_CUDA(cudaMemset(s.status, 0, sizeof(int)));
-      throw Error(QVDG_ERR_TIMEOUT, "a tensor-core stage gave up waiting for its matrix products");
+      throw Error(QVDG_ERR_TIMEOUT, "a tensor-core pass gave up waiting for its matrix products");
     }
   }
   float ms = 0.f;
@@ -281,7 +283,7 @@ void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_s
       float t = 0.f;
       QVDG_CUDA(cudaEventElapsedTime(&t, s.pass_events[i], s.pass_events[i + 1]));
       s.pass_seconds.push_back(double(t) * 1e-3);
-      s.pass_kinds.push_back(p.passes[i].staged ? 1 : 0);
+      s.pass_kinds.push_back(p.passes[i].staged ? 1 : (p.passes[i].plain.tensor ? 2 : 0));
     }
     s.pass_bytes = p.pass_bytes;
   }

@@ -17,6 +17,11 @@ def test_features_describe_each_pass():
         if name.startswith("plain"):
             assert np.all(f[:, 2] == 1.0)
             assert np.all(f[:, 6] > 0)  # targets
+            tensor = f[:, 22] + f[:, 23] > 0
+            if name.startswith("plain-tensor"):
+                assert np.any(tensor) and np.all(f[tensor, 6] >= 4 / 6 - 1e-6)
+            else:
+                assert not np.any(tensor)
         elif name == "staged-cuda":
             assert np.all(f[:, 3] == 1.0) and np.all(f[:, 26] > 0)  # register passes
         else:
@@ -36,3 +41,32 @@ def test_mixed_ops_have_one_to_three_controls():
     controls = {len(o.controls) for o in ops if len(o.targets) == 1 and o.controls and
                 np.allclose(o.matrix, [[0, 1], [1, 0]])}
     assert controls >= {1, 2, 3}
+
+
+def test_tensor_core_plain_passes_are_planned_where_they_fit():
+    """math="tensor" without staging: dense fused gates of 4-6 qubits go to
+    the tensor-core plain pass on complex64 states when at least 8192
+    amplitudes stay selected (2^(n - controls) >= 2^13); narrower gates,
+    complex128 states and heavily controlled gates keep the CUDA-core pass."""
+    from qevedo_simulator_b200 import Op, options
+
+    rng = np.random.default_rng(3)
+
+    def unitary(k):
+        q, _ = np.linalg.qr(rng.normal(size=(2 ** k, 2 ** k)) + 1j * rng.normal(size=(2 ** k, 2 ** k)))
+        return q
+
+    def tensor_plain(ops, n, bits=32):
+        rows = costmodel.plan_features(ops, n, options(6, staged=False, math="tensor"), bits)
+        return [bool(r[2] == 1 and r[22] + r[23] > 0) for r in rows]
+
+    assert tensor_plain([Op([0, 1, 2, 3], [], unitary(4))], 13) == [True]
+    assert tensor_plain([Op([5, 1, 9, 3, 0, 7], [], unitary(6))], 20) == [True]
+    assert tensor_plain([Op([0, 1, 2], [], unitary(3))], 20) == [False]
+    assert tensor_plain([Op([0, 1, 2, 3], [], unitary(4))], 12) == [False]
+    assert tensor_plain([Op([0, 1, 2, 3], [(4, True)], unitary(4))], 13) == [False]
+    assert tensor_plain([Op([0, 1, 2, 3], [(4, True)], unitary(4))], 14) == [True]
+    assert tensor_plain([Op([0, 1, 2, 3], [], unitary(4))], 16, bits=64) == [False]
+    assert tensor_plain([Op([0, 1, 2, 3], [], np.diag(np.exp(1j * rng.normal(size=16))))], 16) == [False]
+    ops = library.random_grid_circuit(4, 4, 14, seed=31).ops()
+    assert sum(tensor_plain(ops, 16)) >= 10

@@ -219,6 +219,65 @@ def test_tensor_core_circuits(oracle, kind):
         assert err < TC_CIRCUIT_TOL, (kind, fuse, err)
 
 
+def _plain_tensor_passes(ops, n):
+    from qevedo_simulator_b200 import costmodel
+
+    rows = costmodel.plan_features(ops, n, options(6, staged=False, math="tensor"))
+    return int(np.sum((rows[:, 2] == 1) & (rows[:, 22] + rows[:, 23] > 0)))
+
+
+@pytest.mark.parametrize("n", [13, 14, 17])
+def test_tensor_core_plain_passes_single_gates(oracle, n):
+    """Plain passes of one fused 4-6 qubit gate on the tensor cores (bf16x3,
+    fp32 accumulation): targets in any order, on bit 0 (paired 16-byte
+    accesses) or not, low and high, with controls where at least 8192
+    amplitudes stay selected (otherwise the CUDA-core pass runs)."""
+    rng = np.random.Generator(np.random.PCG64(300 + n))
+    initial = random_state(rng, n)
+    layouts = [[0, 1, 2, 3], [3, 1, 0, 2, 4], [n - 1, 0, 5, 2, 7, 3], [4, 5, 6, 7], [n - 4, n - 3, n - 2, n - 1, 1],
+               [9, 2, 12, 6, 1, 8], [1, 2, 3, 4, 5, 6], [6, 0, 11, 3]]
+    used = 0
+    for qubits in layouts:
+        for controls in ([], [(max(qubits) + 1 if max(qubits) + 1 < n else min(set(range(n)) - set(qubits)),
+                               bool(rng.integers(2)))]):
+            m = random_unitary(rng, len(qubits))
+            ops = [Op(qubits, controls, m)]
+            used += _plain_tensor_passes(ops, n)
+            expected = oracle.naive_apply_ops(initial, ops)
+            with DeviceState(n, 32) as st:
+                st.set_amplitudes(initial)
+                st.apply_ops(ops, options(6, staged=False, math="tensor"))
+                err = max_distance(st.amplitudes(), expected) / np.max(np.abs(expected))
+            assert err < TC_REL_TOL, (n, qubits, controls, err)
+    assert used >= len(layouts)
+
+
+@pytest.mark.parametrize("kind", ["grid", "mixed", "qft", "gates"])
+def test_tensor_core_plain_circuits(oracle, kind):
+    """Whole circuits as plain passes with fused 4-6 qubit gates on the
+    tensor cores and the rest (diagonals, narrow or heavily controlled
+    gates) on the CUDA-core kernels."""
+    from qevedo_simulator_b200 import library
+
+    n = 16
+    if kind == "grid":
+        ops = library.random_grid_circuit(4, 4, 14, seed=31).ops()
+    elif kind == "mixed":
+        ops = library.mixed_ops(n, 8, seed=32)
+    elif kind == "qft":
+        ops = library.qft(n).ops()
+    else:
+        ops = library.random_gate_circuit(n, 150, seed=33).ops()
+    initial = random_state(np.random.Generator(np.random.PCG64(34)), n)
+    expected = oracle.naive_apply_ops(initial, ops)
+    for fuse in (4, 5, 6):
+        with DeviceState(n, 32) as st:
+            st.set_amplitudes(initial)
+            stats = st.apply_ops(ops, options(fuse, staged=False, math="tensor"))
+            err = max_distance(st.amplitudes(), expected) / np.max(np.abs(expected))
+        assert err < TC_CIRCUIT_TOL, (kind, fuse, err, stats)
+
+
 @pytest.mark.parametrize("bits", [32, 64])
 @pytest.mark.parametrize("kind", ["grid", "mixed", "qft", "gates"])
 def test_plain_passes_applying_groups_gate_by_gate(oracle, bits, kind):
