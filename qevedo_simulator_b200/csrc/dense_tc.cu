@@ -25,6 +25,12 @@
 // the tensor cores and the stores overlap. Every wait on an MMA completion
 // barrier is bounded: on timeout the kernel records an error, every thread
 // leaves the loop at the next CTA barrier and the tensor memory is freed.
+// Group bases advance by a running deposit (the carry of an add skips the
+// fixed bits), so no per-iteration bit insertion sits before the loads.
+//
+// Gates whose targets cover index bits 1-3 take a staged variant
+// (k_dense_tc_tile, below): there each group is a short contiguous run and
+// the direct kernel's warps would stride across runs.
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -43,6 +49,73 @@ constexpr int kThreads = 512;
 constexpr uint32_t kIterAmps = 8192;
 constexpr uint32_t kPartBytes = kIterAmps * 2 * 2;  // one bf16 part (hi or lo) of an iteration's A
 constexpr uint32_t kTmemCols = 256;                 // two buffers of 128 fp32 columns
+
+// One iteration's products, issued by one thread: for each of the T blocks
+// of 128 groups, D = A_hi B_hi + A_hi B_lo + A_lo B_hi into tensor-memory
+// columns `cols` + t * 2^(K+1), then one commit to `bar`.
+template <int K, uint32_t T = 4 / ((1u << K) / 16)>
+__device__ __forceinline__ void issue_products(const unsigned char* ah, const unsigned char* al,
+                                               const unsigned char* bmat, uint32_t cols, uint32_t bar) {
+  constexpr uint32_t D = 1u << K, kd = 2u * D;
+  constexpr uint32_t SBO = kd * 16, BLOCK = 128 * kd * 2, BPART = kd * kd * 2;
+  tc_fence_after();
+  const uint32_t idesc = umma_idesc(kd);
+  const uint64_t dah = umma_desc(smem_addr(ah), 128, SBO), dal = umma_desc(smem_addr(al), 128, SBO);
+  const uint64_t dbh = umma_desc(smem_addr(bmat), 128, SBO), dbl = umma_desc(smem_addr(bmat + BPART), 128, SBO);
+#pragma unroll
+  for (uint32_t t = 0; t < T; ++t) {
+    const uint32_t d = cols + t * kd;
+    const uint64_t boff = (t * BLOCK) >> 4;
+    uint32_t acc = 0;
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      const uint64_t a0 = (p == 2 ? dal : dah) + boff, b0 = p == 1 ? dbl : dbh;
+#pragma unroll
+      for (uint32_t s = 0; s < kd / 16; ++s) {
+        umma_bf16(d, a0 + 16 * s, b0 + 16 * s, idesc, acc);
+        acc = 1;
+      }
+    }
+  }
+  umma_commit(bar);
+}
+
+// Running deposit: with `cur` the deposit of an index into the positions
+// outside `mask` and `step` that of an increment, the deposit of the sum
+// (the carry skips the masked positions).
+__device__ __forceinline__ uint64_t dep_add(uint64_t cur, uint64_t step, uint64_t mask) {
+  return ((cur | mask) + step) & ~mask;
+}
+
+// Bounded wait for a completion barrier phase (about two seconds).
+__device__ __forceinline__ bool wait_products(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  bool done = mbar_try_wait(bar, parity);
+  while (!done && clock64() - t0 <= kWaitCycles) done = mbar_try_wait(bar, parity);
+  return done;
+}
+
+// Split 8 members (x[0..7], members 16 * chunk + 8 * q + i) of one group
+// into bf16 parts at row offset `row` of A.
+template <int K>
+__device__ __forceinline__ void write_a8(const float2* x, unsigned char* ah, unsigned char* al, uint32_t row,
+                                         uint32_t chunk, int q) {
+  constexpr uint32_t D = 1u << K;
+  float re[8], im[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    re[i] = x[i].x;
+    im[i] = x[i].y;
+  }
+  uint4 h, l;
+  const uint32_t cre = (2 * chunk + q) * 128, cim = (D / 8 + 2 * chunk + q) * 128;
+  split8(re, h, l);
+  *reinterpret_cast<uint4*>(ah + row + cre) = h;
+  *reinterpret_cast<uint4*>(al + row + cre) = l;
+  split8(im, h, l);
+  *reinterpret_cast<uint4*>(ah + row + cim) = h;
+  *reinterpret_cast<uint4*>(al + row + cim) = l;
+}
 
 template <int K, bool PAIR>
 __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ psi, const DenseTcGeom g,
@@ -96,9 +169,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ p
   // disjoint bits, so their deposits into the free positions OR together.
   const uint64_t tdep = insert_zeros(blk * 128 + r, fixed, g.num_fixed) | g.control_value | g.offsets[16 * chunk];
   const uint64_t my_iters = blockIdx.x < g.iters ? (g.iters - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  auto base_of = [&](uint64_t li) -> uint64_t {
-    const uint64_t it = blockIdx.x + li * gridDim.x;
-    return insert_zeros(it * GPI, fixed, g.num_fixed) | tdep;
+  // Iteration bases in load order and in store order, advanced by the
+  // deposit of gridDim.x * GPI.
+  uint64_t fmask = 0;
+  for (int i = 0; i < g.num_fixed; ++i) fmask |= uint64_t(1) << fixed[i];
+  const uint64_t dstep = insert_zeros(uint64_t(gridDim.x) * GPI, fixed, g.num_fixed);
+  uint64_t dload = insert_zeros(uint64_t(blockIdx.x) * GPI, fixed, g.num_fixed), dstore = dload;
+  auto next_load = [&]() -> uint64_t {
+    const uint64_t b = dload | tdep;
+    dload = dep_add(dload, dstep, fmask);
+    return b;
+  };
+  auto next_store = [&]() -> uint64_t {
+    const uint64_t b = dstore | tdep;
+    dstore = dep_add(dstore, dstep, fmask);
+    return b;
   };
   auto load = [&](float2 (&x)[16], uint64_t base) {
     if constexpr (PAIR) {
@@ -124,59 +209,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ p
     unsigned char* ah = abuf + b * 2 * kPartBytes;
     unsigned char* al = ah + kPartBytes;
     if (li < my_iters) {
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        float re[8], im[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          re[i] = x[8 * q + i].x;
-          im[i] = x[8 * q + i].y;
-        }
-        uint4 h, l;
-        const uint32_t cre = (2 * chunk + q) * 128, cim = (D / 8 + 2 * chunk + q) * 128;
-        split8(re, h, l);
-        *reinterpret_cast<uint4*>(ah + row + cre) = h;
-        *reinterpret_cast<uint4*>(al + row + cre) = l;
-        split8(im, h, l);
-        *reinterpret_cast<uint4*>(ah + row + cim) = h;
-        *reinterpret_cast<uint4*>(al + row + cim) = l;
-      }
-      if (li + 2 < my_iters) load(x, base_of(li + 2));
+      write_a8<K>(x, ah, al, row, chunk, 0);
+      write_a8<K>(x + 8, ah, al, row, chunk, 1);
+      if (li + 2 < my_iters) load(x, next_load());
       fence_async_shared();
     }
     tc_fence_before();
     if (__syncthreads_or(failed)) return false;
-    if (li < my_iters && tid == 0) {
-      tc_fence_after();
-      const uint32_t idesc = umma_idesc(kd);
-      const uint64_t dah = umma_desc(smem_addr(ah), 128, SBO), dal = umma_desc(smem_addr(al), 128, SBO);
-      const uint64_t dbh = umma_desc(smem_addr(bmat), 128, SBO), dbl = umma_desc(smem_addr(bmat + BPART), 128, SBO);
-#pragma unroll
-      for (uint32_t t = 0; t < T; ++t) {
-        const uint32_t d = tmem + b * 128 + t * kd;
-        const uint64_t boff = (t * BLOCK) >> 4;
-        uint32_t acc = 0;
-#pragma unroll
-        for (int p = 0; p < 3; ++p) {
-          const uint64_t a0 = (p == 2 ? dal : dah) + boff, b0 = p == 1 ? dbl : dbh;
-#pragma unroll
-          for (uint32_t s = 0; s < kd / 16; ++s) {
-            umma_bf16(d, a0 + 16 * s, b0 + 16 * s, idesc, acc);
-            acc = 1;
-          }
-        }
-      }
-      umma_commit(smem_addr(&bar[b]));
-    }
+    if (li < my_iters && tid == 0) issue_products<K>(ah, al, bmat, tmem + b * 128, smem_addr(&bar[b]));
     if (li > 0) {
       const uint32_t pb = b ^ 1u;
       const uint32_t parity = uint32_t(((li - 1) >> 1) & 1);
       const uint32_t barp = smem_addr(&bar[pb]);
-      const uint64_t base = base_of(li - 1);
-      const long long t0 = clock64();
-      bool done = mbar_try_wait(barp, parity);
-      while (!done && clock64() - t0 <= kWaitCycles) done = mbar_try_wait(barp, parity);
-      if (!done) {
+      const uint64_t base = next_store();
+      if (!wait_products(barp, parity)) {
         failed = 1;
         atomicExch(status, 1);
       } else {
@@ -205,8 +251,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ p
   // Two register sets in flight, so each iteration's loads are issued two
   // iterations ahead of their use.
   float2 xa[16], xb[16];
-  if (my_iters > 0) load(xa, base_of(0));
-  if (my_iters > 1) load(xb, base_of(1));
+  if (my_iters > 0) load(xa, next_load());
+  if (my_iters > 1) load(xb, next_load());
   for (uint64_t li = 0;; li += 2) {
     if (!step(li, xa)) break;
     if (!step(li + 1, xb)) break;
@@ -216,6 +262,205 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ p
   if (warp == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  }
+}
+
+// Gates with targets on index bits 1-3: a warp's 32 consecutive groups are
+// then scattered in memory, so the state moves through a shared-memory
+// stage instead. A CTA of 128 * 2^K / 16 threads takes tiles of 128 groups:
+// the 2^(7+K) amplitudes spanned by the bits `g.tile` (the targets and the
+// seven lowest free bits, bit 0 always among them, so a tile is contiguous
+// runs of at least 128 amplitudes). A tile is loaded with coalesced 16-byte
+// accesses (two tiles ahead, in registers) into the stage S, gathered per
+// group from S into A, multiplied, written back into S by the owning
+// threads and stored with coalesced 16-byte accesses. With two A and
+// tensor-memory buffers (NB = 2) a tile's products run while the previous
+// tile is read back and stored. Small CTAs let several run per SM (four for
+// K = 4, two for K = 5), so one CTA's barriers overlap another's memory
+// traffic. S position of tile element e: e ^ s(e), s(e) = (e >> 4 ^ e >> 8
+// ^ e >> 12) & 15, which keeps element pairs (2v, 2v + 1) in one 16-byte
+// slot (swapped when s(e) is odd) and spreads the group-parallel accesses
+// over the banks.
+__device__ __forceinline__ uint32_t stage_pos(uint32_t e) { return e ^ (((e >> 4) ^ (e >> 8) ^ (e >> 12)) & 15u); }
+
+template <int K>
+constexpr int tile_threads() {
+  return 128 * (1 << K) / 16;
+}
+
+template <int K, int NB>
+__global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_dense_tc_tile(float2* __restrict__ psi,
+                                                                     const DenseTcTileGeom g,
+                                                                     const uint8_t* __restrict__ bmats,
+                                                                     int* __restrict__ status) {
+  constexpr uint32_t D = 1u << K, kd = 2u * D;
+  constexpr int NT = tile_threads<K>();      // threads: 16 members of one group each
+  constexpr uint32_t TILE = 128 * D;         // amplitudes per tile
+  constexpr uint32_t PART = TILE * 2 * 2;    // bytes of one bf16 part of A
+  constexpr uint32_t SBO = kd * 16;
+  constexpr uint32_t BPART = kd * kd * 2;
+  constexpr int TB = 7 + K;                  // tile bits
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ uint8_t tile[16];
+  __shared__ uint64_t dep_hi[8];
+  float2* stage = reinterpret_cast<float2*>(smem);             // TILE complex64
+  unsigned char* abuf = smem + size_t(TILE) * sizeof(float2);  // NB x (A hi, A lo)
+  unsigned char* bmat = abuf + NB * 2 * PART;                  // B hi, then B lo
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t r = uint32_t(tid) & 127u, chunk = uint32_t(tid) >> 7;
+
+  if (tid == 0) {  // static indices: a parameter array indexed by tid would be copied to local memory
+#pragma unroll
+    for (int i = 0; i < 16; ++i) tile[i] = g.tile[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dep_hi[i] = g.dep_hi[i];
+  }
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(bmats + g.b_offset);
+    uint4* dst = reinterpret_cast<uint4*>(bmat);
+    for (uint32_t i = tid; i < 2 * BPART / 16; i += NT) dst[i] = src[i];
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[1])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  constexpr uint32_t kCols = NB * kd < 32 ? 32 : NB * kd;  // power of two, at least 32
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                 "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_async_shared();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  // Coalesced part: thread tid moves element pairs v = tid + NT j
+  // (j = 0..7): tile bits 1..K+3 from tid, K+4..K+6 from j.
+  uint64_t dep_t = 0, tmask = 0;
+#pragma unroll
+  for (int b = 1; b < K + 4; ++b)
+    if ((uint32_t(tid) >> (b - 1)) & 1u) dep_t |= uint64_t(1) << tile[b];
+#pragma unroll
+  for (int b = 0; b < TB; ++b) tmask |= uint64_t(1) << tile[b];
+  // Group part: this thread's members 16 * chunk + i of group r are tile
+  // elements eg | tm(i), tm(i) depositing i into the four lowest target
+  // positions.
+  uint32_t eg = 0;
+#pragma unroll
+  for (int i = 0; i < 7; ++i)
+    if ((r >> i) & 1u) eg |= 1u << g.fpos[i];
+#pragma unroll
+  for (int j = 4; j < K; ++j)
+    if ((chunk >> (j - 4)) & 1u) eg |= 1u << g.tpos[j];
+  const uint32_t t0 = 1u << g.tpos[0], t1 = 1u << g.tpos[1], t2 = 1u << g.tpos[2], t3 = 1u << g.tpos[3];
+  auto member = [&](int i) -> uint32_t {
+    return eg | ((i & 1) ? t0 : 0u) | ((i & 2) ? t1 : 0u) | ((i & 4) ? t2 : 0u) | ((i & 8) ? t3 : 0u);
+  };
+  const uint64_t my_iters = blockIdx.x < g.iters ? (g.iters - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // Tile bases in load order and in store order (running deposits of the
+  // tile index into the bits outside the tile).
+  const uint64_t dstep = insert_zeros(gridDim.x, tile, TB);
+  uint64_t dload = insert_zeros(blockIdx.x, tile, TB), dstore = dload;
+  auto load = [&](float4 (&x)[8]) {
+    const uint64_t base = dload | dep_t;
+    dload = dep_add(dload, dstep, tmask);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = ld_early(psi + (base | dep_hi[j]));
+  };
+  const uint32_t row = (r >> 3) * SBO + (r & 7) * 16;
+  const uint32_t lanes = (uint32_t(warp & 3) * 32u) << 16;
+  int failed = 0;
+  // One step: tile li into the stage and gathered into A, its products
+  // issued; then the products of tile li - 1 (NB = 2; the MMA ran during
+  // this step's first half) or of tile li itself (NB = 1) read back into
+  // the stage and stored.
+  auto step = [&](uint64_t li, float4 (&x)[8]) -> bool {
+    const bool have = li < my_iters;
+    const uint32_t b = NB == 2 ? uint32_t(li & 1) : 0u;
+    unsigned char* ah = abuf + b * 2 * PART;
+    unsigned char* al = ah + PART;
+    if (have) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint32_t e = 2u * (uint32_t(tid) + uint32_t(NT) * uint32_t(j));
+        const uint32_t pos = stage_pos(e);
+        const float4 v = x[j];
+        reinterpret_cast<float4*>(stage)[pos >> 1] = (pos & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
+      }
+      if (li + 2 < my_iters) load(x);
+    }
+    __syncthreads();
+    if (have) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        float2 m[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) m[i] = stage[stage_pos(member(8 * q + i))];
+        write_a8<K>(m, ah, al, row, chunk, q);
+      }
+      fence_async_shared();
+    }
+    tc_fence_before();
+    if (__syncthreads_or(failed)) return false;
+    if (have && tid == 0) issue_products<K, 1>(ah, al, bmat, tmem + b * kd, smem_addr(&bar[b]));
+    const bool back = NB == 2 ? li > 0 : have;
+    if (back) {
+      const uint64_t rl = NB == 2 ? li - 1 : li;
+      const uint32_t rb = NB == 2 ? uint32_t(rl & 1) : 0u;
+      const uint32_t parity = uint32_t((NB == 2 ? rl >> 1 : rl) & 1);
+      if (!wait_products(smem_addr(&bar[rb]), parity)) {
+        failed = 1;
+        atomicExch(status, 1);
+      } else {
+        tc_fence_after();
+        const uint32_t taddr = tmem + lanes + rb * kd + 16 * chunk;
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+          float re[8], im[8];
+          tmem_ld8(taddr + 8 * hh, re);
+          tmem_ld8(taddr + D + 8 * hh, im);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 8; ++i) stage[stage_pos(member(8 * hh + i))] = make_float2(re[i], im[i]);
+        }
+      }
+    }
+    tc_fence_before();
+    if (__syncthreads_or(failed)) return false;
+    if (back) {
+      const uint64_t base = dstore | dep_t;
+      dstore = dep_add(dstore, dstep, tmask);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint32_t e = 2u * (uint32_t(tid) + uint32_t(NT) * uint32_t(j));
+        const uint32_t pos = stage_pos(e);
+        float4 v = reinterpret_cast<const float4*>(stage)[pos >> 1];
+        if (pos & 1) v = make_float4(v.z, v.w, v.x, v.y);
+        *reinterpret_cast<float4*>(psi + (base | dep_hi[j])) = v;
+      }
+    }
+    __syncthreads();  // the stage is free for the next step
+    return NB == 2 ? have : li + 1 < my_iters;
+  };
+  float4 xa[8], xb[8];
+  if (my_iters > 0) load(xa);
+  if (my_iters > 1) load(xb);
+  if (my_iters > 0) {
+    for (uint64_t li = 0;; li += 2) {
+      if (!step(li, xa)) break;
+      if (!step(li + 1, xb)) break;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
   }
 }
 
@@ -232,6 +477,23 @@ void launch_k(StateImpl& s, const DenseTcGeom& g, const uint8_t* bmats) {
   QVDG_LAUNCH_CHECK();
 }
 
+// Two A and tensor-memory buffers where they fit in shared memory (K <= 5).
+template <int K>
+void launch_tile(StateImpl& s, const DenseTcTileGeom& g, const uint8_t* bmats) {
+  constexpr int NB = K <= 5 ? 2 : 1;
+  constexpr int NT = tile_threads<K>();
+  const size_t smem = (size_t(128) << K) * (sizeof(float2) + NB * 8) + tc_gate_bytes(K);
+  static int per_sm = 0;  // per instantiation
+  if (!per_sm) {
+    QVDG_CUDA(cudaFuncSetAttribute(k_dense_tc_tile<K, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    QVDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_tc_tile<K, NB>, NT, smem));
+    per_sm = std::max(per_sm, 1);
+  }
+  const unsigned grid = unsigned(std::min<uint64_t>(g.iters, uint64_t(s.sms) * uint64_t(per_sm)));
+  k_dense_tc_tile<K, NB><<<grid, NT, smem, s.stream>>>(static_cast<float2*>(s.amp), g, bmats, s.status);
+  QVDG_LAUNCH_CHECK();
+}
+
 }  // namespace
 
 bool dense_tc_ok(uint32_t n, int bits, const std::vector<uint32_t>& targets, size_t controls) {
@@ -245,6 +507,38 @@ void launch_dense_tc(StateImpl& s, const PlainGate& pg, const uint8_t* tc_blob) 
   const int k = int(pg.targets.size()), c = int(pg.controls.size());
   if (!dense_tc_ok(s.n, s.bits, pg.targets, size_t(c)) || !std::is_sorted(pg.targets.begin(), pg.targets.end()))
     throw Error(QVDG_ERR_INVALID, "internal: gate does not fit the tensor-core plain pass");
+  auto has = [&](uint32_t b) { return std::find(pg.targets.begin(), pg.targets.end(), b) != pg.targets.end(); };
+  if (c == 0 && s.n >= uint32_t(7 + k) && has(1) && has(2) && has(3)) {
+    // Bits 1-3 all targets: each group is a contiguous run of at least 8
+    // amplitudes and the direct kernel's warps stride by that run, so the
+    // state goes through the shared-memory stage. With fewer low targets
+    // the direct kernel is faster (measured on the 30-qubit grid circuit).
+    DenseTcTileGeom tg{};
+    std::vector<uint32_t> bits(pg.targets.begin(), pg.targets.end());
+    const int tb = 7 + k;
+    for (uint32_t b = 0; int(bits.size()) < tb; ++b)
+      if (std::find(pg.targets.begin(), pg.targets.end(), b) == pg.targets.end()) bits.push_back(b);
+    std::sort(bits.begin(), bits.end());
+    for (int i = 0; i < tb; ++i) tg.tile[i] = uint8_t(bits[i]);
+    int nf = 0;
+    for (int i = 0; i < tb; ++i) {
+      const auto it = std::find(pg.targets.begin(), pg.targets.end(), bits[i]);
+      if (it == pg.targets.end())
+        tg.fpos[nf++] = uint8_t(i);
+      else
+        tg.tpos[it - pg.targets.begin()] = uint8_t(i);
+    }
+    for (int j = 0; j < 8; ++j)
+      for (int b = 0; b < 3; ++b)
+        if ((j >> b) & 1) tg.dep_hi[j] |= uint64_t(1) << bits[k + 4 + b];
+    tg.iters = uint64_t(1) << (s.n - uint32_t(tb));
+    tg.b_offset = uint32_t(pg.tc_offset);
+    switch (k) {
+      case 4: return launch_tile<4>(s, tg, tc_blob);
+      case 5: return launch_tile<5>(s, tg, tc_blob);
+      default: return launch_tile<6>(s, tg, tc_blob);
+    }
+  }
   DenseTcGeom g{};
   std::vector<uint8_t> fixed;
   for (auto& cv : pg.controls) {

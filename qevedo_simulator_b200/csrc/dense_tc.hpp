@@ -19,6 +19,16 @@ struct DenseTcGeom {
   uint32_t b_offset;  // byte offset of the gate's bf16 matrices in the tensor-core blob
 };
 
+// The staged form for gates with targets on bits 1, 2 and 3 (no controls).
+struct DenseTcTileGeom {
+  uint64_t iters;      // tiles of 128 groups: 2^(n - 7 - K)
+  uint64_t dep_hi[8];  // physical offset of tile elements 2^(K+4) j (tile bits K+4..K+6)
+  uint32_t b_offset;   // byte offset of the gate's bf16 matrices in the tensor-core blob
+  uint8_t tile[16];    // physical positions of the 7 + K tile bits, ascending
+  uint8_t tpos[8];     // tile position of each target (matrix bit order)
+  uint8_t fpos[16];    // tile positions of the 7 free tile bits, ascending
+};
+
 // Whether a dense gate with these targets (physical) and controls runs on
 // the tensor-core plain pass: complex64, 4-6 targets, at least one CTA
 // iteration (8192 amplitudes) of selected groups, and the four lowest
