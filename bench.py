@@ -45,8 +45,8 @@ METRIC = "30q random-circuit s & HBM GB/s vs peak, tuned vs plain GPU at <=1e-6 
 # DRAM bytes (read + write) per amplitude of one plain fused-gate pass, from
 # ncu captures at 26 qubits (2^26 amplitudes per launch; a full-size launch
 # scales by its amplitude count), by pass kind: 0 k_dense<float,4,2,1>
-# (536.9 MB read + 476.7 MB written), 2 k_dense_tc<6,0> (537.0 + 476.9 MB).
-TRAFFIC_BYTES_PER_AMP = {0: (536.9e6 + 476.7e6) / 2 ** 26, 2: (537.0e6 + 476.9e6) / 2 ** 26}
+# (536.9 MB read + 476.7 MB written), 2 k_dense_tc<6,0> (537.0 + 476.5 MB).
+TRAFFIC_BYTES_PER_AMP = {0: (536.9e6 + 476.7e6) / 2 ** 26, 2: (537.0e6 + 476.5e6) / 2 ** 26}
 KERNEL_OF_KIND = {0: "k_dense<float,K,...> (plain fused-gate pass, CUDA cores)",
                   2: "k_dense_tc<K,...> (plain fused-gate pass, tensor cores)"}
 ROWS, COLS, DEPTH, SEED = 5, 6, 20, 2024
@@ -452,7 +452,7 @@ def run_qft(args):
         ref.apply_ops(ops, costmodel.options(4, staged=False))
         with DeviceState(n, 32) as st:
             for name, opts in costmodel.candidates():
-                if name not in ("plain-f4", "staged-cuda", "staged-tensor-f4", pick):
+                if name not in ("plain-f4", "plain-tensor-f6", "staged-cuda", "staged-tensor-f4", pick):
                     continue
                 with Plan(ops, n, 32, opts) as plan:
                     t, sec, byt = timed_plan(st, plan, psi0)
@@ -480,10 +480,11 @@ def grid_circuit_31():
 
 
 def run_precision(args):
-    """The precision form: grid circuits at 32 qubits complex64 (tensor-core
-    stages, 5-6 qubit fused matrices as bf16x3 products with fp32
-    accumulation) and 31 qubits complex128, 1M shots each; the error of
-    every complex64 path against an FP64 run at 28 qubits."""
+    """The precision form: grid circuits at 32 qubits complex64 (5-6 qubit
+    fused matrices on the tensor cores as bf16x3 products with fp32
+    accumulation: plain passes, and staged tiles for comparison) and 31
+    qubits complex128, 1M shots each; the error of every complex64 path
+    against an FP64 run at 28 qubits."""
     from qevedo_simulator_b200 import DeviceState, Plan, library, options
 
     out = {"metric": "precision form: seconds, 1M-shot sampling seconds, error vs FP64", "unit": "s",
@@ -493,7 +494,9 @@ def run_precision(args):
     with DeviceState(28, 64) as ref:
         ref.apply_ops(c28.ops(), options(4, staged=False))
         errs = {}
-        for name, opts in [("tensor-f5", options(5, True, math="tensor")), ("tensor-f4", options(4, True,
+        for name, opts in [("plain-tensor-f6", options(6, False, math="tensor")),
+                           ("plain-tensor-f5", options(5, False, math="tensor")),
+                           ("tensor-f5", options(5, True, math="tensor")), ("tensor-f4", options(4, True,
                            math="tensor")), ("fp32-staged", options(4, True)), ("fp32-plain", options(4, False))]:
             with DeviceState(28, 32) as st:
                 st.apply_ops(c28.ops(), opts)
@@ -503,7 +506,8 @@ def run_precision(args):
     u = rng.random(1_000_000)
     for label, circuit, bits, plans in [
             ("32q-c64", library.random_grid_circuit(4, 8, DEPTH, SEED), 32,
-             [("tensor-f5", options(5, True, math="tensor")), ("plain-f4", options(4, False))]),
+             [("plain-tensor-f6", options(6, False, math="tensor")), ("tensor-f5", options(5, True, math="tensor")),
+              ("plain-f4", options(4, False))]),
             ("31q-c128", grid_circuit_31(), 64,
              [("staged-fp64", options(4, True)), ("plain-f4", options(4, False))])]:
         n = circuit.num_qubits
@@ -522,7 +526,7 @@ def run_precision(args):
             run["norm_sqr"] = st.norm_sqr()
             run["shots"] = int(shots.size)
         out["runs"][label] = run
-    out["value"] = out["runs"]["32q-c64"]["tensor-f5"]["s"]
+    out["value"] = out["runs"]["32q-c64"]["plain-tensor-f6"]["s"]
     print(json.dumps(out), flush=True)
 
 
