@@ -486,8 +486,22 @@ void launch_tile(StateImpl& s, const DenseTcTileGeom& g, const uint8_t* bmats) {
   static int per_sm = 0;  // per instantiation
   if (!per_sm) {
     QVDG_CUDA(cudaFuncSetAttribute(k_dense_tc_tile<K, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    QVDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_tc_tile<K, NB>, NT, smem));
-    per_sm = std::max(per_sm, 1);
+    // All of the unified L1/shared storage as shared memory, so that several
+    // CTAs fit (the default carveout leaves room for one).
+    QVDG_CUDA(cudaFuncSetAttribute(k_dense_tc_tile<K, NB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   int(cudaSharedmemCarveoutMaxShared)));
+    // CTAs per SM from the kernel's registers and shared memory (the
+    // occupancy query reported one CTA here where four fit).
+    cudaFuncAttributes fa{};
+    QVDG_CUDA(cudaFuncGetAttributes(&fa, k_dense_tc_tile<K, NB>));
+    int dev = 0, smem_sm = 0, regs_sm = 0;
+    QVDG_CUDA(cudaGetDevice(&dev));
+    QVDG_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    QVDG_CUDA(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+    const int regs = (fa.numRegs + 7) / 8 * 8;
+    const int by_smem = smem_sm / int(smem + fa.sharedSizeBytes + 1024);
+    const int by_regs = regs_sm / (regs * NT);
+    per_sm = std::max(1, std::min({by_smem, by_regs, 2048 / NT}));
   }
   const unsigned grid = unsigned(std::min<uint64_t>(g.iters, uint64_t(s.sms) * uint64_t(per_sm)));
   k_dense_tc_tile<K, NB><<<grid, NT, smem, s.stream>>>(static_cast<float2*>(s.amp), g, bmats, s.status);
