@@ -72,41 +72,51 @@ class QvdgBatchSummary(ct.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+# numpy view of a qvdg_op (two uint32 counts, four pointers).
+_OP_DTYPE = np.dtype([("num_targets", "<u4"), ("num_controls", "<u4"), ("targets", "<u8"), ("controls", "<u8"),
+                      ("control_values", "<u8"), ("matrix", "<u8")])
+assert _OP_DTYPE.itemsize == ct.sizeof(QvdgOp)
+
+
 class PackedOps:
     """Ops laid out as a contiguous qvdg_op array; owns every buffer the
     structs point into, so it must outlive the call it is passed to."""
 
     def __init__(self, ops):
         n = len(ops)
-        self.array = (QvdgOp * max(n, 1))()
-        qubits = sum(len(op.targets) + len(op.controls) for op in ops)
-        self._q = np.zeros(max(qubits, 1), dtype=np.uint32)
-        self._v = np.zeros(max(qubits, 1), dtype=np.uint8)
-        sizes = [4 ** len(op.targets) for op in ops]
-        self._m = np.zeros(2 * max(sum(sizes), 1), dtype=np.float64)
-        qpos = mpos = 0
-        qbase = self._q.ctypes.data
-        vbase = self._v.ctypes.data
-        mbase = self._m.ctypes.data
+        qubits, values, mats = [], [], []
+        ks = np.empty(max(n, 1), dtype=np.uint32)
+        cs = np.empty(max(n, 1), dtype=np.uint32)
         for i, op in enumerate(ops):
             k, c = len(op.targets), len(op.controls)
-            self._q[qpos:qpos + k] = op.targets
-            for j, (q, v) in enumerate(op.controls):
-                self._q[qpos + k + j] = q
-                self._v[qpos + k + j] = 1 if v else 0
+            ks[i], cs[i] = k, c
+            qubits.extend(op.targets)
+            values.extend([0] * k)
+            for q, v in op.controls:
+                qubits.append(q)
+                values.append(1 if v else 0)
             m = np.ascontiguousarray(op.matrix, dtype=np.complex128).reshape(-1)
-            if m.size != sizes[i]:
+            if m.size != 4 ** k:
                 raise ValueError("op matrix does not match its targets")
-            self._m[2 * mpos:2 * (mpos + m.size)] = m.view(np.float64)
-            s = self.array[i]
-            s.num_targets = k
-            s.num_controls = c
-            s.targets = ct.cast(qbase + 4 * qpos, ct.POINTER(ct.c_uint32))
-            s.controls = ct.cast(qbase + 4 * (qpos + k), ct.POINTER(ct.c_uint32))
-            s.control_values = ct.cast(vbase + qpos + k, ct.POINTER(ct.c_uint8))
-            s.matrix = ct.cast(mbase + 16 * mpos, ct.POINTER(ct.c_double))
-            qpos += k + c
-            mpos += m.size
+            mats.append(m)
+        self._q = np.array(qubits or [0], dtype=np.uint32)
+        self._v = np.array(values or [0], dtype=np.uint8)
+        self._m = np.concatenate(mats).view(np.float64) if mats else np.zeros(2)
+        self._ops = np.zeros(max(n, 1), dtype=_OP_DTYPE)
+        if n:
+            ks, cs = ks[:n], cs[:n]
+            qpos = np.concatenate(([0], np.cumsum(ks.astype(np.uint64) + cs)[:-1])).astype(np.uint64)
+            sizes = np.uint64(4) ** ks.astype(np.uint64)
+            mpos = np.concatenate(([0], np.cumsum(sizes)[:-1])).astype(np.uint64)
+            qbase, vbase, mbase = (np.uint64(a.ctypes.data) for a in (self._q, self._v, self._m))
+            o = self._ops[:n]
+            o["num_targets"] = ks
+            o["num_controls"] = cs
+            o["targets"] = qbase + np.uint64(4) * qpos
+            o["controls"] = qbase + np.uint64(4) * (qpos + ks)
+            o["control_values"] = vbase + qpos + ks
+            o["matrix"] = mbase + np.uint64(16) * mpos
+        self.array = (QvdgOp * max(n, 1)).from_buffer(self._ops)
         self.count = n
 
 

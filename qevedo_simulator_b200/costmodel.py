@@ -63,11 +63,12 @@ def plan_features(ops, num_qubits: int, opts, precision_bits: int = 32) -> np.nd
     """Per-pass feature rows of the plan `opts` builds for `ops` (host only)."""
     packed = PackedOps(ops)
     count = ct.c_size_t()
-    check(lib().qvdg_plan_features(num_qubits, precision_bits, packed.array, packed.count, ct.byref(opts), None, 0,
-                                   ct.byref(count)))
-    rows = np.zeros((max(count.value, 1), FEATURES), dtype=np.float32)
+    # A plan has at most one pass per op: one call fills every row.
+    rows = np.zeros((max(len(ops), 1), FEATURES), dtype=np.float32)
     check(lib().qvdg_plan_features(num_qubits, precision_bits, packed.array, packed.count, ct.byref(opts),
                                    _fptr(rows), rows.shape[0], ct.byref(count)))
+    if count.value > rows.shape[0]:
+        raise RuntimeError("more passes than ops")
     return rows[:count.value]
 
 

@@ -1,7 +1,11 @@
 // Host gate algebra and greedy fusion (see host.hpp for the reference map).
 #include "host.hpp"
 
+#include <atomic>
+#include <exception>
+#include <mutex>
 #include <stdexcept>
+#include <thread>
 
 namespace qvdg {
 
@@ -164,6 +168,54 @@ std::vector<FusedGroup> fuse_groups(const std::vector<HOp>& ops, size_t max_qubi
   return groups;
 }
 
+// m <- embed(g, gate_qubits -> qubits) * m without forming the embedded
+// matrix: each set of rows that differ only in the gate's bits is mixed by g.
+// Same products, same zero skipping and same order of additions (ascending
+// row of the embedded matrix) as mul, so the result is identical.
+void apply_left(HMatrix& m, const HMatrix& g, const std::vector<uint32_t>& gate_qubits,
+                const std::vector<uint32_t>& qubits) {
+  const size_t k = gate_qubits.size(), gd = size_t(1) << k;
+  std::vector<size_t> off(gd, 0);
+  size_t mask = 0;
+  for (size_t j = 0; j < k; ++j) {
+    const size_t p = size_t(std::find(qubits.begin(), qubits.end(), gate_qubits[j]) - qubits.begin());
+    if (p == qubits.size()) throw std::logic_error("qubit missing from embedding");
+    mask |= size_t(1) << p;
+    for (size_t t = 0; t < gd; ++t)
+      if ((t >> j) & 1) off[t] |= size_t(1) << p;
+  }
+  std::vector<size_t> order(gd);
+  for (size_t t = 0; t < gd; ++t) order[t] = t;
+  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return off[a] < off[b]; });
+  // Nonzero entries of g by output row, each row's in ascending embedded column.
+  struct Entry {
+    size_t t;
+    C x;
+  };
+  std::vector<std::vector<Entry>> rows(gd);
+  for (size_t s = 0; s < gd; ++s)
+    for (size_t t : order)
+      if (norm2(g.at(s, t)) != 0.0) rows[s].push_back({t, g.at(s, t)});
+  const size_t dim = m.dim;
+  std::vector<C> in(gd * dim);
+  for (size_t b = 0; b < dim; ++b) {
+    if (b & mask) continue;
+    for (size_t t = 0; t < gd; ++t) std::copy_n(&m.a[(b | off[t]) * dim], dim, &in[t * dim]);
+    for (size_t s = 0; s < gd; ++s) {
+      C* dst = &m.a[(b | off[s]) * dim];
+      for (size_t c = 0; c < dim; ++c) dst[c] = {0.0, 0.0};
+      for (const Entry& e : rows[s]) {
+        const C* src = &in[e.t * dim];
+        for (size_t c = 0; c < dim; ++c) {
+          const C p = e.x * src[c];
+          dst[c].re += p.re;
+          dst[c].im += p.im;
+        }
+      }
+    }
+  }
+}
+
 HOp fuse_group(const std::vector<HOp>& ops, const FusedGroup& g) {
   const std::vector<size_t>& members = g.members;
   const std::vector<uint32_t>& qubits = g.qubits;
@@ -174,7 +226,7 @@ HOp fuse_group(const std::vector<HOp>& ops, const FusedGroup& g) {
       std::vector<uint32_t> oq;
       HMatrix om;
       ops[i].full(oq, om);
-      m = om.embed(oq, qubits).mul(m);
+      apply_left(m, om, oq, qubits);
     }
     HOp f;
     f.targets = qubits;
@@ -189,6 +241,33 @@ std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
   std::vector<HOp> fused;
   for (const FusedGroup& g : fuse_groups(ops, max_qubits, fusable)) fused.push_back(fuse_group(ops, g));
   return fused;
+}
+
+void parallel_for(size_t n, const std::function<void(size_t)>& f, unsigned threads) {
+  if (threads == 0) threads = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+  threads = unsigned(std::min<size_t>(threads, n));
+  if (threads <= 1) {
+    for (size_t i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::exception_ptr error;
+  std::mutex error_mutex;
+  auto work = [&] {
+    for (size_t i; (i = next.fetch_add(1)) < n;) {
+      try {
+        f(i);
+      } catch (...) {
+        std::lock_guard<std::mutex> lock(error_mutex);
+        if (!error) error = std::current_exception();
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < threads; ++t) pool.emplace_back(work);
+  work();
+  for (std::thread& t : pool) t.join();
+  if (error) std::rethrow_exception(error);
 }
 
 std::vector<HOp> fuse(const std::vector<HOp>& ops, size_t max_qubits) {

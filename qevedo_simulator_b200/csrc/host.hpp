@@ -71,4 +71,8 @@ std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
                             const std::function<bool(const HOp&)>& fusable);
 std::vector<HOp> fuse(const std::vector<HOp>& ops, size_t max_qubits);
 
+// f(0) .. f(n - 1) on up to `threads` host threads (0: the hardware's
+// count, at most 16); the first exception thrown is rethrown here.
+void parallel_for(size_t n, const std::function<void(size_t)>& f, unsigned threads = 0);
+
 }  // namespace qvdg

@@ -259,64 +259,64 @@ __global__ void k_active(const uint64_t* __restrict__ bounds, uint64_t nchunks, 
   if (lo < hi) active[atomicAdd(count, 1u)] = uint32_t(c);
 }
 
-// Pass 2: each lane walks one chunk that holds shots (src/measure.rs:134-167).
+// Pass 2: one warp per chunk that holds shots (src/measure.rs:134-167). The
+// warp computes the chunk's probabilities a window at a time (coalesced, the
+// next window while the current one is folded) into shared memory, and lane
+// 0 folds them in index order exactly as the reference does: one
+// sequential f64 sum from prefix[chunk], emitting an index while the next
+// target is below the running sum.
+constexpr int kWalkWarps = 4;
+constexpr int kWalkPerLane = 8;
+constexpr int kWalkWindow = 32 * kWalkPerLane;
+
 template <typename T>
-__global__ void __launch_bounds__(32 * kSampWarps) k_walk(const cplx_t<T>* __restrict__ psi, uint64_t len,
+__global__ void __launch_bounds__(32 * kWalkWarps) k_walk(const cplx_t<T>* __restrict__ psi, uint64_t len,
                                                           uint64_t chunk_len, const uint32_t* __restrict__ active,
                                                           const uint32_t* __restrict__ num_active,
                                                           const double* __restrict__ prefix,
                                                           const uint64_t* __restrict__ bounds, size_t shots,
                                                           const double* __restrict__ targets,
                                                           uint64_t* __restrict__ out) {
-  constexpr int W = Step<T>::width;
-  __shared__ double sp[kSampWarps][32][W + 1];
+  __shared__ double sp[kWalkWarps][2][kWalkWindow];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t first = (blockIdx.x * kSampWarps + warp) * 32;
-  const uint32_t total_active = *num_active;
-  if (first >= total_active) return;
-  const int live = int(umin64(32, total_active - first));
-  uint64_t chunk = 0, shot = 0, hi = 0, last_nonzero = 0;
-  double cumulative = 0.0;
-  bool walking = false;
-  if (lane < live) {
-    chunk = active[first + lane];
-    shot = bounds[chunk];
-    hi = umin64(bounds[chunk + 1], shots);
-    cumulative = prefix[chunk];
-    last_nonzero = chunk * chunk_len;
-    walking = shot < hi;
-  }
-  for (uint64_t pos = 0; pos < chunk_len; pos += W) {
-    const unsigned busy = __ballot_sync(0xffffffffu, walking);
-    if (!busy) break;
-    for (int c = 0; c < live; ++c) {
-      if (!((busy >> c) & 1)) continue;
-      const uint64_t cc = __shfl_sync(0xffffffffu, chunk, c);
-      const uint64_t base = cc * chunk_len + pos;
+  const uint32_t a = blockIdx.x * kWalkWarps + warp;
+  if (a >= *num_active) return;
+  const uint64_t chunk = active[a];
+  const uint64_t base = chunk * chunk_len;
+  const uint64_t end = umin64(chunk_len, len - base);
+  const uint64_t hi = umin64(bounds[chunk + 1], shots);
+  uint64_t shot = bounds[chunk];
+  uint64_t last_nonzero = base;
+  double cumulative = prefix[chunk];
+  auto fill = [&](uint64_t pos, int buf) {
 #pragma unroll
-      for (int e = 0; e < Step<T>::per_lane; ++e) {
-        const uint64_t off = uint64_t(lane) * Step<T>::per_lane + e;
-        sp[warp][c][off] = (base + off < len && pos + off < chunk_len) ? prob<T>(psi[base + off]) : 0.0;
-      }
+    for (int e = 0; e < kWalkPerLane; ++e) {
+      const uint64_t off = pos + uint64_t(lane + 32 * e);
+      sp[warp][buf][lane + 32 * e] = off < end ? prob<T>(psi[base + off]) : 0.0;
     }
-    __syncwarp();
-    if (walking) {
-      for (int j = 0; j < W; ++j) {
-        const double p = sp[warp][lane][j];
+  };
+  bool walking = shot < hi;
+  if (walking) fill(0, 0);
+  __syncwarp();
+  int buf = 0;
+  for (uint64_t pos = 0; walking && pos < end; pos += kWalkWindow) {
+    if (pos + kWalkWindow < end) fill(pos + kWalkWindow, buf ^ 1);
+    if (lane == 0) {
+      for (int j = 0; j < kWalkWindow; ++j) {
+        const double p = sp[warp][buf][j];
         if (p == 0.0) continue;
-        const uint64_t index = chunk * chunk_len + pos + j;
+        const uint64_t index = base + pos + uint64_t(j);
         last_nonzero = index;
         cumulative = __dadd_rn(cumulative, p);
         while (shot < hi && targets[shot] < cumulative) out[shot++] = index;
-        if (shot == hi) {
-          walking = false;
-          break;
-        }
+        if (shot == hi) break;
       }
     }
+    walking = __shfl_sync(0xffffffffu, shot < hi ? 1 : 0, 0) != 0;
     __syncwarp();
+    buf ^= 1;
   }
-  if (lane < live)
+  if (lane == 0)
     for (; shot < hi; ++shot) out[shot] = umin64(last_nonzero, len - 1);
 }
 
@@ -510,8 +510,8 @@ size_t sample_device_t(StateImpl& s, size_t shots, const double* uniforms_host, 
   const size_t found = size_t(umin64(hb[0], shots));
   const uint32_t num_active = *hc;
   if (num_active > 0) {
-    const unsigned walk_blocks = unsigned((num_active + 32 * kSampWarps - 1) / (32 * kSampWarps));
-    k_walk<T><<<walk_blocks, 32 * kSampWarps, 0, s.stream>>>(psi, len, chunk_len, active, count, prefix, bounds,
+    const unsigned walk_blocks = unsigned((num_active + kWalkWarps - 1) / kWalkWarps);
+    k_walk<T><<<walk_blocks, 32 * kWalkWarps, 0, s.stream>>>(psi, len, chunk_len, active, count, prefix, bounds,
                                                             shots, targets, out);
     QVDG_LAUNCH_CHECK();
   }

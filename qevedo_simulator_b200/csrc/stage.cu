@@ -376,7 +376,39 @@ bool tensor_pass_ok(const Target& s, const PlannedPass& p) {
   return true;
 }
 
-LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig& cfg, StageUpload& up) {
+bool plain_tc_eligible(const Target& s, const PlannedPass& p, const StageConfig& cfg) {
+  if (p.staged || p.block || !cfg.plain_tensor || p.ops[0].diagonal) return false;
+  std::vector<uint32_t> targets;
+  for (uint32_t q : p.ops[0].targets) targets.push_back(s.layout[q]);
+  return dense_tc_ok(s.n, s.bits, targets, p.ops[0].controls.size());
+}
+
+PlainTcBlob plain_tc_blob(const Target& s, const HOp& op) {
+  // Targets ascending, the matrix permuted to match: new index bit i is old
+  // bit order[i].
+  const size_t k = op.targets.size(), D = op.matrix.dim;
+  std::vector<uint32_t> phys;
+  for (uint32_t q : op.targets) phys.push_back(s.layout[q]);
+  std::vector<size_t> order(k);
+  for (size_t i = 0; i < k; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return phys[a] < phys[b]; });
+  PlainTcBlob b;
+  for (size_t i = 0; i < k; ++i) b.targets.push_back(phys[order[i]]);
+  std::vector<size_t> old_index(D);
+  for (size_t h = 0; h < D; ++h) {
+    size_t o = 0;
+    for (size_t i = 0; i < k; ++i) o |= ((h >> i) & 1) << order[i];
+    old_index[h] = o;
+  }
+  HMatrix m(D);
+  for (size_t r = 0; r < D; ++r)
+    for (size_t c = 0; c < D; ++c) m.at(r, c) = op.matrix.at(old_index[r], old_index[c]);
+  append_tc_gate(m, b.blob);
+  return b;
+}
+
+LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig& cfg, StageUpload& up,
+                       const PlainTcBlob* pre) {
   if (p.block) return lower_block_pass(s, p, up);
   if (p.staged && cfg.tensor && cfg.low_bits >= 1 && tensor_pass_ok(s, p)) return lower_tensor_pass(s, p, cfg, up);
   if (p.staged && cfg.reg && cfg.low_bits >= 1 && register_pass_ok(s, p)) return lower_register_pass(s, p, cfg, up);
@@ -392,28 +424,13 @@ LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig&
       if (op.targets.size() > QVDG_MAX_DIAGONAL_QUBITS)
         throw Error(QVDG_ERR_UNSUPPORTED, "diagonal gates on more than 10 qubits are not supported");
       g.matrix_offset = up.push_matrix(op.matrix.diagonal_entries());
-    } else if (cfg.plain_tensor && dense_tc_ok(s.n, s.bits, g.targets, g.controls.size())) {
-      // Targets ascending, the matrix permuted to match: new index bit i is
-      // old bit order[i].
-      const size_t k = g.targets.size(), D = op.matrix.dim;
-      std::vector<size_t> order(k);
-      for (size_t i = 0; i < k; ++i) order[i] = i;
-      std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return g.targets[a] < g.targets[b]; });
-      std::vector<uint32_t> sorted(k);
-      for (size_t i = 0; i < k; ++i) sorted[i] = g.targets[order[i]];
-      auto old_index = [&](size_t h) {
-        size_t o = 0;
-        for (size_t i = 0; i < k; ++i) o |= ((h >> i) & 1) << order[i];
-        return o;
-      };
-      HMatrix m(D);
-      for (size_t r = 0; r < D; ++r)
-        for (size_t c = 0; c < D; ++c) m.at(r, c) = op.matrix.at(old_index(r), old_index(c));
-      g.targets = sorted;
+    } else if (plain_tc_eligible(s, p, cfg)) {
+      const PlainTcBlob b = pre ? *pre : plain_tc_blob(s, op);
+      g.targets = b.targets;
       g.tensor = true;
       blob_align(up.tc);
       g.tc_offset = up.tc.size();
-      append_tc_gate(m, up.tc);
+      up.tc.insert(up.tc.end(), b.blob.begin(), b.blob.end());
     } else {
       if (op.targets.size() > QVDG_MAX_GATE_QUBITS)
         throw Error(QVDG_ERR_UNSUPPORTED, "dense gates on more than 6 qubits are not supported");

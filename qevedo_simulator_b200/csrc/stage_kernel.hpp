@@ -72,7 +72,17 @@ struct StageUpload {
 };
 
 struct Target;
-LoweredPass lower_pass(const Target& t, const PlannedPass& p, const StageConfig& cfg, StageUpload& up);
+// A plain pass's gate for the tensor-core kernel: targets (physical)
+// ascending and its bf16 matrices permuted to match.
+struct PlainTcBlob {
+  std::vector<uint32_t> targets;
+  std::vector<uint8_t> blob;
+};
+bool plain_tc_eligible(const Target& t, const PlannedPass& p, const StageConfig& cfg);
+PlainTcBlob plain_tc_blob(const Target& t, const HOp& op);
+// `pre`: the pass's plain_tc_blob when the caller computed it already.
+LoweredPass lower_pass(const Target& t, const PlannedPass& p, const StageConfig& cfg, StageUpload& up,
+                       const PlainTcBlob* pre = nullptr);
 void launch_pass(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
 void launch_stage_tc(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
 // Plain passes applying a fused group gate by gate in registers (block.cu).

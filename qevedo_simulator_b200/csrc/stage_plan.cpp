@@ -184,9 +184,14 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     // One pass per fused op (src/simulator.rs:136-143). With the gates math,
     // an eligible group is applied member by member in registers instead of
     // as its product matrix.
+    // The groups' product matrices are independent: built on host threads.
     const bool gates = opt.math == QVDG_MATH_GATES;
-    for (const FusedGroup& g : fuse_groups(ops, max_fused, [](const HOp&) { return true; })) {
-      PlannedPass p;
+    const std::vector<FusedGroup> groups = fuse_groups(ops, max_fused, [](const HOp&) { return true; });
+    passes.resize(groups.size());
+    std::vector<size_t> products;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+      const FusedGroup& g = groups[gi];
+      PlannedPass& p = passes[gi];
       p.staged = false;
       if (gates) {
         std::vector<HOp> members;
@@ -195,17 +200,27 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
           p.block = true;
           p.block_qubits = g.qubits;
           p.ops = std::move(members);
-          passes.push_back(std::move(p));
           continue;
         }
       }
-      p.ops.push_back(fuse_group(ops, g));
-      passes.push_back(std::move(p));
+      p.ops.resize(1);
+      products.push_back(gi);
     }
+    const bool wide = max_fused >= 5 && products.size() >= 8;
+    parallel_for(products.size(), [&](size_t j) { passes[products[j]].ops[0] = fuse_group(ops, groups[products[j]]); },
+                 wide ? 0u : 1u);
   }
+  // Tensor-core plain passes' bf16 matrices, also on host threads.
+  std::vector<PlainTcBlob> blobs(passes.size());
+  std::vector<size_t> tc;
+  for (size_t i = 0; i < passes.size(); ++i)
+    if (plain_tc_eligible(t, passes[i], prog.cfg)) tc.push_back(i);
+  parallel_for(tc.size(), [&](size_t j) { blobs[tc[j]] = plain_tc_blob(t, passes[tc[j]].ops[0]); },
+               tc.size() >= 8 ? 0u : 1u);
   const double state_bytes = double(uint64_t(t.bits == 32 ? 8 : 16) << t.n);
-  for (const PlannedPass& p : passes) {
-    prog.passes.push_back(lower_pass(t, p, prog.cfg, prog.upload));
+  for (size_t pi = 0; pi < passes.size(); ++pi) {
+    const PlannedPass& p = passes[pi];
+    prog.passes.push_back(lower_pass(t, p, prog.cfg, prog.upload, blobs[pi].blob.empty() ? nullptr : &blobs[pi]));
     prog.features.resize(prog.features.size() + kPassFeatures);
     pass_features(t, p, prog.passes.back(), prog.upload, prog.features.data() + prog.features.size() - kPassFeatures);
     prog.kernels += p.block ? 1 : p.ops.size();
