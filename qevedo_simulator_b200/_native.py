@@ -281,9 +281,9 @@ class DeviceState:
         n = ct.c_size_t()
         args = (self._h, u.size, as_double_ptr(u), q.ctypes.data_as(ct.POINTER(ct.c_uint32)),
                 c.ctypes.data_as(ct.POINTER(ct.c_uint32)), len(measures))
-        check(lib().qvdg_sample_counts(*args, None, None, 0, ct.byref(n)))
-        keys = np.zeros(max(n.value, 1), dtype=np.uint64)
-        counts = np.zeros(max(n.value, 1), dtype=np.uint64)
+        # At most one distinct key per shot: one call samples and fills.
+        keys = np.zeros(max(u.size, 1), dtype=np.uint64)
+        counts = np.zeros(max(u.size, 1), dtype=np.uint64)
         check(lib().qvdg_sample_counts(*args, as_u64_ptr(keys), as_u64_ptr(counts), keys.size, ct.byref(n)))
         return keys[:n.value], counts[:n.value]
 

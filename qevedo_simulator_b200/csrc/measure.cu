@@ -180,16 +180,25 @@ __global__ void __launch_bounds__(32 * kSampWarps) k_chunk_sums(const cplx_t<T>*
   if (chunk0 >= nchunks) return;
   const int live = int(umin64(32, nchunks - chunk0));
   double s = 0.0;
+  constexpr int PL = Step<T>::per_lane;
   for (uint64_t pos = 0; pos < chunk_len; pos += W) {
-    for (int c = 0; c < live; ++c) {
-      const uint64_t base = (chunk0 + c) * chunk_len + pos;
+    // Eight chunks' windows in flight at a time (loads first, then the
+    // probabilities into shared memory).
+    for (int c0 = 0; c0 < live; c0 += 8) {
+      cplx_t<T> v[8][PL];
 #pragma unroll
-      for (int e = 0; e < Step<T>::per_lane; ++e) {
-        const uint64_t i = base + uint64_t(lane) * Step<T>::per_lane + e;
-        sp[warp][c][lane * Step<T>::per_lane + e] = (i < len && pos + lane * Step<T>::per_lane + e < chunk_len)
-                                                        ? prob<T>(psi[i])
-                                                        : 0.0;
-      }
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int e = 0; e < PL; ++e) {
+          const uint64_t i = (chunk0 + c0 + u) * chunk_len + pos + uint64_t(lane) * PL + e;
+          const bool ok = c0 + u < live && i < len && pos + uint64_t(lane) * PL + e < chunk_len;
+          v[u][e] = ok ? psi[i] : make_c<T>(T(0), T(0));
+        }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int e = 0; e < PL; ++e)
+          if (c0 + u < live) sp[warp][c0 + u][lane * PL + e] = prob<T>(v[u][e]);
     }
     __syncwarp();
     if (lane < live)
@@ -201,13 +210,22 @@ __global__ void __launch_bounds__(32 * kSampWarps) k_chunk_sums(const cplx_t<T>*
 
 // prefix[0] = 0, prefix[c + 1] = prefix[c] + sums[c], sequentially
 // (src/measure.rs:119-124).
-__global__ void k_prefix(const double* __restrict__ sums, uint64_t nchunks, double* __restrict__ prefix) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void __launch_bounds__(256) k_prefix(const double* __restrict__ sums, uint64_t nchunks,
+                                                double* __restrict__ prefix) {
+  constexpr int kTile = 2048;
+  __shared__ double tile[kTile];
   double p = 0.0;
-  prefix[0] = 0.0;
-  for (uint64_t c = 0; c < nchunks; ++c) {
-    p = __dadd_rn(p, sums[c]);
-    prefix[c + 1] = p;
+  if (threadIdx.x == 0) prefix[0] = 0.0;
+  for (uint64_t t0 = 0; t0 < nchunks; t0 += kTile) {
+    const int n = int(umin64(kTile, nchunks - t0));
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tile[i] = sums[t0 + i];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int i = 0; i < n; ++i) {
+        p = __dadd_rn(p, tile[i]);
+        prefix[t0 + i + 1] = p;
+      }
   }
 }
 
@@ -302,14 +320,23 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(const cplx_t<T>* __res
   for (uint64_t pos = 0; walking && pos < end; pos += kWalkWindow) {
     if (pos + kWalkWindow < end) fill(pos + kWalkWindow, buf ^ 1);
     if (lane == 0) {
-      for (int j = 0; j < kWalkWindow; ++j) {
-        const double p = sp[warp][buf][j];
-        if (p == 0.0) continue;
-        const uint64_t index = base + pos + uint64_t(j);
-        last_nonzero = index;
-        cumulative = __dadd_rn(cumulative, p);
-        while (shot < hi && targets[shot] < cumulative) out[shot++] = index;
-        if (shot == hi) break;
+      double next = targets[shot];  // shot < hi here
+      for (int j0 = 0; j0 < kWalkWindow && shot < hi; j0 += 8) {
+        double p[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) p[j] = sp[warp][buf][j0 + j];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (p[j] == 0.0 || shot == hi) continue;
+          const uint64_t index = base + pos + uint64_t(j0 + j);
+          last_nonzero = index;
+          cumulative = __dadd_rn(cumulative, p[j]);
+          while (next < cumulative) {
+            out[shot++] = index;
+            if (shot == hi) break;
+            next = targets[shot];
+          }
+        }
       }
     }
     walking = __shfl_sync(0xffffffffu, shot < hi ? 1 : 0, 0) != 0;
@@ -488,7 +515,7 @@ size_t sample_device_t(StateImpl& s, size_t shots, const double* uniforms_host, 
   const unsigned chunk_blocks = unsigned((nchunks + 32 * kSampWarps - 1) / (32 * kSampWarps));
   k_chunk_sums<T><<<chunk_blocks, 32 * kSampWarps, 0, s.stream>>>(psi, len, chunk_len, nchunks, sums);
   QVDG_LAUNCH_CHECK();
-  k_prefix<<<1, 1, 0, s.stream>>>(sums, nchunks, prefix);
+  k_prefix<<<1, 256, 0, s.stream>>>(sums, nchunks, prefix);
   QVDG_LAUNCH_CHECK();
   k_target_keys<<<blocks_for(shots, kThreads), kThreads, 0, s.stream>>>(uni, shots, prefix + nchunks, keys);
   QVDG_LAUNCH_CHECK();
