@@ -45,10 +45,13 @@ METRIC = "30q random-circuit s & HBM GB/s vs peak, tuned vs plain GPU at <=1e-6 
 # DRAM bytes (read + write) per amplitude of one plain fused-gate pass, from
 # ncu captures at 26 qubits (2^26 amplitudes per launch; a full-size launch
 # scales by its amplitude count), by pass kind: 0 k_dense<float,4,2,1>
-# (536.9 MB read + 476.7 MB written), 2 k_dense_tc<6,0> (537.0 + 476.5 MB).
-TRAFFIC_BYTES_PER_AMP = {0: (536.9e6 + 476.7e6) / 2 ** 26, 2: (537.0e6 + 476.5e6) / 2 ** 26}
+# (536.9 MB read + 476.7 MB written), 2 k_dense_tc<6,0> (537.0 + 476.5 MB),
+# 3 k_dense_tc_tile<4,2> (536.9 + 477.6 MB).
+TRAFFIC_BYTES_PER_AMP = {0: (536.9e6 + 476.7e6) / 2 ** 26, 2: (537.0e6 + 476.5e6) / 2 ** 26,
+                         3: (536.9e6 + 477.6e6) / 2 ** 26}
 KERNEL_OF_KIND = {0: "k_dense<float,K,...> (plain fused-gate pass, CUDA cores)",
-                  2: "k_dense_tc<K,...> (plain fused-gate pass, tensor cores)"}
+                  2: "k_dense_tc<K,PAIR> (plain fused-gate pass, tensor cores)",
+                  3: "k_dense_tc_tile<K,NB> (plain fused-gate pass on bits 1-3, tensor cores)"}
 ROWS, COLS, DEPTH, SEED = 5, 6, 20, 2024
 SHOTS = 1000
 
@@ -335,7 +338,7 @@ def run_ours(args, rank: int, world: int):
     byt = np.concatenate(pass_b)
     kind = np.concatenate(pass_k)
     peaks = measured_peaks()
-    dom = max((0, 1, 2), key=lambda k: sec[kind == k].sum())
+    dom = max((0, 1, 2, 3), key=lambda k: sec[kind == k].sum())
     dsec, dbyt = sec[kind == dom], byt[kind == dom]
     avg = float(dsec.mean())
     per_launch = float(dbyt.mean())

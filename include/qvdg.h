@@ -354,7 +354,8 @@ qvdg_status qvdg_batch_tuning(const qvdg_batch* batch, uint32_t* tile_qubits, ui
 qvdg_status qvdg_set_pass_timing(qvdg_state* state, int32_t enabled);
 
 /* Per-pass device seconds, algorithmic bytes and kind (1 staged tile pass,
- * 0 single-gate pass, 2 single-gate pass on the tensor cores) of the last
+ * 0 single-gate pass, 2 single-gate pass on the tensor cores, 3 the same
+ * through a shared-memory stage for gates on index bits 1-3) of the last
  * gate run; `*count` receives the number of
  * passes, at most `capacity` entries are written. */
 qvdg_status qvdg_pass_times(const qvdg_state* state, double* seconds, double* bytes, int32_t* staged,

@@ -517,12 +517,16 @@ bool dense_tc_ok(uint32_t n, int bits, const std::vector<uint32_t>& targets, siz
   return t[3] < 32;  // member offsets of the four lowest targets in 32 bits
 }
 
+bool dense_tc_staged(uint32_t n, const std::vector<uint32_t>& targets, size_t controls) {
+  auto has = [&](uint32_t b) { return std::find(targets.begin(), targets.end(), b) != targets.end(); };
+  return controls == 0 && n >= uint32_t(7 + targets.size()) && has(1) && has(2) && has(3);
+}
+
 void launch_dense_tc(StateImpl& s, const PlainGate& pg, const uint8_t* tc_blob) {
   const int k = int(pg.targets.size()), c = int(pg.controls.size());
   if (!dense_tc_ok(s.n, s.bits, pg.targets, size_t(c)) || !std::is_sorted(pg.targets.begin(), pg.targets.end()))
     throw Error(QVDG_ERR_INVALID, "internal: gate does not fit the tensor-core plain pass");
-  auto has = [&](uint32_t b) { return std::find(pg.targets.begin(), pg.targets.end(), b) != pg.targets.end(); };
-  if (c == 0 && s.n >= uint32_t(7 + k) && has(1) && has(2) && has(3)) {
+  if (dense_tc_staged(s.n, pg.targets, size_t(c))) {
     // Bits 1-3 all targets: each group is a contiguous run of at least 8
     // amplitudes and the direct kernel's warps stride by that run, so the
     // state goes through the shared-memory stage. With fewer low targets

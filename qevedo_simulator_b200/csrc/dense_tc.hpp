@@ -35,6 +35,10 @@ struct DenseTcTileGeom {
 // targets below bit 32.
 bool dense_tc_ok(uint32_t n, int bits, const std::vector<uint32_t>& targets, size_t controls);
 
+// Whether such a gate takes the staged variant (k_dense_tc_tile): no
+// controls and targets (physical) on bits 1, 2 and 3.
+bool dense_tc_staged(uint32_t n, const std::vector<uint32_t>& targets, size_t controls);
+
 // `pg.targets` ascending, `pg.tc_offset` the byte offset of its bf16
 // matrices (hi then lo, as the stage kernel's) in `tc_blob`.
 void launch_dense_tc(StateImpl& s, const PlainGate& pg, const uint8_t* tc_blob);

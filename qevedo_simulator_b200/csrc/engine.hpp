@@ -55,7 +55,7 @@ struct StateImpl {
   bool record_passes = false;
   std::vector<cudaEvent_t> pass_events;
   std::vector<double> pass_seconds, pass_bytes;
-  std::vector<int> pass_kinds;  // 1 staged tile pass, 0 plain gate pass, 2 plain pass on the tensor cores
+  std::vector<int> pass_kinds;  // 1 staged tile pass, 0 plain gate pass, 2/3 plain pass on the tensor cores (direct/staged)
 
   size_t elem_bytes() const { return bits == 32 ? 8 : 16; }
   uint64_t size() const { return uint64_t(1) << n; }

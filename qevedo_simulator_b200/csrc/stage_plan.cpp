@@ -7,6 +7,7 @@
 #include <cstring>
 #include <string>
 
+#include "dense_tc.hpp"
 #include "program.hpp"
 #include "stage.hpp"
 #include "stage_kernel.hpp"
@@ -298,7 +299,11 @@ void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_s
       float t = 0.f;
       QVDG_CUDA(cudaEventElapsedTime(&t, s.pass_events[i], s.pass_events[i + 1]));
       s.pass_seconds.push_back(double(t) * 1e-3);
-      s.pass_kinds.push_back(p.passes[i].staged ? 1 : (p.passes[i].plain.tensor ? 2 : 0));
+      const LoweredPass& lp = p.passes[i];
+      int kind = lp.staged ? 1 : 0;
+      if (!lp.staged && lp.plain.tensor)
+        kind = dense_tc_staged(s.n, lp.plain.targets, lp.plain.controls.size()) ? 3 : 2;
+      s.pass_kinds.push_back(kind);
     }
     s.pass_bytes = p.pass_bytes;
   }

@@ -246,9 +246,16 @@ def test_tensor_core_plain_passes_single_gates(oracle, n):
             expected = oracle.naive_apply_ops(initial, ops)
             with DeviceState(n, 32) as st:
                 st.set_amplitudes(initial)
+                st.set_pass_timing(True)
                 st.apply_ops(ops, options(6, staged=False, math="tensor"))
                 err = max_distance(st.amplitudes(), expected) / np.max(np.abs(expected))
+                kind = st.pass_times()[2]
             assert err < TC_REL_TOL, (n, qubits, controls, err)
+            if n - len(controls) >= 13:
+                # direct kernel (2), or the shared-memory stage (3) for
+                # uncontrolled gates on bits 1, 2 and 3
+                staged = not controls and {1, 2, 3} <= set(qubits)
+                assert list(kind) == [3 if staged else 2], (qubits, controls, kind)
     assert used >= len(layouts)
 
 
