@@ -50,7 +50,7 @@ METRIC = "30q random-circuit s & HBM GB/s vs peak, tuned vs plain GPU at <=1e-6 
 TRAFFIC_BYTES_PER_AMP = {0: (536.9e6 + 476.7e6) / 2 ** 26, 2: (537.0e6 + 476.5e6) / 2 ** 26,
                          3: (536.9e6 + 477.6e6) / 2 ** 26}
 KERNEL_OF_KIND = {0: "k_dense<float,K,...> (plain fused-gate pass, CUDA cores)",
-                  2: "k_dense_tc<K,PAIR> (plain fused-gate pass, tensor cores)",
+                  2: "k_dense_tc<K,VW> (plain fused-gate pass, tensor cores)",
                   3: "k_dense_tc_tile<K,NB> (plain fused-gate pass on bits 1-3, tensor cores)"}
 ROWS, COLS, DEPTH, SEED = 5, 6, 20, 2024
 SHOTS = 1000

@@ -17,7 +17,8 @@
 // owns 16 members of group r of block w / P, P = 2^K / 16: it loads them
 // (consecutive threads take consecutive groups, so a warp's loads of one
 // member are contiguous when bit 0 is free; with a target on bit 0 the
-// members pair into 16-byte accesses), writes their bf16 parts into one of
+// members pair into 16-byte accesses, with targets on bits 0 and 1 into
+// 32-byte ones), writes their bf16 parts into one of
 // two A buffers, and, once TMEM lane r holds the block's products, reads
 // its 16 members back and stores them where they came from. The loads of
 // iteration i + 1 are issued before iteration i's products, and iteration
@@ -36,6 +37,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "dense_tc.hpp"
 #include "stage_kernel.hpp"
@@ -117,7 +119,7 @@ __device__ __forceinline__ void write_a8(const float2* x, unsigned char* ah, uns
   *reinterpret_cast<uint4*>(al + row + cim) = l;
 }
 
-template <int K, bool PAIR>
+template <int K, int VW>
 __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ psi, const DenseTcGeom g,
                                                           const uint8_t* __restrict__ bmats,
                                                           int* __restrict__ status) {
@@ -186,7 +188,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ p
     return b;
   };
   auto load = [&](float2 (&x)[16], uint64_t base) {
-    if constexpr (PAIR) {
+    if constexpr (VW == 4) {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) ld_early32(psi + base + off_lo[4 * m], &x[4 * m]);
+    } else if constexpr (VW == 2) {
 #pragma unroll
       for (int m = 0; m < 8; ++m) {
         const float4 v = ld_early(psi + base + off_lo[2 * m]);
@@ -234,7 +239,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ p
           tmem_ld8(taddr + 8 * hh, re);
           tmem_ld8(taddr + D + 8 * hh, im);
           tmem_wait_ld();
-          if constexpr (PAIR) {
+          if constexpr (VW == 4) {
+#pragma unroll
+            for (int m = 0; m < 2; ++m) st32(psi + base + off_lo[8 * hh + 4 * m], re + 4 * m, im + 4 * m);
+          } else if constexpr (VW == 2) {
 #pragma unroll
             for (int m = 0; m < 4; ++m)
               *reinterpret_cast<float4*>(psi + base + off_lo[8 * hh + 2 * m]) =
@@ -464,16 +472,16 @@ __global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_
   }
 }
 
-template <int K, bool PAIR>
+template <int K, int VW>
 void launch_k(StateImpl& s, const DenseTcGeom& g, const uint8_t* bmats) {
   const size_t smem = 4 * size_t(kPartBytes) + tc_gate_bytes(K);
   static bool configured = false;  // per instantiation
   if (!configured) {
-    QVDG_CUDA(cudaFuncSetAttribute(k_dense_tc<K, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    QVDG_CUDA(cudaFuncSetAttribute(k_dense_tc<K, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     configured = true;
   }
   const unsigned grid = unsigned(std::min<uint64_t>(g.iters, uint64_t(s.sms)));
-  k_dense_tc<K, PAIR><<<grid, kThreads, smem, s.stream>>>(static_cast<float2*>(s.amp), g, bmats, s.status);
+  k_dense_tc<K, VW><<<grid, kThreads, smem, s.stream>>>(static_cast<float2*>(s.amp), g, bmats, s.status);
   QVDG_LAUNCH_CHECK();
 }
 
@@ -519,7 +527,10 @@ bool dense_tc_ok(uint32_t n, int bits, const std::vector<uint32_t>& targets, siz
 
 bool dense_tc_staged(uint32_t n, const std::vector<uint32_t>& targets, size_t controls) {
   auto has = [&](uint32_t b) { return std::find(targets.begin(), targets.end(), b) != targets.end(); };
-  return controls == 0 && n >= uint32_t(7 + targets.size()) && has(1) && has(2) && has(3);
+  // With bit 0 a target too, 6-qubit gates go faster on the direct kernel's
+  // 32-byte accesses; narrower ones (several CTAs per SM here) on this one.
+  return controls == 0 && n >= uint32_t(7 + targets.size()) && has(1) && has(2) && has(3) &&
+         (targets.size() <= 5 || !has(0));
 }
 
 void launch_dense_tc(StateImpl& s, const PlainGate& pg, const uint8_t* tc_blob) {
@@ -529,8 +540,9 @@ void launch_dense_tc(StateImpl& s, const PlainGate& pg, const uint8_t* tc_blob) 
   if (dense_tc_staged(s.n, pg.targets, size_t(c))) {
     // Bits 1-3 all targets: each group is a contiguous run of at least 8
     // amplitudes and the direct kernel's warps stride by that run, so the
-    // state goes through the shared-memory stage. With fewer low targets
-    // the direct kernel is faster (measured on the 30-qubit grid circuit).
+    // state goes through the shared-memory stage. With fewer low targets,
+    // and for 6-qubit gates that also target bit 0, the direct kernel is
+    // faster (measured on the 30-qubit grid circuit).
     DenseTcTileGeom tg{};
     std::vector<uint32_t> bits(pg.targets.begin(), pg.targets.end());
     const int tb = 7 + k;
@@ -576,11 +588,19 @@ void launch_dense_tc(StateImpl& s, const PlainGate& pg, const uint8_t* tc_blob) 
   g.b_offset = uint32_t(pg.tc_offset);
   // Members 2m and 2m + 1 are neighbours when targets[0] is bit 0 (the
   // lowering sorts targets ascending).
-  const bool pair = pg.targets[0] == 0;
+  // Access width: members 4m..4m+3 are neighbours when bits 0 and 1 are
+  // both targets (32-byte accesses), 2m and 2m+1 when bit 0 is (16-byte).
+  const int vw = pg.targets[0] == 0 ? (pg.targets[1] == 1 ? 4 : 2) : 1;
+  auto go = [&](auto kk) {
+    constexpr int KK = decltype(kk)::value;
+    if (vw == 4) return launch_k<KK, 4>(s, g, tc_blob);
+    if (vw == 2) return launch_k<KK, 2>(s, g, tc_blob);
+    return launch_k<KK, 1>(s, g, tc_blob);
+  };
   switch (k) {
-    case 4: return pair ? launch_k<4, true>(s, g, tc_blob) : launch_k<4, false>(s, g, tc_blob);
-    case 5: return pair ? launch_k<5, true>(s, g, tc_blob) : launch_k<5, false>(s, g, tc_blob);
-    default: return pair ? launch_k<6, true>(s, g, tc_blob) : launch_k<6, false>(s, g, tc_blob);
+    case 4: return go(std::integral_constant<int, 4>());
+    case 5: return go(std::integral_constant<int, 5>());
+    default: return go(std::integral_constant<int, 6>());
   }
 }
 

@@ -36,7 +36,8 @@ struct DenseTcTileGeom {
 bool dense_tc_ok(uint32_t n, int bits, const std::vector<uint32_t>& targets, size_t controls);
 
 // Whether such a gate takes the staged variant (k_dense_tc_tile): no
-// controls and targets (physical) on bits 1, 2 and 3.
+// controls, targets (physical) on bits 1, 2 and 3, and not a 6-qubit gate
+// that also targets bit 0.
 bool dense_tc_staged(uint32_t n, const std::vector<uint32_t>& targets, size_t controls);
 
 // `pg.targets` ascending, `pg.tc_offset` the byte offset of its bf16

@@ -89,6 +89,23 @@ static __device__ __forceinline__ float2 ld_early8(const float2* p) {
   return v;
 }
 
+// The same for four complex64 (32 bytes, 32-byte aligned).
+static __device__ __forceinline__ void ld_early32(const float2* p, float2* v) {
+  float f[8];
+  asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]), "=f"(f[6]), "=f"(f[7])
+               : "l"(p));
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = make_float2(f[2 * i], f[2 * i + 1]);
+}
+
+// A 32-byte store of four complex64 (32-byte aligned).
+static __device__ __forceinline__ void st32(float2* p, const float* re, const float* im) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(re[0]), "f"(im[0]),
+               "f"(re[1]), "f"(im[1]), "f"(re[2]), "f"(im[2]), "f"(re[3]), "f"(im[3])
+               : "memory");
+}
+
 static __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 static __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 static __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }

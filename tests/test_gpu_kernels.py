@@ -230,12 +230,14 @@ def _plain_tensor_passes(ops, n):
 def test_tensor_core_plain_passes_single_gates(oracle, n):
     """Plain passes of one fused 4-6 qubit gate on the tensor cores (bf16x3,
     fp32 accumulation): targets in any order, on bit 0 (paired 16-byte
-    accesses) or not, low and high, with controls where at least 8192
-    amplitudes stay selected (otherwise the CUDA-core pass runs)."""
+    accesses), on bits 0 and 1 (32-byte accesses) or neither, low and high,
+    with controls where at least 8192 amplitudes stay selected (otherwise
+    the CUDA-core pass runs)."""
     rng = np.random.Generator(np.random.PCG64(300 + n))
     initial = random_state(rng, n)
     layouts = [[0, 1, 2, 3], [3, 1, 0, 2, 4], [n - 1, 0, 5, 2, 7, 3], [4, 5, 6, 7], [n - 4, n - 3, n - 2, n - 1, 1],
-               [9, 2, 12, 6, 1, 8], [1, 2, 3, 4, 5, 6], [6, 0, 11, 3]]
+               [9, 2, 12, 6, 1, 8], [1, 2, 3, 4, 5, 6], [6, 0, 11, 3], [5, 1, 0, 9], [0, 1, 2, 8, 10, 12],
+               [3, 0, 2, 1, 9, 11]]
     used = 0
     for qubits in layouts:
         for controls in ([], [(max(qubits) + 1 if max(qubits) + 1 < n else min(set(range(n)) - set(qubits)),
@@ -253,8 +255,9 @@ def test_tensor_core_plain_passes_single_gates(oracle, n):
             assert err < TC_REL_TOL, (n, qubits, controls, err)
             if n - len(controls) >= 13:
                 # direct kernel (2), or the shared-memory stage (3) for
-                # uncontrolled gates on bits 1, 2 and 3
-                staged = not controls and {1, 2, 3} <= set(qubits)
+                # uncontrolled gates on bits 1, 2 and 3 (6-qubit ones only
+                # without bit 0)
+                staged = not controls and {1, 2, 3} <= set(qubits) and (len(qubits) <= 5 or 0 not in qubits)
                 assert list(kind) == [3 if staged else 2], (qubits, controls, kind)
     assert used >= len(layouts)
 
