@@ -533,6 +533,77 @@ def run_precision(args):
     print(json.dumps(out), flush=True)
 
 
+def run_batch(args):
+    """The batched form: 4096 hardware-efficient ansatz circuits (width
+    uniform in 10-22, 4-12 layers of RZ(phi) RY(theta) on every qubit plus a
+    CNOT ladder; seeded angles) to <Z_q> for every qubit in one persistent,
+    graph-captured launch with an autotuned tile shape, against the
+    per-circuit plain path (apply_ops + expect_z_all per circuit on a reused
+    state, timed on a sample and scaled to the batch). Error: max |delta
+    <Z>| of the batch against complex128 per-circuit runs on the sample."""
+    from qevedo_simulator_b200 import Batch, DeviceState, library, options
+
+    count, sample = 4096, 64
+    specs = library.hea_batch(count, seed=SEED)
+    circuits = [(w, library.hea_layers(w, l, s), "cx") for w, l, s in specs]
+    t0 = time.perf_counter()
+    b = Batch(circuits)
+    create_s = time.perf_counter() - t0
+    flat, _ = b.run()
+    times = []
+    for _ in range(max(args.warmup, 1)):
+        b.run()
+    for _ in range(args.steps):
+        flat, sec = b.run()
+        times.append(sec)
+    z = b.split(flat)
+    info, tuning = b.info(), b.tuning()
+    b.close()
+
+    def ladder(n, gates):
+        from qevedo_simulator_b200 import Circuit
+
+        c = Circuit(n)
+        for layer in gates:
+            for q in range(n):
+                c.unitary(layer[q], [q])
+            for q in range(n - 1):
+                c.cx(q, q + 1)
+        return c.ops()
+
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    picks = sorted(rng.choice(count, size=sample, replace=False).tolist())
+    per_circuit, err = 0.0, 0.0
+    states = {}
+    for i in picks:
+        w, gates = circuits[i][0], circuits[i][1]
+        ops = ladder(w, gates)
+        if w not in states:
+            states[w] = (DeviceState(w, 32), DeviceState(w, 64))
+        st32, st64 = states[w]
+        st32.zero()
+        t0 = time.perf_counter()
+        st32.apply_ops(ops, options(4, staged=False))
+        st32.expect_z_all()
+        per_circuit += time.perf_counter() - t0
+        st64.zero()
+        st64.apply_ops(ops, options(4, staged=False))
+        err = max(err, float(np.abs(z[i] - st64.expect_z_all()).max()))
+    for a, c in states.values():
+        a.close()
+        c.close()
+    per_circuit_s = per_circuit / sample * count
+    batch_s = float(np.mean(times))
+    out = {"metric": "batched HEA: seconds for 4096 circuits to <Z_q>", "unit": "s", "higher_is_better": False,
+           "value": batch_s, "steps": args.steps, "warmup": max(args.warmup, 1),
+           "workload": "4096 HEA circuits, width U{10..22}, layers U{4..12}, RZ(phi) RY(theta) per qubit + CX ladder, "
+                       "complex64, seeded", "shape": info, "tuning": [list(t) for t in tuning],
+           "create_and_tune_s": create_s,
+           "per_circuit_path_s": per_circuit_s, "per_circuit_sample": sample,
+           "speedup_vs_per_circuit": per_circuit_s / batch_s, "max_abs_dz_vs_c128_sample": err}
+    print(json.dumps(out), flush=True)
+
+
 def tuned_upload_bytes(ops) -> int:
     """Upper bound of the gate-program and matrix bytes a plan uploads per
     run (complex64 matrices plus a 96-byte descriptor per op)."""
@@ -546,7 +617,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--qubits", type=int, default=30)
-    ap.add_argument("--workload", choices=["grid", "qft", "precision"], default="grid",
+    ap.add_argument("--workload", choices=["grid", "qft", "precision", "batch"], default="grid",
                     help="grid: the 30-qubit random-circuit benchmark (the bench line); qft and precision: the "
                          "other configurations, one JSON line each")
     ap.add_argument("--plan", nargs=3, metavar=("FUSION", "plain|staged", "fp32|tensor"), default=None,
@@ -567,6 +638,9 @@ def main():
     elif args.workload == "precision":
         if rank == 0:
             run_precision(args)
+    elif args.workload == "batch":
+        if rank == 0:
+            run_batch(args)
     else:
         run_ours(args, rank, world)
 

@@ -350,7 +350,9 @@ int batch_kernel_occupancy(int threads, int tile_qubits) {
   // Allow the largest tile once, so that launches (also under stream
   // capture) need no attribute change.
   if (cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(float2) << 14)) !=
-      cudaSuccess) {
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_batch, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           int(cudaSharedmemCarveoutMaxShared)) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
