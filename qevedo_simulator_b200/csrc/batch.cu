@@ -69,9 +69,93 @@ __device__ __forceinline__ float2 cfma2(float2 m0, float2 x0, float2 m1, float2 
   return o;
 }
 
+// The part of the entangler ladder that lands in the group's G qubits
+// (local bits q..q+G-1 of subcube `base`, global qubit of bit q = qglob).
+template <int G>
+__device__ __forceinline__ void ladder(float2 (&a)[1 << G], int entangler, int qglob, const TileMap& map,
+                                       uint32_t base) {
+  constexpr int S = 1 << G;
+  if (entangler != QVDG_ENTANGLE_NONE) {
+    const bool ctrl = qglob > 0 && ((map.global(base) >> (qglob - 1)) & 1u);
+    if (entangler == QVDG_ENTANGLE_CX_LADDER) {
+      // cx(qglob-1, qglob): flip local bit 0 where the outside control is 1.
+#pragma unroll
+      for (int j = 0; j < S; j += 2) {
+        const float2 t0 = a[j], t1 = a[j + 1];
+        a[j] = ctrl ? t1 : t0;
+        a[j + 1] = ctrl ? t0 : t1;
+      }
+      // cx(q+g, q+g+1) inside the group, in ladder order.
+#pragma unroll
+      for (int g = 0; g + 1 < G; ++g) {
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+          if (!(j & (1 << g)) || (j & (2 << g))) continue;
+          const float2 t = a[j];
+          a[j] = a[j | (2 << g)];
+          a[j | (2 << g)] = t;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 1; j < S; j += 2)
+        if (ctrl) a[j] = make_float2(-a[j].x, -a[j].y);
+#pragma unroll
+      for (int g = 0; g + 1 < G; ++g) {
+#pragma unroll
+        for (int j = 0; j < S; ++j)
+          if ((j & (1 << g)) && (j & (2 << g))) a[j] = make_float2(-a[j].x, -a[j].y);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+// The same for a phased circuit: each qubit's gate is diag(p) R diag(q)
+// with R real, so a group applies its right phases (one complex multiply per
+// element from the table `right`, the product of the group's q), the real
+// rotations (half the multiply-adds of a complex 2x2) and its left phases.
+template <int G>
+__device__ void apply_group_phased(float2* __restrict__ tile, int nb, int q, const float2* __restrict__ mats,
+                                   const float2* __restrict__ left, const float2* __restrict__ right, uint32_t form,
+                                   int entangler, int qglob, const TileMap& map) {
+  constexpr int S = 1 << G;
+  const uint32_t subcubes = 1u << (nb - G);
+  const uint32_t low_mask = (1u << q) - 1u;
+  for (uint32_t b = threadIdx.x; b < subcubes; b += blockDim.x) {
+    const uint32_t base = ((b & ~low_mask) << G) | (b & low_mask);
+    float2 a[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) a[j] = tile[swz(base | (uint32_t(j) << q))];
+    if (form & kBatchRight)
+#pragma unroll
+      for (int j = 0; j < S; ++j) a[j] = cmul(a[j], right[j]);
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const float2 r0 = mats[kBatchGateSlots * (q + g) + 0], r1 = mats[kBatchGateSlots * (q + g) + 1];
+#pragma unroll
+      for (int j = 0; j < S; ++j) {
+        if (j & (1 << g)) continue;
+        const float2 x0 = a[j], x1 = a[j | (1 << g)];
+        a[j] = make_float2(fmaf(r0.x, x0.x, r0.y * x1.x), fmaf(r0.x, x0.y, r0.y * x1.y));
+        a[j | (1 << g)] = make_float2(fmaf(r1.x, x0.x, r1.y * x1.x), fmaf(r1.x, x0.y, r1.y * x1.y));
+      }
+    }
+    if (form & kBatchLeft)
+#pragma unroll
+      for (int j = 0; j < S; ++j) a[j] = cmul(a[j], left[j]);
+    ladder<G>(a, entangler, qglob, map, base);
+#pragma unroll
+    for (int j = 0; j < S; ++j) tile[swz(base | (uint32_t(j) << q))] = a[j];
+  }
+}
+
 // Apply the gates of local qubits q..q+G-1 (and their ladder part) to every
-// subcube of the 2^nb-element tile. `mats` holds 4 complex entries per local
-// qubit (m00, m01, m10, m11). `qglob` = global qubit of local bit q.
+// subcube of the 2^nb-element tile. `mats` holds a gate record per local
+// qubit (m00, m01, m10, m11 first). `qglob` = global qubit of local bit q.
 template <int G>
 __device__ void apply_group(float2* __restrict__ tile, int nb, int q, const float2* __restrict__ mats,
                             int entangler, int qglob, const TileMap& map) {
@@ -85,8 +169,8 @@ __device__ void apply_group(float2* __restrict__ tile, int nb, int q, const floa
     for (int j = 0; j < S; ++j) a[j] = tile[swz(base | (uint32_t(j) << q))];
 #pragma unroll
     for (int g = 0; g < G; ++g) {
-      const float2 m00 = mats[4 * (q + g) + 0], m01 = mats[4 * (q + g) + 1];
-      const float2 m10 = mats[4 * (q + g) + 2], m11 = mats[4 * (q + g) + 3];
+      const float2 m00 = mats[kBatchGateSlots * (q + g) + 0], m01 = mats[kBatchGateSlots * (q + g) + 1];
+      const float2 m10 = mats[kBatchGateSlots * (q + g) + 2], m11 = mats[kBatchGateSlots * (q + g) + 3];
 #pragma unroll
       for (int j = 0; j < S; ++j) {
         if (j & (1 << g)) continue;
@@ -95,58 +179,70 @@ __device__ void apply_group(float2* __restrict__ tile, int nb, int q, const floa
         a[j | (1 << g)] = cfma2(m10, x0, m11, x1);
       }
     }
-    if (entangler != QVDG_ENTANGLE_NONE) {
-      const bool ctrl = qglob > 0 && ((map.global(base) >> (qglob - 1)) & 1u);
-      if (entangler == QVDG_ENTANGLE_CX_LADDER) {
-        // cx(qglob-1, qglob): flip local bit 0 where the outside control is 1.
-#pragma unroll
-        for (int j = 0; j < S; j += 2) {
-          const float2 t0 = a[j], t1 = a[j + 1];
-          a[j] = ctrl ? t1 : t0;
-          a[j + 1] = ctrl ? t0 : t1;
-        }
-        // cx(q+g, q+g+1) inside the group, in ladder order.
-#pragma unroll
-        for (int g = 0; g + 1 < G; ++g) {
-#pragma unroll
-          for (int j = 0; j < S; ++j) {
-            if (!(j & (1 << g)) || (j & (2 << g))) continue;
-            const float2 t = a[j];
-            a[j] = a[j | (2 << g)];
-            a[j | (2 << g)] = t;
-          }
-        }
-      } else {
-#pragma unroll
-        for (int j = 1; j < S; j += 2)
-          if (ctrl) a[j] = make_float2(-a[j].x, -a[j].y);
-#pragma unroll
-        for (int g = 0; g + 1 < G; ++g) {
-#pragma unroll
-          for (int j = 0; j < S; ++j)
-            if ((j & (1 << g)) && (j & (2 << g))) a[j] = make_float2(-a[j].x, -a[j].y);
-        }
-      }
-    }
+    ladder<G>(a, entangler, qglob, map, base);
 #pragma unroll
     for (int j = 0; j < S; ++j) tile[swz(base | (uint32_t(j) << q))] = a[j];
   }
 }
 
-// Gates of local qubits [q0, q1) in groups of up to four, ascending.
-__device__ void apply_range(float2* tile, int nb, int q0, int q1, const float2* mats, int entangler, int qglob0,
-                            const TileMap& map) {
-  for (int q = q0; q < q1; q += 4) {
-    const int G = min(4, q1 - q);
-    const int qg = qglob0 + (q - q0);
-    if (G == 4)
-      apply_group<4>(tile, nb, q, mats, entangler, qg, map);
-    else if (G == 3)
-      apply_group<3>(tile, nb, q, mats, entangler, qg, map);
-    else if (G == 2)
-      apply_group<2>(tile, nb, q, mats, entangler, qg, map);
+// Gates of local qubits [q0, q1) in register groups of up to four qubits,
+// ascending, the range split as evenly as possible (13 qubits: 4 + 3 + 3 +
+// 3); each group costs one shared-memory round trip of the tile (groups of
+// five spill registers at 512 threads). For a phased circuit the groups'
+// phase tables (products of the members' left and right phases over the 2^G
+// elements of a subcube) go to `tabs` first.
+constexpr int kMaxGroup = 4;
+
+template <bool PHASED>
+__device__ __forceinline__ void apply_one(int G, float2* tile, int nb, int q, const float2* mats, const float2* l,
+                                          const float2* r, uint32_t form, int entangler, int qg, const TileMap& map) {
+  if constexpr (PHASED) {
+    switch (G) {
+      case 4: return apply_group_phased<4>(tile, nb, q, mats, l, r, form, entangler, qg, map);
+      case 3: return apply_group_phased<3>(tile, nb, q, mats, l, r, form, entangler, qg, map);
+      case 2: return apply_group_phased<2>(tile, nb, q, mats, l, r, form, entangler, qg, map);
+      default: return apply_group_phased<1>(tile, nb, q, mats, l, r, form, entangler, qg, map);
+    }
+  } else {
+    switch (G) {
+      case 4: return apply_group<4>(tile, nb, q, mats, entangler, qg, map);
+      case 3: return apply_group<3>(tile, nb, q, mats, entangler, qg, map);
+      case 2: return apply_group<2>(tile, nb, q, mats, entangler, qg, map);
+      default: return apply_group<1>(tile, nb, q, mats, entangler, qg, map);
+    }
+  }
+}
+
+__device__ void apply_range(float2* tile, int nb, int q0, int q1, const float2* mats, uint32_t form, int entangler,
+                            int qglob0, const TileMap& map, float2 (*tabs)[1 << kMaxGroup]) {
+  const int m = q1 - q0;
+  if (m <= 0) return;
+  const bool phased = (form & kBatchPhased) != 0;
+  const int groups = (m + kMaxGroup - 1) / kMaxGroup, small = m / groups, extra = m % groups;
+  auto start = [&](int gi) { return q0 + gi * small + min(gi, extra); };
+  auto size = [&](int gi) { return small + (gi < extra ? 1 : 0); };
+  if (phased) {
+    for (int i = threadIdx.x; i < groups << kMaxGroup; i += blockDim.x) {
+      const int gi = i >> kMaxGroup, j = i & ((1 << kMaxGroup) - 1), q = start(gi), G = size(gi);
+      if (j >= (1 << G)) continue;
+      float2 l = make_float2(1.f, 0.f), r = make_float2(1.f, 0.f);
+      for (int b = 0; b < G; ++b) {
+        const float2* rec = mats + kBatchGateSlots * (q + b);
+        const int bit = (j >> b) & 1;
+        l = cmul(l, rec[2 + bit]);
+        r = cmul(r, rec[4 + bit]);
+      }
+      tabs[2 * gi][j] = l;
+      tabs[2 * gi + 1][j] = r;
+    }
+    __syncthreads();
+  }
+  for (int gi = 0; gi < groups; ++gi) {
+    const int q = start(gi), qg = qglob0 + (q - q0);
+    if (phased)
+      apply_one<true>(size(gi), tile, nb, q, mats, tabs[2 * gi], tabs[2 * gi + 1], form, entangler, qg, map);
     else
-      apply_group<1>(tile, nb, q, mats, entangler, qg, map);
+      apply_one<false>(size(gi), tile, nb, q, mats, nullptr, nullptr, form, entangler, qg, map);
     __syncthreads();
   }
 }
@@ -241,8 +337,8 @@ __device__ void store_tile(const float2* tile, float2* __restrict__ slot, const 
 }
 
 __device__ void load_mats(float2* smem_mats, const float2* gates, int first_global, int count, int local0) {
-  for (int i = threadIdx.x; i < 4 * count; i += blockDim.x)
-    smem_mats[4 * local0 + i] = gates[4 * first_global + i];
+  for (int i = threadIdx.x; i < kBatchGateSlots * count; i += blockDim.x)
+    smem_mats[kBatchGateSlots * local0 + i] = gates[kBatchGateSlots * first_global + i];
 }
 
 __global__ void __launch_bounds__(512) k_batch(const BatchCircuit* __restrict__ circuits,
@@ -251,7 +347,8 @@ __global__ void __launch_bounds__(512) k_batch(const BatchCircuit* __restrict__ 
                                                uint64_t slot_elems, double* __restrict__ out,
                                                uint32_t* __restrict__ queue, int L) {
   extern __shared__ float2 tile[];
-  __shared__ float2 mats[4 * kBatchMaxQubits];
+  __shared__ float2 mats[kBatchGateSlots * kBatchMaxQubits];
+  __shared__ float2 tabs[8][1 << kMaxGroup];  // phase tables of up to four groups (left, right)
   __shared__ double red[32 * kVec];
   __shared__ double tmp[kVec];
   __shared__ double acc[1 + kBatchMaxQubits];
@@ -272,9 +369,9 @@ __global__ void __launch_bounds__(512) k_batch(const BatchCircuit* __restrict__ 
       const TileMap map{0, 0, L, 0};
       for (uint32_t l = 0; l < c.num_layers; ++l) {
         __syncthreads();
-        load_mats(mats, gates + 4 * c.gates, int(l) * n, n, 0);
+        load_mats(mats, gates + kBatchGateSlots * c.gates, int(l) * n, n, 0);
         __syncthreads();
-        apply_range(tile, n, 0, n, mats, int(c.entangler), 0, map);
+        apply_range(tile, n, 0, n, mats, c.form, int(c.entangler), 0, map, tabs);
       }
       __syncthreads();
       reduce_tile(tile, n, map, n, red, tmp, acc);
@@ -290,7 +387,7 @@ __global__ void __launch_bounds__(512) k_batch(const BatchCircuit* __restrict__ 
       for (uint32_t l = 0; l < c.num_layers; ++l) {
         const bool last = l + 1 == c.num_layers;
         __syncthreads();
-        load_mats(mats, gates + 4 * c.gates, int(l) * n, n, 0);
+        load_mats(mats, gates + kBatchGateSlots * c.gates, int(l) * n, n, 0);
         __syncthreads();
         // pass A: low Lw qubits
         if (l > 0) issue_tile(buf[0], slot, TileMap{0, 0, Lw, 0});
@@ -308,7 +405,7 @@ __global__ void __launch_bounds__(512) k_batch(const BatchCircuit* __restrict__ 
             wait_prev();
           }
           __syncthreads();
-          apply_range(cur, Lw, 0, Lw, mats, int(c.entangler), 0, map);
+          apply_range(cur, Lw, 0, Lw, mats, c.form, int(c.entangler), 0, map, tabs);
           store_tile(cur, slot, map);
           __threadfence_block();
           __syncthreads();
@@ -325,7 +422,7 @@ __global__ void __launch_bounds__(512) k_batch(const BatchCircuit* __restrict__ 
           wait_prev();
           __syncthreads();
           // Local bits r..Lw-1 are global qubits Lw..n-1 (matrices at local index).
-          apply_range(cur, Lw, r, Lw, mats + 4 * (Lw - r), int(c.entangler), Lw, map);
+          apply_range(cur, Lw, r, Lw, mats + kBatchGateSlots * (Lw - r), c.form, int(c.entangler), Lw, map, tabs);
           if (last) {
             reduce_tile(cur, Lw, map, n, red, tmp, acc);
           } else {

@@ -13,10 +13,17 @@ constexpr int kBatchMaxQubits = QVDG_BATCH_MAX_QUBITS;
 
 // One circuit of the batch on the device.
 struct BatchCircuit {
-  uint32_t num_qubits, num_layers, entangler, reserved;
-  uint64_t gates;  // index of its first 2x2 matrix (4 complex64 each) in the gate buffer
+  uint32_t num_qubits, num_layers, entangler;
+  uint32_t form;   // kBatchPhased | kBatchLeft | kBatchRight, or 0: generic 2x2 matrices
+  uint64_t gates;  // index of its first gate record (kBatchGateSlots complex64 each) in the gate buffer
   uint64_t out;    // index of its first <Z> output
 };
+
+// A gate record: the 2x2 matrix (m00, m01, m10, m11) in slots 0-3 for a
+// generic circuit; for a phased one U = diag(p0, p1) R diag(q0, q1) with R
+// real: slots (r00, r01), (r10, r11), p0, p1, q0, q1.
+constexpr int kBatchGateSlots = 8;
+constexpr uint32_t kBatchPhased = 1, kBatchLeft = 2, kBatchRight = 4;
 
 // Everything one launch of the batch kernel reads.
 struct BatchLaunch {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <complex>
 #include <chrono>
 #include <cstring>
 #include <numeric>
@@ -67,9 +68,81 @@ int ctas_for(const qvdg_batch* b, int threads, int L) {
   return ctas;
 }
 
-void convert_gates(const double* src, size_t num_matrices, std::vector<float2>& dst) {
-  dst.resize(num_matrices * 4);
-  for (size_t i = 0; i < num_matrices * 4; ++i) dst[i] = make_float2(float(src[2 * i]), float(src[2 * i + 1]));
+// U = diag(p0, p1) R diag(q0, q1) with R real and unit p, q: rows with one
+// common phase (q = 1) or columns with one (p = 1) when possible, otherwise
+// p0 = 1 and the rest from U's entries (all four nonzero for a unitary that
+// is neither diagonal nor anti-diagonal). False when U has no such form.
+bool decompose(const double* m, float2* rec, bool& left, bool& right) {
+  using Cd = std::complex<double>;
+  const Cd u[4] = {{m[0], m[1]}, {m[2], m[3]}, {m[4], m[5]}, {m[6], m[7]}};
+  auto unit = [](Cd c) { return c / std::abs(c); };
+  const double tol = 1e-9;
+  double r[4];
+  Cd p[2] = {1.0, 1.0}, q[2] = {1.0, 1.0};
+  auto real_of = [&](Cd c, double& out) {
+    if (std::abs(c.imag()) > tol) return false;
+    out = c.real();
+    return true;
+  };
+  auto rows = [&]() {
+    for (int i = 0; i < 2; ++i) {
+      const int k = std::abs(u[2 * i]) >= std::abs(u[2 * i + 1]) ? 0 : 1;
+      if (std::abs(u[2 * i + k]) == 0.0) return false;
+      p[i] = unit(u[2 * i + k]);
+      if (!real_of(u[2 * i] / p[i], r[2 * i]) || !real_of(u[2 * i + 1] / p[i], r[2 * i + 1])) return false;
+    }
+    q[0] = q[1] = 1.0;
+    return true;
+  };
+  auto cols = [&]() {
+    for (int j = 0; j < 2; ++j) {
+      const int k = std::abs(u[j]) >= std::abs(u[2 + j]) ? 0 : 1;
+      if (std::abs(u[2 * k + j]) == 0.0) return false;
+      q[j] = unit(u[2 * k + j]);
+      if (!real_of(u[j] / q[j], r[j]) || !real_of(u[2 + j] / q[j], r[2 + j])) return false;
+    }
+    p[0] = p[1] = 1.0;
+    return true;
+  };
+  auto general = [&]() {
+    for (const Cd& c : u)
+      if (std::abs(c) == 0.0) return false;
+    p[0] = 1.0;
+    q[0] = unit(u[0]);
+    q[1] = unit(u[1]);
+    p[1] = unit(u[2] / q[0]);
+    for (int i = 0; i < 2; ++i)
+      for (int j = 0; j < 2; ++j)
+        if (!real_of(u[2 * i + j] / (p[i] * q[j]), r[2 * i + j])) return false;
+    return true;
+  };
+  if (!rows() && !cols() && !general()) return false;
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j)
+      if (std::abs(p[i] * r[2 * i + j] * q[j] - u[2 * i + j]) > tol) return false;
+  rec[0] = make_float2(float(r[0]), float(r[1]));
+  rec[1] = make_float2(float(r[2]), float(r[3]));
+  rec[2] = make_float2(float(p[0].real()), float(p[0].imag()));
+  rec[3] = make_float2(float(p[1].real()), float(p[1].imag()));
+  rec[4] = make_float2(float(q[0].real()), float(q[0].imag()));
+  rec[5] = make_float2(float(q[1].real()), float(q[1].imag()));
+  left = left || p[0] != Cd(1.0) || p[1] != Cd(1.0);
+  right = right || q[0] != Cd(1.0) || q[1] != Cd(1.0);
+  return true;
+}
+
+// A circuit's gate records (kBatchGateSlots complex64 per matrix) and its
+// form: phased when every matrix decomposes, else the generic matrices.
+uint32_t encode_gates(const double* src, size_t num_matrices, float2* dst) {
+  bool left = false, right = false, phased = true;
+  for (size_t i = 0; i < num_matrices && phased; ++i)
+    phased = decompose(src + 8 * i, dst + kBatchGateSlots * i, left, right);
+  if (phased) return kBatchPhased | (left ? kBatchLeft : 0u) | (right ? kBatchRight : 0u);
+  for (size_t i = 0; i < num_matrices; ++i)
+    for (int k = 0; k < kBatchGateSlots; ++k)
+      dst[kBatchGateSlots * i + k] =
+          k < 4 ? make_float2(float(src[8 * i + 2 * k]), float(src[8 * i + 2 * k + 1])) : make_float2(0.f, 0.f);
+  return 0;
 }
 
 BatchLaunch shape(const BatchLaunch& base, int L, int threads, int ctas, uint32_t max_qubits) {
@@ -127,7 +200,7 @@ qvdg_batch* batch_create(const qvdg_layered_circuit* circuits, size_t count, con
       d.num_qubits = c.num_qubits;
       d.num_layers = c.num_layers;
       d.entangler = c.entangler;
-      d.reserved = 0;
+      d.form = 0;
       d.gates = b->num_matrices;
       d.out = b->outputs;
       b->num_matrices += uint64_t(c.num_layers) * c.num_qubits;
@@ -135,13 +208,10 @@ qvdg_batch* batch_create(const qvdg_layered_circuit* circuits, size_t count, con
       b->max_qubits = std::max(b->max_qubits, c.num_qubits);
     }
     if (want_tile) require(shape_fits(b->max_qubits, int(want_tile)), "tile_qubits too small for the widest circuit");
-    std::vector<float2> gates;
-    gates.reserve(b->num_matrices * 4);
-    for (size_t i = 0; i < count; ++i) {
-      std::vector<float2> g;
-      convert_gates(circuits[i].gates, size_t(circuits[i].num_layers) * circuits[i].num_qubits, g);
-      gates.insert(gates.end(), g.begin(), g.end());
-    }
+    std::vector<float2> gates(b->num_matrices * kBatchGateSlots);
+    for (size_t i = 0; i < count; ++i)
+      b->circuits[i].form = encode_gates(circuits[i].gates, size_t(circuits[i].num_layers) * circuits[i].num_qubits,
+                                         gates.data() + kBatchGateSlots * b->circuits[i].gates);
     // Largest first: an atomic counter then hands out work longest-first.
     std::vector<uint32_t> order(count);
     std::iota(order.begin(), order.end(), 0u);
@@ -264,12 +334,16 @@ void batch_set_gates(qvdg_batch* b, const double* gates, size_t num_matrices) {
   require(num_matrices == b->num_matrices, "expected " + std::to_string(b->num_matrices) + " matrices");
   require(gates != nullptr || num_matrices == 0, "null gates");
   if (num_matrices == 0) return;
-  std::vector<float2> g;
-  convert_gates(gates, num_matrices, g);
+  // Each circuit's records and form (the form follows the new matrices).
+  std::vector<float2> g(num_matrices * kBatchGateSlots);
+  for (BatchCircuit& c : b->circuits)
+    c.form = encode_gates(gates + 8 * c.gates, size_t(c.num_layers) * c.num_qubits, g.data() + kBatchGateSlots * c.gates);
   QVDG_CUDA(cudaSetDevice(b->device));
   QVDG_CUDA(cudaStreamSynchronize(b->stream));
   QVDG_CUDA(cudaMemcpy(const_cast<float2*>(b->launch.gates), g.data(), g.size() * sizeof(float2),
                        cudaMemcpyHostToDevice));
+  QVDG_CUDA(cudaMemcpy(const_cast<BatchCircuit*>(b->launch.circuits), b->circuits.data(),
+                       b->circuits.size() * sizeof(BatchCircuit), cudaMemcpyHostToDevice));
 }
 
 void batch_run(qvdg_batch* b, double* expect_z, size_t count, double* seconds) {

@@ -35,6 +35,20 @@ def layered_circuit(n, gates, entangler):
     return c
 
 
+def layered_ops(n, gates, entangler):
+    """The same circuit as ops (matrices need not be unitary)."""
+    from qevedo_simulator_b200 import Op
+
+    x = np.array([[0, 1], [1, 0]], dtype=complex)
+    z = np.diag([1, -1]).astype(complex)
+    ops = []
+    for layer in gates:
+        ops += [Op([q], [], layer[q]) for q in range(n)]
+        if entangler != "none":
+            ops += [Op([q + 1], [(q, True)], x if entangler == "cx" else z) for q in range(n - 1)]
+    return ops
+
+
 def test_small_batch_matches_the_naive_oracle(oracle):
     specs = library.hea_batch(40, seed=3, widths=(1, 13), layers=(0, 6))
     circuits, expected = [], []
@@ -105,6 +119,53 @@ def test_hea_circuits_match_their_gate_by_gate_form(oracle):
         with Batch([(w, library.hea_layers(w, l, s), "cx")], tile_qubits=12, threads=128) as b:
             got, _ = b.run()
         assert np.abs(got - expected).max() < Z_TOL
+
+
+@pytest.mark.parametrize("tile", [12, 14])
+def test_every_gate_form(oracle, tile):
+    """Gate records in every form the host encodes: Haar-random SU(2) (left
+    and right phases around a real rotation), diagonal and anti-diagonal
+    gates, RZ.RY (left phases only), real rotations (no phases), and a
+    non-unitary matrix, which keeps its circuit on the generic 2x2 path;
+    narrow circuits in shared memory and wide ones in HBM slots."""
+    rng = np.random.Generator(np.random.PCG64(77))
+    s = np.array([[1, 0], [0, 1j]])
+    x = np.array([[0, 1], [1, 0]], dtype=complex)
+    shear = np.array([[1, 0.25], [0, 1]], dtype=complex)
+
+    def gates(w, layers, kind):
+        out = np.empty((layers, w, 2, 2), dtype=complex)
+        for layer in range(layers):
+            for q in range(w):
+                if kind == "haar":
+                    out[layer, q] = library.haar_su2(rng)
+                elif kind == "mixed":
+                    out[layer, q] = (s, x, library.haar_su2(rng), np.eye(2))[(layer + q) % 4]
+                elif kind == "real":
+                    t = rng.random() * 6.28
+                    out[layer, q] = [[np.cos(t), -np.sin(t)], [np.sin(t), np.cos(t)]]
+                else:  # one non-unitary gate, the rest Haar
+                    out[layer, q] = shear if (layer, q) == (0, 1) else library.haar_su2(rng)
+        return out
+
+    specs = [(9, 3, "haar", "cx"), (11, 4, "mixed", "cz"), (10, 3, "real", "cx"), (8, 3, "shear", "cx"),
+             (tile + 3, 3, "haar", "cx"), (tile + 2, 2, "mixed", "cz"), (tile + 1, 2, "shear", "none")]
+    circuits, expected = [], []
+    for w, layers, kind, ent in specs:
+        g = gates(w, layers, kind)
+        circuits.append((w, g, ent))
+        expected.append(z_of(oracle.naive_statevector(layered_ops(w, g, ent), w), w))
+    with Batch(circuits, tile_qubits=tile, threads=256) as b:
+        flat, _ = b.run()
+        for i, (got, exp) in enumerate(zip(b.split(flat), expected)):
+            assert np.abs(got - exp).max() < Z_TOL, (i, specs[i])
+        # New matrices of another form through set_gates.
+        new = [gates(w, layers, "haar" if kind != "haar" else "real") for w, layers, kind, _ in specs]
+        b.set_gates(new)
+        flat, _ = b.run()
+        for i, (w, layers, kind, ent) in enumerate(specs):
+            exp = z_of(oracle.naive_statevector(layered_ops(w, new[i], ent), w), w)
+            assert np.abs(b.split(flat)[i] - exp).max() < Z_TOL, ("set_gates", i)
 
 
 def test_invalid_batches_are_rejected():
