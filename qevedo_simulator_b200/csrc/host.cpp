@@ -109,63 +109,90 @@ void HOp::full(std::vector<uint32_t>& qs, HMatrix& m) const {
 
 namespace {
 
-bool contains(const std::vector<uint32_t>& v, uint32_t x) { return std::find(v.begin(), v.end(), x) != v.end(); }
-
 // One growth sweep of a fused group over the ops after its seed
-// (src/fusion.rs:126-170).
-void grow(const std::vector<HOp>& ops, std::vector<bool>& done, size_t seed, std::vector<size_t>& members,
-          std::vector<uint32_t>& qubits, size_t max_qubits, bool connected_only,
-          const std::function<size_t(const HOp&)>& width) {
-  std::vector<uint32_t> blocked;
-  for (size_t i = seed + 1; i < ops.size(); ++i) {
-    if (done[i]) continue;
-    if (connected_only &&
-        std::all_of(qubits.begin(), qubits.end(), [&](uint32_t q) { return contains(blocked, q); }))
-      break;
-    const std::vector<uint32_t> oq = ops[i].qubits();
-    bool touches_blocked = false;
-    std::vector<uint32_t> fresh;
-    for (uint32_t q : oq) {
-      if (contains(blocked, q)) touches_blocked = true;
-      if (!contains(qubits, q)) fresh.push_back(q);
-    }
-    const bool connected = fresh.size() < oq.size();
-    const bool fits = width(ops[i]) <= max_qubits && qubits.size() + fresh.size() <= max_qubits;
-    if (!touches_blocked && fits && (connected || !connected_only)) {
-      done[i] = true;
+// (src/fusion.rs:126-170), on qubit bit masks: an op joins when it touches
+// no blocked qubit and fits; otherwise its qubits become blocked. `pre`:
+// qubits of unfused ops before the seed (they block from the start).
+void grow(const std::vector<uint64_t>& mask, const std::vector<size_t>& width, const std::vector<bool>& done,
+          std::vector<bool>& taken, size_t seed, uint64_t pre, std::vector<size_t>& members, uint64_t& qubits,
+          size_t max_qubits, bool connected_only) {
+  uint64_t blocked = pre;
+  for (size_t i = seed + 1; i < mask.size(); ++i) {
+    if (done[i] || taken[i]) continue;
+    if (connected_only && (qubits & ~blocked) == 0) break;
+    const uint64_t m = mask[i], fresh = m & ~qubits;
+    const bool connected = fresh != m;
+    const bool fits = width[i] <= max_qubits && size_t(__builtin_popcountll(qubits | m)) <= max_qubits;
+    if (!(m & blocked) && fits && (connected || !connected_only)) {
+      taken[i] = true;
       members.push_back(i);
-      qubits.insert(qubits.end(), fresh.begin(), fresh.end());
+      qubits |= m;
     } else {
-      for (uint32_t q : oq)
-        if (!contains(blocked, q)) blocked.push_back(q);
+      blocked |= m;
     }
   }
-  std::sort(members.begin(), members.end());
 }
 
 }  // namespace
 
-std::vector<FusedGroup> fuse_groups(const std::vector<HOp>& ops, size_t max_qubits,
-                                    const std::function<bool(const HOp&)>& fusable) {
-  const std::function<size_t(const HOp&)> width = [&](const HOp& op) {
-    return fusable(op) ? op.width() : SIZE_MAX;
-  };
-  std::vector<bool> done(ops.size(), false);
-  std::vector<FusedGroup> groups;
-  for (size_t seed = 0; seed < ops.size(); ++seed) {
-    if (done[seed]) continue;
-    done[seed] = true;
-    FusedGroup g;
-    g.members = {seed};
-    g.qubits = ops[seed].qubits();
-    if (width(ops[seed]) <= max_qubits) {
-      grow(ops, done, seed, g.members, g.qubits, max_qubits, true, width);
-      grow(ops, done, seed, g.members, g.qubits, max_qubits, false, width);
+std::vector<FusedGroup> fuse_groups_lookahead(const std::vector<HOp>& ops, size_t max_qubits,
+                                              const std::function<bool(const HOp&)>& fusable, size_t lookahead) {
+  const size_t n = ops.size();
+  std::vector<uint64_t> mask(n, 0);
+  std::vector<size_t> width(n);
+  for (size_t i = 0; i < n; ++i) {
+    for (uint32_t q : ops[i].qubits()) {
+      if (q >= 64) throw std::logic_error("fusion supports qubits 0..63");
+      mask[i] |= uint64_t(1) << q;
     }
-    std::sort(g.qubits.begin(), g.qubits.end());
+    width[i] = fusable(ops[i]) ? ops[i].width() : SIZE_MAX;
+  }
+  std::vector<bool> done(n, false), taken(n, false);
+  std::vector<FusedGroup> groups;
+  size_t first = 0;
+  std::vector<size_t> members, best_members;
+  while (true) {
+    while (first < n && done[first]) ++first;
+    if (first == n) break;
+    // Seeds: the first unfused op, then up to `lookahead` later ones that
+    // no unfused earlier op holds back; keep the seed whose group takes the
+    // most ops (ties: the earliest).
+    uint64_t pending = 0, best_qubits = 0;
+    size_t tried = 0;
+    best_members.clear();
+    for (size_t s = first; s < n && tried <= lookahead; ++s) {
+      if (done[s]) continue;
+      if (!(mask[s] & pending)) {
+        ++tried;
+        members.assign(1, s);
+        uint64_t qubits = mask[s];
+        taken[s] = true;
+        if (width[s] <= max_qubits) {
+          grow(mask, width, done, taken, s, pending, members, qubits, max_qubits, true);
+          grow(mask, width, done, taken, s, pending, members, qubits, max_qubits, false);
+        }
+        for (size_t i : members) taken[i] = false;
+        if (members.size() > best_members.size()) {
+          best_members = members;
+          best_qubits = qubits;
+        }
+      }
+      pending |= mask[s];
+    }
+    FusedGroup g;
+    g.members = best_members;
+    std::sort(g.members.begin(), g.members.end());
+    for (size_t i : g.members) done[i] = true;
+    for (uint32_t q = 0; q < 64; ++q)
+      if ((best_qubits >> q) & 1) g.qubits.push_back(q);
     groups.push_back(std::move(g));
   }
   return groups;
+}
+
+std::vector<FusedGroup> fuse_groups(const std::vector<HOp>& ops, size_t max_qubits,
+                                    const std::function<bool(const HOp&)>& fusable) {
+  return fuse_groups_lookahead(ops, max_qubits, fusable, 0);
 }
 
 // m <- embed(g, gate_qubits -> qubits) * m without forming the embedded

@@ -62,6 +62,13 @@ struct FusedGroup {
 std::vector<FusedGroup> fuse_groups(const std::vector<HOp>& ops, size_t max_qubits,
                                     const std::function<bool(const HOp&)>& fusable);
 
+// The same greedy growth, but each group is seeded by whichever of the
+// first unfused op and the next `lookahead` ready ones (no unfused earlier
+// op shares a qubit with it) grows the largest group; 0 is the greedy
+// fusion above.
+std::vector<FusedGroup> fuse_groups_lookahead(const std::vector<HOp>& ops, size_t max_qubits,
+                                              const std::function<bool(const HOp&)>& fusable, size_t lookahead);
+
 // The group's ops as one op (the product matrix on its qubits; a group of one
 // op is that op, controls kept).
 HOp fuse_group(const std::vector<HOp>& ops, const FusedGroup& g);

@@ -288,6 +288,27 @@ def test_tensor_core_plain_circuits(oracle, kind):
         assert err < TC_CIRCUIT_TOL, (kind, fuse, err, stats)
 
 
+@pytest.mark.parametrize("kind", ["grid", "mixed"])
+def test_tensor_core_plain_passes_at_24_qubits(kind):
+    """24-qubit circuits (many CTA iterations, every access width and the
+    shared-memory stage) through tensor-core plain passes at fusion 4-6,
+    against a complex128 run of the same ops on the device: max |delta
+    amplitude| within the 1e-6 amplitude bound for complex64."""
+    from qevedo_simulator_b200 import library
+
+    n = 24
+    ops = library.random_grid_circuit(4, 6, 12, seed=41).ops() if kind == "grid" else library.mixed_ops(n, 10, seed=42)
+    with DeviceState(n, 64) as ref:
+        ref.apply_ops(ops, options(4, staged=False))
+        for fuse in (4, 5, 6):
+            with DeviceState(n, 32) as st:
+                st.set_pass_timing(True)
+                st.apply_ops(ops, options(fuse, staged=False, math="tensor"))
+                kinds = set(st.pass_times()[2].tolist())
+                assert 2 in kinds, kinds
+                assert ref.max_abs_diff(st) < 1e-6, (kind, fuse)
+
+
 @pytest.mark.parametrize("bits", [32, 64])
 @pytest.mark.parametrize("kind", ["grid", "mixed", "qft", "gates"])
 def test_plain_passes_applying_groups_gate_by_gate(oracle, bits, kind):
