@@ -188,13 +188,40 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     // The groups' product matrices are independent: built on host threads.
     const bool gates = opt.math == QVDG_MATH_GATES;
     // Tensor-core plain plans of 5-6 qubit groups seed each group among the
-    // next few ready ops (fewer passes: 51 instead of 55 on the 30-qubit
-    // grid circuit at fusion 6, 66 instead of 70 at fusion 5; at fusion 4 it
-    // would add passes); other plain plans keep the reference's greedy
-    // fusion.
-    const size_t lookahead = opt.math == QVDG_MATH_TENSOR && max_fused >= 5 ? 4 : 0;
-    const std::vector<FusedGroup> groups =
-        fuse_groups_lookahead(ops, max_fused, [](const HOp&) { return true; }, lookahead);
+    // next few ready ops: the fusions with 1-8 candidate seeds are scored by
+    // their passes, a pass with targets on index bits 1-3 counting as the
+    // 1.2-2.1 clean passes it takes on the tensor-core kernels, and the
+    // cheapest is kept (50 passes instead of 55 on the 30-qubit grid circuit
+    // at fusion 6, 64 instead of 70 at fusion 5; at fusion 4 the seeds would
+    // add passes). Other plain plans keep the reference's greedy fusion.
+    const auto all = [](const HOp&) { return true; };
+    std::vector<FusedGroup> groups = fuse_groups(ops, max_fused, all);
+    if (opt.math == QVDG_MATH_TENSOR && max_fused >= 5) {
+      auto score = [&](const std::vector<FusedGroup>& gs) {
+        double c = 0.0;
+        for (const FusedGroup& g : gs) {
+          int low = 0;
+          bool bit0 = false;
+          for (uint32_t q : g.qubits) {
+            const uint32_t ph = t.layout[q];
+            low += (ph >= 1 && ph <= 3) ? 1 : 0;
+            bit0 = bit0 || ph == 0;
+          }
+          c += low == 0 ? (bit0 ? 1.1 : 1.0) : (low == 1 ? 1.2 : (low == 2 ? 1.45 : 2.1));
+        }
+        return c;
+      };
+      std::vector<std::vector<FusedGroup>> cand(8);
+      parallel_for(cand.size(), [&](size_t i) { cand[i] = fuse_groups_lookahead(ops, max_fused, all, i + 1); });
+      double best = score(groups);
+      for (std::vector<FusedGroup>& gs : cand) {
+        const double sc = score(gs);
+        if (sc < best) {
+          best = sc;
+          groups = std::move(gs);
+        }
+      }
+    }
     passes.resize(groups.size());
     std::vector<size_t> products;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
