@@ -45,6 +45,7 @@ struct StateImpl {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   std::vector<uint32_t> layout;  // logical -> physical
+  bool zero_state = false;       // |0...0> since the last zero(): a relabel costs no data movement
   DeviceScratch work;            // device workspace (uploads, reductions, sampling)
   DeviceScratch work2;
   HostScratch host;              // pinned staging

@@ -25,7 +25,8 @@ struct Target {
 constexpr int kPassFeatures = 32;
 
 struct Program {
-  Target target;
+  Target target;                      // the state the program starts from (layout included)
+  std::vector<uint32_t> run_layout;   // the layout its passes use, when it relabels first (else empty)
   StageConfig cfg{};
   std::vector<LoweredPass> passes;
   std::vector<double> pass_bytes;  // algorithmic HBM bytes of each pass
@@ -43,7 +44,8 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
 // pinned staging buffer.
 DeviceUpload upload_program(StateImpl& s, const Program& p, DeviceScratch& dst);
 
-// Launch every pass on the state's stream and wait; fills stats (device
+// Relabel the state to the program's layout (free on a |0...0> state, swap
+// passes otherwise), launch every pass on the state's stream and wait; fills stats (device
 // time between the first and last launch) and, when the state records pass
 // timings, the per-pass device times.
 void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_stats* stats);

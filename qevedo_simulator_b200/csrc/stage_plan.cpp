@@ -196,30 +196,101 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     // add passes). Other plain plans keep the reference's greedy fusion.
     const auto all = [](const HOp&) { return true; };
     std::vector<FusedGroup> groups = fuse_groups(ops, max_fused, all);
-    if (opt.math == QVDG_MATH_TENSOR && max_fused >= 5) {
-      auto score = [&](const std::vector<FusedGroup>& gs) {
+    if (opt.math == QVDG_MATH_TENSOR && max_fused >= 5 && t.n >= 13) {
+      // Candidate fusions (seed lookahead 0-8) and, for each, the three
+      // qubits to place on physical bits 1-3 (a relabel that costs nothing
+      // on a |0...0> state and one swap pass otherwise): the pair with the
+      // lowest estimated cost, a pass with k targets on bits 1-3 counting as
+      // 1, 1.2, 1.45 or 2.1 clean passes.
+      std::vector<std::vector<FusedGroup>> cand(9);
+      std::vector<double> cost(cand.size());
+      std::vector<uint64_t> low_set(cand.size());
+      std::vector<uint32_t> at(t.n);  // physical -> logical
+      for (uint32_t q = 0; q < t.n; ++q) at[t.layout[q]] = q;
+      const uint64_t now = (uint64_t(1) << at[1]) | (uint64_t(1) << at[2]) | (uint64_t(1) << at[3]);
+      parallel_for(cand.size(), [&](size_t i) {
+        cand[i] = i == 0 ? groups : fuse_groups_lookahead(ops, max_fused, all, i);
+        std::vector<uint64_t> gm;
+        for (const FusedGroup& g : cand[i]) {
+          uint64_t m = 0;
+          for (uint32_t q : g.qubits) m |= uint64_t(1) << q;
+          gm.push_back(m);
+        }
+        auto eval = [&](uint64_t s) {
+          double c = 0.0;
+          for (uint64_t m : gm) {
+            const int low = __builtin_popcountll(m & s);
+            c += low == 0 ? 1.0 : (low == 1 ? 1.2 : (low == 2 ? 1.45 : 2.1));
+          }
+          return c;
+        };
+        // Triples among the 12 qubits in the fewest groups (the cost grows
+        // with every group a chosen qubit is in).
+        std::vector<uint32_t> by_use(t.n);
+        std::vector<int> use(t.n, 0);
+        for (uint64_t m : gm)
+          for (uint32_t q = 0; q < t.n; ++q) use[q] += int((m >> q) & 1);
+        for (uint32_t q = 0; q < t.n; ++q) by_use[q] = q;
+        std::stable_sort(by_use.begin(), by_use.end(), [&](uint32_t x, uint32_t y) { return use[x] < use[y]; });
+        const uint32_t pool = std::min<uint32_t>(t.n, 12);
+        double best = eval(now);
+        uint64_t best_set = now;
+        for (uint32_t a = 0; a < pool; ++a)
+          for (uint32_t b = a + 1; b < pool; ++b)
+            for (uint32_t c = b + 1; c < pool; ++c) {
+              const uint64_t s =
+                  (uint64_t(1) << by_use[a]) | (uint64_t(1) << by_use[b]) | (uint64_t(1) << by_use[c]);
+              const double v = eval(s);
+              if (v < best - 1e-9) {
+                best = v;
+                best_set = s;
+              }
+            }
+        cost[i] = best;
+        low_set[i] = best_set;
+      });
+      size_t pick = 0;
+      for (size_t i = 1; i < cand.size(); ++i)
+        if (cost[i] < cost[pick] - 1e-9) pick = i;
+      // Relabel only where it saves at least 1.5 passes (it costs one when
+      // the state is not |0...0>).
+      auto eval_now = [&](const std::vector<FusedGroup>& gs) {
         double c = 0.0;
         for (const FusedGroup& g : gs) {
           int low = 0;
-          bool bit0 = false;
-          for (uint32_t q : g.qubits) {
-            const uint32_t ph = t.layout[q];
-            low += (ph >= 1 && ph <= 3) ? 1 : 0;
-            bit0 = bit0 || ph == 0;
-          }
-          c += low == 0 ? (bit0 ? 1.1 : 1.0) : (low == 1 ? 1.2 : (low == 2 ? 1.45 : 2.1));
+          for (uint32_t q : g.qubits) low += ((now >> q) & 1) ? 1 : 0;
+          c += low == 0 ? 1.0 : (low == 1 ? 1.2 : (low == 2 ? 1.45 : 2.1));
         }
         return c;
       };
-      std::vector<std::vector<FusedGroup>> cand(8);
-      parallel_for(cand.size(), [&](size_t i) { cand[i] = fuse_groups_lookahead(ops, max_fused, all, i + 1); });
-      double best = score(groups);
-      for (std::vector<FusedGroup>& gs : cand) {
-        const double sc = score(gs);
-        if (sc < best) {
-          best = sc;
-          groups = std::move(gs);
+      size_t keep = 0;
+      double keep_cost = eval_now(cand[0]);
+      for (size_t i = 1; i < cand.size(); ++i) {
+        const double c = eval_now(cand[i]);
+        if (c < keep_cost - 1e-9) {
+          keep = i;
+          keep_cost = c;
         }
+      }
+      if (cost[pick] > keep_cost - 1.5) {
+        pick = keep;
+        low_set[pick] = now;
+      }
+      groups = std::move(cand[pick]);
+      if (low_set[pick] != now) {
+        // The chosen qubits onto bits 1-3 (those already there stay).
+        std::vector<uint32_t> layout = t.layout;
+        std::vector<uint32_t> phys_of_free;
+        std::vector<uint32_t> incoming;
+        for (uint32_t q = 0; q < t.n; ++q)
+          if (((low_set[pick] >> q) & 1) && !(layout[q] >= 1 && layout[q] <= 3)) incoming.push_back(q);
+        for (uint32_t p = 1; p <= 3; ++p)
+          if (!((low_set[pick] >> at[p]) & 1)) phys_of_free.push_back(p);
+        for (size_t k = 0; k < incoming.size(); ++k) {
+          const uint32_t q = incoming[k], p = phys_of_free[k], out = at[p];
+          std::swap(layout[q], layout[out]);
+        }
+        prog.run_layout = layout;
       }
     }
     passes.resize(groups.size());
@@ -245,19 +316,23 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     parallel_for(products.size(), [&](size_t j) { passes[products[j]].ops[0] = fuse_group(ops, groups[products[j]]); },
                  wide ? 0u : 1u);
   }
+  // Passes are lowered on the layout they run with.
+  Target run_target = t;
+  if (!prog.run_layout.empty()) run_target.layout = prog.run_layout;
+  const Target& tt = run_target;
   // Tensor-core plain passes' bf16 matrices, also on host threads.
   std::vector<PlainTcBlob> blobs(passes.size());
   std::vector<size_t> tc;
   for (size_t i = 0; i < passes.size(); ++i)
-    if (plain_tc_eligible(t, passes[i], prog.cfg)) tc.push_back(i);
-  parallel_for(tc.size(), [&](size_t j) { blobs[tc[j]] = plain_tc_blob(t, passes[tc[j]].ops[0]); },
+    if (plain_tc_eligible(tt, passes[i], prog.cfg)) tc.push_back(i);
+  parallel_for(tc.size(), [&](size_t j) { blobs[tc[j]] = plain_tc_blob(tt, passes[tc[j]].ops[0]); },
                tc.size() >= 8 ? 0u : 1u);
   const double state_bytes = double(uint64_t(t.bits == 32 ? 8 : 16) << t.n);
   for (size_t pi = 0; pi < passes.size(); ++pi) {
     const PlannedPass& p = passes[pi];
-    prog.passes.push_back(lower_pass(t, p, prog.cfg, prog.upload, blobs[pi].blob.empty() ? nullptr : &blobs[pi]));
+    prog.passes.push_back(lower_pass(tt, p, prog.cfg, prog.upload, blobs[pi].blob.empty() ? nullptr : &blobs[pi]));
     prog.features.resize(prog.features.size() + kPassFeatures);
-    pass_features(t, p, prog.passes.back(), prog.upload, prog.features.data() + prog.features.size() - kPassFeatures);
+    pass_features(tt, p, prog.passes.back(), prog.upload, prog.features.data() + prog.features.size() - kPassFeatures);
     prog.kernels += p.block ? 1 : p.ops.size();
     double b = 2.0 * state_bytes;
     if (p.staged)
@@ -296,6 +371,35 @@ DeviceUpload upload_program(StateImpl& s, const Program& p, DeviceScratch& dst) 
   return u;
 }
 
+// Bring the state to the layout the program's passes use: free on a
+// |0...0> state, otherwise swap passes of disjoint physical bit pairs.
+static void relabel_to(StateImpl& s, const std::vector<uint32_t>& layout) {
+  if (layout == s.layout) return;
+  if (s.zero_state) {
+    s.layout = layout;
+    return;
+  }
+  while (s.layout != layout) {
+    std::vector<std::pair<uint32_t, uint32_t>> pairs;
+    uint64_t used = 0;
+    for (uint32_t q = 0; q < s.n; ++q) {
+      const uint32_t a = s.layout[q], b = layout[q];
+      const uint64_t m = (uint64_t(1) << a) | (uint64_t(1) << b);
+      if (a == b || (used & m)) continue;
+      used |= m;
+      pairs.push_back({a, b});
+    }
+    launch_swap_bits(s, pairs);
+    for (auto& q : s.layout)
+      for (auto& pr : pairs) {
+        if (q == pr.first)
+          q = pr.second;
+        else if (q == pr.second)
+          q = pr.first;
+      }
+  }
+}
+
 void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_stats* stats) {
   const bool timing = s.record_passes;
   if (timing) {
@@ -306,6 +410,9 @@ void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_s
     }
   }
   QVDG_CUDA(cudaEventRecord(s.ev_start, s.stream));
+  // The passes' layout (a relabel pass is timed with them).
+  relabel_to(s, p.run_layout.empty() ? p.target.layout : p.run_layout);
+  s.zero_state = false;
   for (size_t i = 0; i < p.passes.size(); ++i) {
     if (timing) QVDG_CUDA(cudaEventRecord(s.pass_events[i], s.stream));
     launch_pass(s, p.passes[i], dev);

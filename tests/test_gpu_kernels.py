@@ -309,6 +309,39 @@ def test_tensor_core_plain_passes_at_24_qubits(kind):
                 assert ref.max_abs_diff(st) < 1e-6, (kind, fuse)
 
 
+def test_tensor_core_plain_plans_relabel_low_bits():
+    """Tensor-core plain plans may first move three qubits onto index bits
+    1-3 (the bits whose targets slow the passes down): free on a |0...0>
+    state, one swap pass otherwise, and again when a plan runs on a state
+    left in another layout. Amplitudes in logical order match a complex128
+    run either way."""
+    from qevedo_simulator_b200 import Plan, library
+
+    relabelled = 0
+    for rows, cols, depth, seed in [(4, 5, 20, 5), (4, 6, 20, 2024), (3, 7, 16, 9)]:
+        n = rows * cols
+        ops = library.random_grid_circuit(rows, cols, depth, seed).ops()
+        psi = random_state(np.random.Generator(np.random.PCG64(seed)), n)
+        opts = options(6, staged=False, math="tensor")
+        with DeviceState(n, 64) as ref, DeviceState(n, 32) as st, Plan(ops, n, 32, opts) as plan:
+            ref.apply_ops(ops, options(4, staged=False))
+            st.execute(plan)  # from |0...0>
+            relabelled += st.layout() != list(range(n))
+            assert ref.max_abs_diff(st) < 1e-6, (n, "zero start")
+            expected = ref.amplitudes()
+            assert np.abs(st.amplitudes() - expected).max() < 1e-6
+            ref.set_amplitudes(psi)
+            ref.apply_ops(ops, options(4, staged=False))
+            st.set_amplitudes(psi)
+            st.apply_ops(ops, opts)  # from a general state
+            assert ref.max_abs_diff(st) < 1e-6, (n, "general start")
+            st.set_amplitudes(psi)
+            st.swap_physical([(1, n - 1)])
+            st.execute(plan)  # from a state in another layout
+            assert ref.max_abs_diff(st) < 1e-6, (n, "other layout")
+    assert relabelled >= 1
+
+
 @pytest.mark.parametrize("bits", [32, 64])
 @pytest.mark.parametrize("kind", ["grid", "mixed", "qft", "gates"])
 def test_plain_passes_applying_groups_gate_by_gate(oracle, bits, kind):
