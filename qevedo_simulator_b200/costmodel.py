@@ -7,8 +7,8 @@ There is no learned planner in the reference: it plans with fixed greedy
 rules (fusion in src/fusion.rs:63-170, stages in src/blocking.rs:151-302,
 defaults in src/simulator.rs:37-66). Here those rules build every candidate
 plan; the model only ranks them, and the greedy default stays both the
-fallback and the judge: `choose_measured` times the model's pick against
-the default on the device and keeps the faster.
+fallback and the judge: `choose_measured` times the model's three best
+ranked plans and the default on the device and keeps the fastest.
 
 Features come from the planner itself (qvdg_plan_features, one row of
 QVDG_PASS_FEATURES per pass, no device work). Targets are the engine's own
@@ -173,15 +173,16 @@ class CostModel:
     def predict_plan(self, ops, num_qubits: int, opts) -> float:
         return float(self.predict_passes(plan_features(ops, num_qubits, opts), num_qubits).sum())
 
+    def rank(self, ops, num_qubits: int, cands=None) -> list:
+        """[(name, options, predicted seconds)] of every candidate, fastest
+        predicted first."""
+        out = [(name, opts, self.predict_plan(ops, num_qubits, opts)) for name, opts in cands or candidates()]
+        return sorted(out, key=lambda r: r[2])
+
     def choose(self, ops, num_qubits: int, cands=None):
         """(name, options, predicted seconds) of the candidate with the least
         predicted time."""
-        best = None
-        for name, opts in cands or candidates():
-            sec = self.predict_plan(ops, num_qubits, opts)
-            if best is None or sec < best[2]:
-                best = (name, opts, sec)
-        return best
+        return self.rank(ops, num_qubits, cands)[0]
 
 
 def measure_plan(ops, num_qubits: int, opts, state: DeviceState, repeats: int = 2):
@@ -215,15 +216,16 @@ def collect(op_lists, num_qubits: int, cands=None, repeats: int = 2):
     return np.concatenate(xs), np.concatenate(ts)
 
 
-def choose_measured(model: CostModel, ops, num_qubits: int, state: DeviceState, cands=None):
-    """The model's pick, judged against the greedy default by measurement:
-    (chosen name, options, seconds, default seconds)."""
-    name, opts, _ = model.choose(ops, num_qubits, cands)
-    t_pick, _ = measure_plan(ops, num_qubits, opts, state)
+def choose_measured(model: CostModel, ops, num_qubits: int, state: DeviceState, cands=None, top: int = 3):
+    """The model's `top` picks and the greedy default, judged by
+    measurement: (chosen name, options, seconds, default seconds)."""
     t_default, _ = measure_plan(ops, num_qubits, default_options(), state)
-    if t_default <= t_pick:
-        return "default", default_options(), t_default, t_default
-    return name, opts, t_pick, t_default
+    best = ("default", default_options(), t_default)
+    for name, opts, _ in model.rank(ops, num_qubits, cands)[:top]:
+        t, _ = measure_plan(ops, num_qubits, opts, state)
+        if t < best[2]:
+            best = (name, opts, t)
+    return best[0], best[1], best[2], t_default
 
 
 def _spec(seed: int, qubits, depth):
