@@ -60,6 +60,11 @@ _CONTROLLED = {"cx": (1, "x"), "cy": (1, "y"), "cz": (1, "z"), "ch": (1, "h"), "
                "crx": (1, "rx"), "cry": (1, "ry"), "crz": (1, "rz"), "ccx": (2, "x"), "cswap": (1, "swap")}
 
 
+# Matrices of named gates by (name, parameters), bounded.
+_MATRICES: dict = {}
+_MATRICES_MAX = 65536
+
+
 @dataclass(frozen=True)
 class Gate:
     """A gate by name with its parameters, or an arbitrary unitary."""
@@ -88,15 +93,23 @@ class Gate:
         return controls, Gate(target, self.params)
 
     def matrix(self) -> np.ndarray:
-        """The gate's unitary (src/circuit.rs:133-202)."""
+        """The gate's unitary (src/circuit.rs:133-202).
+
+        Named gates share one read-only array per (name, parameters): a
+        circuit repeats a handful of gates many times, and building each
+        small array again dominates lowering a circuit to ops.
+        """
+        if self.name == "unitary":
+            return np.array(self.unitary, dtype=np.complex128)
+        return _named_matrix(self.name, self.params)
+
+    def _build_matrix(self) -> np.ndarray:
         form = self.controlled_form()
         if form is not None:
             controls, target = form
             return _controlled(target.matrix(), controls, (1 << controls) - 1)
         n, p = self.name, self.params
         c = complex
-        if n == "unitary":
-            return np.array(self.unitary, dtype=np.complex128)
         if n == "id":
             return np.eye(2, dtype=np.complex128)
         if n == "h":
@@ -160,14 +173,33 @@ class Op:
         return list(self.targets) + [q for q, _ in self.controls]
 
 
+def _named_matrix(name: str, params: tuple) -> np.ndarray:
+    """Gate(name, params).matrix() through the shared read-only cache."""
+    key = (name, params)
+    try:
+        hit = _MATRICES.get(key)
+    except TypeError:  # unhashable parameters
+        return Gate(name, params)._build_matrix()
+    if hit is None:
+        hit = Gate(name, params)._build_matrix()
+        hit.flags.writeable = False
+        if len(_MATRICES) >= _MATRICES_MAX:
+            _MATRICES.clear()
+        _MATRICES[key] = hit
+    return hit
+
+
 def gate_op(gate: Gate, qubits) -> Op:
     """simulator::gate_op (src/simulator.rs:106-119): controls stay separate so
     the kernel touches only the controlled part of the state."""
-    form = gate.controlled_form()
+    form = _CONTROLLED.get(gate.name)
     if form is not None:
         controls, target = form
-        return Op(list(qubits[controls:]), [(q, True) for q in qubits[:controls]], target.matrix())
-    return Op(list(qubits), [], gate.matrix())
+        return Op(list(qubits[controls:]), [(q, True) for q in qubits[:controls]],
+                  _named_matrix(target, gate.params))
+    if gate.name == "unitary":
+        return Op(list(qubits), [], gate.matrix())
+    return Op(list(qubits), [], _named_matrix(gate.name, gate.params))
 
 
 class Circuit:

@@ -125,20 +125,32 @@ std::vector<HOp> lower_ops(const qvdg_op* ops, size_t n, uint32_t num_qubits) {
   out.reserve(n);
   for (size_t i = 0; i < n; ++i) {
     const qvdg_op& o = ops[i];
-    require(o.num_targets <= 16 && o.num_controls <= 64, "op " + std::to_string(i) + " is too wide");
-    require(o.num_targets == 0 || (o.targets && o.matrix), "op " + std::to_string(i) + " has no targets or matrix");
-    require(o.num_controls == 0 || o.controls, "op " + std::to_string(i) + " has no control list");
+    // Messages are built only on failure.
+    if (!(o.num_targets <= 16 && o.num_controls <= 64)) require(false, "op " + std::to_string(i) + " is too wide");
+    if (!(o.num_targets == 0 || (o.targets && o.matrix)))
+      require(false, "op " + std::to_string(i) + " has no targets or matrix");
+    if (!(o.num_controls == 0 || o.controls)) require(false, "op " + std::to_string(i) + " has no control list");
     HOp h;
-    std::vector<uint32_t> seen;
-    for (uint32_t j = 0; j < o.num_targets; ++j) h.targets.push_back(o.targets[j]);
+    h.targets.assign(o.targets, o.targets + o.num_targets);
+    h.controls.reserve(o.num_controls);
     for (uint32_t j = 0; j < o.num_controls; ++j)
       h.controls.push_back({o.controls[j], o.control_values ? o.control_values[j] != 0 : true});
-    for (uint32_t q : h.qubits()) {
-      require(q < num_qubits, "qubit " + std::to_string(q) + " out of range for " + std::to_string(num_qubits) +
-                                  " qubits");
-      require(std::find(seen.begin(), seen.end(), q) == seen.end(),
-              "op " + std::to_string(i) + " uses qubit " + std::to_string(q) + " twice");
-      seen.push_back(q);
+    uint64_t seen = 0;  // qubits below 64 seen so far
+    const uint32_t width = o.num_targets + o.num_controls;
+    for (uint32_t j = 0; j < width; ++j) {
+      const uint32_t q = j < o.num_targets ? o.targets[j] : o.controls[j - o.num_targets];
+      if (q >= num_qubits)
+        require(false, "qubit " + std::to_string(q) + " out of range for " + std::to_string(num_qubits) + " qubits");
+      bool twice;
+      if (q < 64) {
+        twice = (seen >> q) & 1;
+        seen |= uint64_t(1) << q;
+      } else {
+        twice = false;
+        for (uint32_t k = 0; k < j; ++k)
+          twice = twice || (k < o.num_targets ? o.targets[k] : o.controls[k - o.num_targets]) == q;
+      }
+      if (twice) require(false, "op " + std::to_string(i) + " uses qubit " + std::to_string(q) + " twice");
     }
     const size_t dim = size_t(1) << o.num_targets;
     h.matrix = HMatrix(dim);

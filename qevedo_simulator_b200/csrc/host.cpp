@@ -2,6 +2,7 @@
 #include "host.hpp"
 
 #include <atomic>
+#include <cmath>
 #include <exception>
 #include <mutex>
 #include <stdexcept>
@@ -112,42 +113,56 @@ namespace {
 // One growth sweep of a fused group over the ops after its seed
 // (src/fusion.rs:126-170), on qubit bit masks: an op joins when it touches
 // no blocked qubit and fits; otherwise its qubits become blocked. `pre`:
-// qubits of unfused ops before the seed (they block from the start).
-void grow(const std::vector<uint64_t>& mask, const std::vector<size_t>& width, const std::vector<bool>& done,
-          std::vector<bool>& taken, size_t seed, uint64_t pre, std::vector<size_t>& members, uint64_t& qubits,
-          size_t max_qubits, bool connected_only) {
+// qubits of unfused ops before the seed (they block from the start). The
+// sweep may stop early once the group has max_qubits qubits, all blocked:
+// a later op could then join only if it touched no qubit at all, and
+// `can_stop` says that no op is like that.
+void grow(const FusionInput& in, const std::vector<uint8_t>& done, std::vector<uint8_t>& taken, size_t seed,
+          uint64_t pre, std::vector<size_t>& members, uint64_t& qubits, size_t max_qubits, bool connected_only,
+          bool can_stop) {
   uint64_t blocked = pre;
-  for (size_t i = seed + 1; i < mask.size(); ++i) {
+  const size_t n = in.mask.size();
+  for (size_t i = seed + 1; i < n; ++i) {
     if (done[i] || taken[i]) continue;
     if (connected_only && (qubits & ~blocked) == 0) break;
-    const uint64_t m = mask[i], fresh = m & ~qubits;
+    const uint64_t m = in.mask[i], fresh = m & ~qubits;
     const bool connected = fresh != m;
-    const bool fits = width[i] <= max_qubits && size_t(__builtin_popcountll(qubits | m)) <= max_qubits;
+    const bool fits = in.width[i] <= max_qubits && size_t(__builtin_popcountll(qubits | m)) <= max_qubits;
     if (!(m & blocked) && fits && (connected || !connected_only)) {
       taken[i] = true;
       members.push_back(i);
       qubits |= m;
     } else {
       blocked |= m;
+      if (can_stop && (qubits & ~blocked) == 0 && size_t(__builtin_popcountll(qubits)) >= max_qubits) break;
     }
   }
 }
 
 }  // namespace
 
-std::vector<FusedGroup> fuse_groups_lookahead(const std::vector<HOp>& ops, size_t max_qubits,
-                                              const std::function<bool(const HOp&)>& fusable, size_t lookahead) {
+FusionInput fusion_input(const std::vector<HOp>& ops, const std::function<bool(const HOp&)>& fusable) {
+  FusionInput in;
   const size_t n = ops.size();
-  std::vector<uint64_t> mask(n, 0);
-  std::vector<size_t> width(n);
+  in.mask.assign(n, 0);
+  in.width.resize(n);
   for (size_t i = 0; i < n; ++i) {
-    for (uint32_t q : ops[i].qubits()) {
+    auto add = [&](uint32_t q) {
       if (q >= 64) throw std::logic_error("fusion supports qubits 0..63");
-      mask[i] |= uint64_t(1) << q;
-    }
-    width[i] = fusable(ops[i]) ? ops[i].width() : SIZE_MAX;
+      in.mask[i] |= uint64_t(1) << q;
+    };
+    for (uint32_t q : ops[i].targets) add(q);
+    for (auto& c : ops[i].controls) add(c.first);
+    in.width[i] = fusable(ops[i]) ? ops[i].width() : SIZE_MAX;
+    in.any_empty = in.any_empty || in.mask[i] == 0;
   }
-  std::vector<bool> done(n, false), taken(n, false);
+  return in;
+}
+
+std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_qubits, size_t lookahead) {
+  const size_t n = in.mask.size();
+  const std::vector<uint64_t>& mask = in.mask;
+  std::vector<uint8_t> done(n, 0), taken(n, 0);
   std::vector<FusedGroup> groups;
   size_t first = 0;
   std::vector<size_t> members, best_members;
@@ -167,9 +182,9 @@ std::vector<FusedGroup> fuse_groups_lookahead(const std::vector<HOp>& ops, size_
         members.assign(1, s);
         uint64_t qubits = mask[s];
         taken[s] = true;
-        if (width[s] <= max_qubits) {
-          grow(mask, width, done, taken, s, pending, members, qubits, max_qubits, true);
-          grow(mask, width, done, taken, s, pending, members, qubits, max_qubits, false);
+        if (in.width[s] <= max_qubits) {
+          grow(in, done, taken, s, pending, members, qubits, max_qubits, true, false);
+          grow(in, done, taken, s, pending, members, qubits, max_qubits, false, !in.any_empty);
         }
         for (size_t i : members) taken[i] = false;
         if (members.size() > best_members.size()) {
@@ -190,6 +205,11 @@ std::vector<FusedGroup> fuse_groups_lookahead(const std::vector<HOp>& ops, size_
   return groups;
 }
 
+std::vector<FusedGroup> fuse_groups_lookahead(const std::vector<HOp>& ops, size_t max_qubits,
+                                              const std::function<bool(const HOp&)>& fusable, size_t lookahead) {
+  return fuse_groups_lookahead(fusion_input(ops, fusable), max_qubits, lookahead);
+}
+
 std::vector<FusedGroup> fuse_groups(const std::vector<HOp>& ops, size_t max_qubits,
                                     const std::function<bool(const HOp&)>& fusable) {
   return fuse_groups_lookahead(ops, max_qubits, fusable, 0);
@@ -199,8 +219,14 @@ std::vector<FusedGroup> fuse_groups(const std::vector<HOp>& ops, size_t max_qubi
 // matrix: each set of rows that differ only in the gate's bits is mixed by g.
 // Same products, same zero skipping and same order of additions (ascending
 // row of the embedded matrix) as mul, so the result is identical.
+//
+// `live` (optional) tracks the sparsity of a product grown from the
+// identity: entry (r, c) is exactly +0 unless r ^ c lies within *live (the
+// positions of every gate applied so far). Only those columns are computed;
+// the others would come out +0 (sums of +-0 products of finite entries,
+// starting from +0), which they already hold.
 void apply_left(HMatrix& m, const HMatrix& g, const std::vector<uint32_t>& gate_qubits,
-                const std::vector<uint32_t>& qubits) {
+                const std::vector<uint32_t>& qubits, size_t* live) {
   const size_t k = gate_qubits.size(), gd = size_t(1) << k;
   std::vector<size_t> off(gd, 0);
   size_t mask = 0;
@@ -224,6 +250,45 @@ void apply_left(HMatrix& m, const HMatrix& g, const std::vector<uint32_t>& gate_
     for (size_t t : order)
       if (norm2(g.at(s, t)) != 0.0) rows[s].push_back({t, g.at(s, t)});
   const size_t dim = m.dim;
+  if (live) {
+    bool finite = true;
+    for (const C& x : g.a) finite = finite && std::isfinite(x.re) && std::isfinite(x.im);
+    *live = finite ? ((*live | mask) & (dim - 1)) : dim - 1;
+    if (*live != dim - 1) {
+      // Columns that can be nonzero in the rows of block b: (b & ~u) | sub,
+      // sub a subset of u (ascending).
+      const size_t u = *live;
+      std::vector<size_t> sub;
+      size_t x = 0;
+      do {
+        sub.push_back(x);
+        x = (x - u) & u;
+      } while (x != 0);
+      const size_t ns = sub.size();
+      std::vector<C> in(gd * ns);
+      for (size_t b = 0; b < dim; ++b) {
+        if (b & mask) continue;
+        const size_t cb = b & ~u;
+        for (size_t t = 0; t < gd; ++t) {
+          const C* src = &m.a[(b | off[t]) * dim];
+          for (size_t j = 0; j < ns; ++j) in[t * ns + j] = src[cb | sub[j]];
+        }
+        for (size_t s = 0; s < gd; ++s) {
+          C* dst = &m.a[(b | off[s]) * dim];
+          for (size_t j = 0; j < ns; ++j) {
+            C acc{0.0, 0.0};
+            for (const Entry& e : rows[s]) {
+              const C p = e.x * in[e.t * ns + j];
+              acc.re += p.re;
+              acc.im += p.im;
+            }
+            dst[cb | sub[j]] = acc;
+          }
+        }
+      }
+      return;
+    }
+  }
   std::vector<C> in(gd * dim);
   for (size_t b = 0; b < dim; ++b) {
     if (b & mask) continue;
@@ -249,11 +314,12 @@ HOp fuse_group(const std::vector<HOp>& ops, const FusedGroup& g) {
   if (members.size() == 1) return ops[members[0]];
   {
     HMatrix m = HMatrix::identity(qubits.size());
+    size_t live = 0;
     for (size_t i : members) {
       std::vector<uint32_t> oq;
       HMatrix om;
       ops[i].full(oq, om);
-      apply_left(m, om, oq, qubits);
+      apply_left(m, om, oq, qubits, &live);
     }
     HOp f;
     f.targets = qubits;

@@ -69,6 +69,17 @@ std::vector<FusedGroup> fuse_groups(const std::vector<HOp>& ops, size_t max_qubi
 std::vector<FusedGroup> fuse_groups_lookahead(const std::vector<HOp>& ops, size_t max_qubits,
                                               const std::function<bool(const HOp&)>& fusable, size_t lookahead);
 
+// What the fusion reads of each op: its qubits as a bit mask and its width
+// (SIZE_MAX where it may not be merged). Built once, shared by several
+// fusions of the same ops.
+struct FusionInput {
+  std::vector<uint64_t> mask;
+  std::vector<size_t> width;
+  bool any_empty = false;  // some op touches no qubit
+};
+FusionInput fusion_input(const std::vector<HOp>& ops, const std::function<bool(const HOp&)>& fusable);
+std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_qubits, size_t lookahead);
+
 // The group's ops as one op (the product matrix on its qubits; a group of one
 // op is that op, controls kept).
 HOp fuse_group(const std::vector<HOp>& ops, const FusedGroup& g);

@@ -129,19 +129,27 @@ void append_tc_gate(const HMatrix& m, std::vector<uint8_t>& blob) {
   blob.resize(base + 4 * kd * kd, 0);
   uint8_t* hi = blob.data() + base;
   uint8_t* lo = hi + 2 * kd * kd;
-  for (size_t n = 0; n < kd; ++n)
-    for (size_t kk = 0; kk < kd; ++kk) {
-      const C e = m.at(n % half, kk % half);
-      double v;
-      if (n < half)
-        v = kk < half ? e.re : -e.im;
-      else
-        v = kk < half ? e.im : e.re;
-      const uint16_t h = to_bf16(float(v));
-      const uint16_t l = to_bf16(float(v - double(from_bf16(h))));
-      const size_t off = (n / 8) * (kd * 16) + (kk / 8) * 128 + (n % 8) * 16 + (kk % 8) * 2;
-      std::memcpy(hi + off, &h, 2);
-      std::memcpy(lo + off, &l, 2);
+  auto split = [](double v, uint16_t& h, uint16_t& l) {
+    h = to_bf16(float(v));
+    l = to_bf16(float(v - double(from_bf16(h))));
+  };
+  auto put = [&](size_t n, size_t kk, uint16_t h, uint16_t l) {
+    const size_t off = (n / 8) * (kd * 16) + (kk / 8) * 128 + (n % 8) * 16 + (kk % 8) * 2;
+    std::memcpy(hi + off, &h, 2);
+    std::memcpy(lo + off, &l, 2);
+  };
+  // Entry (r, c) of M fills one element of each quadrant.
+  for (size_t r = 0; r < half; ++r)
+    for (size_t c = 0; c < half; ++c) {
+      const C e = m.at(r, c);
+      uint16_t h, l;
+      split(e.re, h, l);
+      put(r, c, h, l);
+      put(r + half, c + half, h, l);
+      split(-e.im, h, l);
+      put(r, c + half, h, l);
+      split(e.im, h, l);
+      put(r + half, c, h, l);
     }
 }
 
@@ -408,7 +416,7 @@ PlainTcBlob plain_tc_blob(const Target& s, const HOp& op) {
 }
 
 LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig& cfg, StageUpload& up,
-                       const PlainTcBlob* pre) {
+                       PlainTcBlob* pre) {
   if (p.block) return lower_block_pass(s, p, up);
   if (p.staged && cfg.tensor && cfg.low_bits >= 1 && tensor_pass_ok(s, p)) return lower_tensor_pass(s, p, cfg, up);
   if (p.staged && cfg.reg && cfg.low_bits >= 1 && register_pass_ok(s, p)) return lower_register_pass(s, p, cfg, up);
@@ -425,7 +433,7 @@ LoweredPass lower_pass(const Target& s, const PlannedPass& p, const StageConfig&
         throw Error(QVDG_ERR_UNSUPPORTED, "diagonal gates on more than 10 qubits are not supported");
       g.matrix_offset = up.push_matrix(op.matrix.diagonal_entries());
     } else if (plain_tc_eligible(s, p, cfg)) {
-      const PlainTcBlob b = pre ? *pre : plain_tc_blob(s, op);
+      const PlainTcBlob b = pre ? std::move(*pre) : plain_tc_blob(s, op);
       g.targets = b.targets;
       g.tensor = true;
       blob_align(up.tc);

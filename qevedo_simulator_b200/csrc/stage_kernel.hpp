@@ -80,9 +80,10 @@ struct PlainTcBlob {
 };
 bool plain_tc_eligible(const Target& t, const PlannedPass& p, const StageConfig& cfg);
 PlainTcBlob plain_tc_blob(const Target& t, const HOp& op);
-// `pre`: the pass's plain_tc_blob when the caller computed it already.
+// `pre`: the pass's plain_tc_blob when the caller computed it already
+// (moved from).
 LoweredPass lower_pass(const Target& t, const PlannedPass& p, const StageConfig& cfg, StageUpload& up,
-                       const PlainTcBlob* pre = nullptr);
+                       PlainTcBlob* pre = nullptr);
 void launch_pass(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
 void launch_stage_tc(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev);
 // Plain passes applying a fused group gate by gate in registers (block.cu).

@@ -179,6 +179,8 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
   prog.cfg = stage_config(t, opt.tile_qubits, opt.staged && opt.math == QVDG_MATH_TENSOR);
   prog.cfg.plain_tensor = !opt.staged && opt.math == QVDG_MATH_TENSOR && t.bits == 32;
   std::vector<PlannedPass> passes;
+  // Tensor-core plain passes' bf16 matrices (by pass; empty for the others).
+  std::vector<PlainTcBlob> blobs;
   if (opt.staged) {
     passes = plan_stages(ops, t.layout, t.n, prog.cfg, max_fused);
   } else {
@@ -194,8 +196,8 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     // cheapest is kept (50 passes instead of 55 on the 30-qubit grid circuit
     // at fusion 6, 64 instead of 70 at fusion 5; at fusion 4 the seeds would
     // add passes). Other plain plans keep the reference's greedy fusion.
-    const auto all = [](const HOp&) { return true; };
-    std::vector<FusedGroup> groups = fuse_groups(ops, max_fused, all);
+    const FusionInput fin = fusion_input(ops, [](const HOp&) { return true; });
+    std::vector<FusedGroup> groups = fuse_groups_lookahead(fin, max_fused, 0);
     if (opt.math == QVDG_MATH_TENSOR && max_fused >= 5 && t.n >= 13) {
       // Candidate fusions (seed lookahead 0-8) and, for each, the three
       // qubits to place on physical bits 1-3 (a relabel that costs nothing
@@ -208,8 +210,10 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       std::vector<uint32_t> at(t.n);  // physical -> logical
       for (uint32_t q = 0; q < t.n; ++q) at[t.layout[q]] = q;
       const uint64_t now = (uint64_t(1) << at[1]) | (uint64_t(1) << at[2]) | (uint64_t(1) << at[3]);
-      parallel_for(cand.size(), [&](size_t i) {
-        cand[i] = i == 0 ? groups : fuse_groups_lookahead(ops, max_fused, all, i);
+      // The longest lookaheads first: they take the longest.
+      parallel_for(cand.size(), [&](size_t j) {
+        const size_t i = cand.size() - 1 - j;
+        cand[i] = i == 0 ? groups : fuse_groups_lookahead(fin, max_fused, i);
         std::vector<uint64_t> gm;
         for (const FusedGroup& g : cand[i]) {
           uint64_t m = 0;
@@ -312,21 +316,30 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       p.ops.resize(1);
       products.push_back(gi);
     }
+    // Each product and, for a tensor-core pass, its bf16 matrices (on the
+    // layout the passes run with) in one task.
+    Target rt = t;
+    if (!prog.run_layout.empty()) rt.layout = prog.run_layout;
+    blobs.resize(passes.size());
     const bool wide = max_fused >= 5 && products.size() >= 8;
-    parallel_for(products.size(), [&](size_t j) { passes[products[j]].ops[0] = fuse_group(ops, groups[products[j]]); },
-                 wide ? 0u : 1u);
+    parallel_for(products.size(), [&](size_t j) {
+      PlannedPass& p = passes[products[j]];
+      p.ops[0] = fuse_group(ops, groups[products[j]]);
+      if (plain_tc_eligible(rt, p, prog.cfg)) blobs[products[j]] = plain_tc_blob(rt, p.ops[0]);
+    }, wide ? 0u : 1u);
   }
   // Passes are lowered on the layout they run with.
   Target run_target = t;
   if (!prog.run_layout.empty()) run_target.layout = prog.run_layout;
   const Target& tt = run_target;
-  // Tensor-core plain passes' bf16 matrices, also on host threads.
-  std::vector<PlainTcBlob> blobs(passes.size());
-  std::vector<size_t> tc;
-  for (size_t i = 0; i < passes.size(); ++i)
-    if (plain_tc_eligible(tt, passes[i], prog.cfg)) tc.push_back(i);
-  parallel_for(tc.size(), [&](size_t j) { blobs[tc[j]] = plain_tc_blob(tt, passes[tc[j]].ops[0]); },
-               tc.size() >= 8 ? 0u : 1u);
+  blobs.resize(passes.size());
+  size_t tc_bytes = 0;
+  for (size_t i = 0; i < passes.size(); ++i) {
+    if (blobs[i].blob.empty() && plain_tc_eligible(tt, passes[i], prog.cfg))
+      blobs[i] = plain_tc_blob(tt, passes[i].ops[0]);
+    tc_bytes += blobs[i].blob.size() + 16;
+  }
+  prog.upload.tc.reserve(tc_bytes);
   const double state_bytes = double(uint64_t(t.bits == 32 ? 8 : 16) << t.n);
   for (size_t pi = 0; pi < passes.size(); ++pi) {
     const PlannedPass& p = passes[pi];
