@@ -84,24 +84,27 @@ class PackedOps:
 
     def __init__(self, ops):
         n = len(ops)
-        qubits, values, mats = [], [], []
-        ks = np.empty(max(n, 1), dtype=np.uint32)
-        cs = np.empty(max(n, 1), dtype=np.uint32)
-        for i, op in enumerate(ops):
-            k, c = len(op.targets), len(op.controls)
-            ks[i], cs[i] = k, c
-            qubits.extend(op.targets)
-            values.extend([0] * k)
-            for q, v in op.controls:
+        qubits, values, mats, ks, cs = [], [], [], [], []
+        for op in ops:
+            t, ctl = op.targets, op.controls
+            ks.append(len(t))
+            cs.append(len(ctl))
+            qubits += t
+            values += [0] * len(t)
+            for q, v in ctl:
                 qubits.append(q)
                 values.append(1 if v else 0)
-            m = np.ascontiguousarray(op.matrix, dtype=np.complex128).reshape(-1)
-            if m.size != 4 ** k:
+            mats.append(op.matrix)
+        ks = np.array(ks or [0], dtype=np.uint32)
+        cs = np.array(cs or [0], dtype=np.uint32)
+        if n:
+            sizes = np.fromiter((np.size(m) for m in mats), dtype=np.uint64, count=n)
+            if np.any(sizes != np.uint64(4) ** ks.astype(np.uint64)):
                 raise ValueError("op matrix does not match its targets")
-            mats.append(m)
         self._q = np.array(qubits or [0], dtype=np.uint32)
         self._v = np.array(values or [0], dtype=np.uint8)
-        self._m = np.concatenate(mats).view(np.float64) if mats else np.zeros(2)
+        self._m = (np.concatenate([np.ravel(m) for m in mats], dtype=np.complex128).view(np.float64)
+                   if mats else np.zeros(2))
         self._ops = np.zeros(max(n, 1), dtype=_OP_DTYPE)
         if n:
             ks, cs = ks[:n], cs[:n]

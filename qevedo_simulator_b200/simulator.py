@@ -75,6 +75,11 @@ def bitstring(bits) -> str:
     return "".join("1" if b else "0" for b in reversed(bits))
 
 
+def key_bitstring(key: int, num_clbits: int) -> str:
+    """bitstring() of the classical bits packed in `key` (bit c = clbit c)."""
+    return format(key, "b").zfill(num_clbits) if num_clbits else ""
+
+
 def count_outcomes(outcomes: np.ndarray, measures, num_clbits: int) -> dict:
     """Counts from sampled basis states (src/simulator.rs:187-230): each shot
     becomes an integer key (bit c = classical bit c), keys are counted, and
@@ -86,7 +91,7 @@ def count_outcomes(outcomes: np.ndarray, measures, num_clbits: int) -> dict:
         uniq, cnt = np.unique(keys, return_counts=True)
         out = {}
         for k, n in zip(uniq.tolist(), cnt.tolist()):
-            out[bitstring([(k >> c) & 1 for c in range(num_clbits)])] = n
+            out[key_bitstring(k, num_clbits)] = n
         return dict(sorted(out.items()))
     out = {}
     for index in outcomes.tolist():
@@ -142,8 +147,8 @@ def run(circuit: Circuit, shots: int = 1024, *, backend: str = "auto", seed: int
                 # Keys built, sorted and counted on the device; only the
                 # distinct keys come back to be formatted.
                 keys, cnt = st.sample_counts(uniforms(rng, shots), measures)
-                result.counts = {bitstring([(int(k) >> c) & 1 for c in range(circuit.num_clbits)]): int(n)
-                                 for k, n in zip(keys, cnt)}
+                result.counts = {key_bitstring(k, circuit.num_clbits): n
+                                 for k, n in zip(keys.tolist(), cnt.tolist())}
                 result.counts = dict(sorted(result.counts.items()))
             else:
                 outcomes = st.sample_unordered(uniforms(rng, shots))
