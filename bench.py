@@ -372,6 +372,7 @@ def run_ours(args, rank: int, world: int):
     # End to end through the public API: plan on the host, upload gate data
     # from pinned memory, run, sample SHOTS shots, outcomes back to the host.
     e2e = []
+    st.set_pass_timing(False)  # the user's path records no per-pass events
     staged = bool(tuned_opts.staged)
     math_name = {0: "fp32", 1: "tensor", 2: "gates"}[int(tuned_opts.math)]
     for i in range(args.warmup + args.steps):

@@ -11,8 +11,7 @@
 //     src/measure.rs:13 and src/simd.rs:71-97), in physical index order;
 //   - p = re*re + im*im in f64 without contraction (__dmul_rn/__dadd_rn);
 //   - each chunk sum is one sequential left fold in index order (one lane
-//     owns a chunk; a warp loads 32 chunks' data coalesced and transposes it
-//     through shared memory);
+//     owns a chunk; a warp streams 32 chunks' data through shared memory);
 //   - the chunk prefix is sequential; targets = u * total are sorted in f64
 //     total order; bounds are partition points of the prefix;
 //   - the walk adds nonzero p in index order from prefix[chunk] and emits an
@@ -158,51 +157,98 @@ __global__ void k_probs(const cplx_t<T>* __restrict__ psi, double* __restrict__ 
 }
 
 // ---------------------------------------------------------------- sampler
-// Amplitudes per lane per step: two complex64 (one 16-byte load) or one
-// complex128.
-template <typename T>
-struct Step {
-  static constexpr int per_lane = sizeof(T) == 4 ? 2 : 1;
-  static constexpr int width = 32 * per_lane;  // amplitudes per chunk per step
-};
-
-constexpr int kSampWarps = 2;
-
 // Pass 1: sequential f64 sum of p over each chunk (src/measure.rs:110-118).
+// A warp owns 32 consecutive chunks and lane c folds chunk c, in index
+// order. The chunks stream through shared memory in windows of 256 bytes
+// per chunk, copied with cp.async (16 bytes a lane, lanes 0-15 on one chunk
+// and 16-31 on the next) kSumStages - 1 windows ahead of the fold, so each
+// warp keeps 16 KB of loads in flight. Rows are padded by 16 bytes: the
+// fold's 16-byte reads (one row per lane) then hit distinct banks.
+constexpr int kSumStages = 3;
+constexpr int kSumWindow = 256;             // bytes per chunk per window
+constexpr int kSumRow = kSumWindow + 16;    // padded row in shared memory
+constexpr int kSumStageBytes = 32 * kSumRow;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// p of the amplitudes of one 16-byte read, in index order.
 template <typename T>
-__global__ void __launch_bounds__(32 * kSampWarps) k_chunk_sums(const cplx_t<T>* __restrict__ psi, uint64_t len,
-                                                                 uint64_t chunk_len, uint64_t nchunks,
-                                                                 double* __restrict__ sums) {
-  constexpr int W = Step<T>::width;
-  __shared__ double sp[kSampWarps][32][W + 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint64_t chunk0 = (uint64_t(blockIdx.x) * kSampWarps + warp) * 32;
+__device__ __forceinline__ double fold16(double s, const float4& v);
+template <>
+__device__ __forceinline__ double fold16<float>(double s, const float4& v) {
+  s = __dadd_rn(s, prob<float>(make_float2(v.x, v.y)));
+  return __dadd_rn(s, prob<float>(make_float2(v.z, v.w)));
+}
+template <>
+__device__ __forceinline__ double fold16<double>(double s, const float4& v) {
+  return __dadd_rn(s, prob<double>(*reinterpret_cast<const double2*>(&v)));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32) k_chunk_sums(const cplx_t<T>* __restrict__ psi, uint64_t len,
+                                                   uint64_t chunk_len, uint64_t nchunks,
+                                                   double* __restrict__ sums) {
+  constexpr int kAmp = int(sizeof(cplx_t<T>));  // 8 or 16 bytes
+  constexpr int kPerWin = kSumWindow / kAmp;     // amplitudes per chunk per window
+  constexpr int kPerRead = 16 / kAmp;            // amplitudes per 16-byte read
+  __shared__ __align__(16) unsigned char sbuf[kSumStages][kSumStageBytes];
+  const int lane = threadIdx.x;
+  const uint64_t chunk0 = uint64_t(blockIdx.x) * 32;
   if (chunk0 >= nchunks) return;
   const int live = int(umin64(32, nchunks - chunk0));
-  double s = 0.0;
-  constexpr int PL = Step<T>::per_lane;
-  for (uint64_t pos = 0; pos < chunk_len; pos += W) {
-    // Eight chunks' windows in flight at a time (loads first, then the
-    // probabilities into shared memory).
-    for (int c0 = 0; c0 < live; c0 += 8) {
-      cplx_t<T> v[8][PL];
-#pragma unroll
-      for (int u = 0; u < 8; ++u)
-#pragma unroll
-        for (int e = 0; e < PL; ++e) {
-          const uint64_t i = (chunk0 + c0 + u) * chunk_len + pos + uint64_t(lane) * PL + e;
-          const bool ok = c0 + u < live && i < len && pos + uint64_t(lane) * PL + e < chunk_len;
-          v[u][e] = ok ? psi[i] : make_c<T>(T(0), T(0));
-        }
-#pragma unroll
-      for (int u = 0; u < 8; ++u)
-#pragma unroll
-        for (int e = 0; e < PL; ++e)
-          if (c0 + u < live) sp[warp][c0 + u][lane * PL + e] = prob<T>(v[u][e]);
+  // Windows of the warp's first chunk (no later chunk is longer).
+  const uint64_t windows = (umin64(chunk_len, len - chunk0 * chunk_len) + kPerWin - 1) / kPerWin;
+  const unsigned char* src0 = reinterpret_cast<const unsigned char*>(psi);
+  auto issue = [&](uint64_t w, int stage) {
+    const int half = lane >> 4, sub = lane & 15;
+    for (int r = 0; r < 16; ++r) {
+      const int c = 2 * r + half;
+      if (c >= live) break;
+      const uint64_t chunk = chunk0 + c;
+      const uint64_t end_b = umin64(chunk_len, len - chunk * chunk_len) * kAmp;
+      const uint64_t off_b = w * kSumWindow + uint64_t(sub) * 16;
+      unsigned char* dst = &sbuf[stage][c * kSumRow + sub * 16];
+      const unsigned char* src = src0 + chunk * chunk_len * kAmp + off_b;
+      if (off_b + 16 <= end_b)
+        cp_async16(dst, src);
+      else if (off_b < end_b)  // one complex64 left (a state of one amplitude)
+        *reinterpret_cast<cplx_t<T>*>(dst) = *reinterpret_cast<const cplx_t<T>*>(src);
     }
+  };
+  for (int st = 0; st < kSumStages - 1; ++st) {
+    if (uint64_t(st) < windows) issue(uint64_t(st), st);
+    cp_async_commit();
+  }
+  double s = 0.0;
+  const uint64_t my_end = lane < live ? umin64(chunk_len, len - (chunk0 + lane) * chunk_len) : 0;
+  for (uint64_t w = 0; w < windows; ++w) {
+    const uint64_t ahead = w + kSumStages - 1;
+    if (ahead < windows) issue(ahead, int(ahead % kSumStages));
+    cp_async_commit();
+    cp_async_wait<kSumStages - 1>();  // window w has landed
     __syncwarp();
-    if (lane < live)
-      for (int j = 0; j < W; ++j) s = __dadd_rn(s, sp[warp][lane][j]);
+    const uint64_t pos = w * kPerWin;
+    if (pos < my_end) {
+      const float4* row = reinterpret_cast<const float4*>(&sbuf[w % kSumStages][lane * kSumRow]);
+      const uint64_t n = umin64(kPerWin, my_end - pos);
+      if (n == uint64_t(kPerWin)) {
+#pragma unroll
+        for (int j = 0; j < kPerWin / kPerRead; ++j) s = fold16<T>(s, row[j]);
+      } else {
+        const cplx_t<T>* amps = reinterpret_cast<const cplx_t<T>*>(row);
+        for (uint64_t j = 0; j < n; ++j) s = __dadd_rn(s, prob<T>(amps[j]));
+      }
+    }
     __syncwarp();
   }
   if (lane < live) sums[chunk0 + lane] = s;
@@ -512,8 +558,15 @@ size_t sample_device_t(StateImpl& s, size_t shots, const double* uniforms_host, 
   const cplx_t<T>* psi = static_cast<const cplx_t<T>*>(s.amp);
 
   QVDG_CUDA(cudaMemcpyAsync(uni, uniforms_host, shots * 8, cudaMemcpyHostToDevice, s.stream));
-  const unsigned chunk_blocks = unsigned((nchunks + 32 * kSampWarps - 1) / (32 * kSampWarps));
-  k_chunk_sums<T><<<chunk_blocks, 32 * kSampWarps, 0, s.stream>>>(psi, len, chunk_len, nchunks, sums);
+  static bool carveout = false;  // per instantiation
+  if (!carveout) {
+    // Eight one-warp blocks per SM (26 KB of shared memory each): all of the
+    // unified L1/shared storage as shared memory.
+    QVDG_CUDA(cudaFuncSetAttribute(k_chunk_sums<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   int(cudaSharedmemCarveoutMaxShared)));
+    carveout = true;
+  }
+  k_chunk_sums<T><<<unsigned((nchunks + 31) / 32), 32, 0, s.stream>>>(psi, len, chunk_len, nchunks, sums);
   QVDG_LAUNCH_CHECK();
   k_prefix<<<1, 256, 0, s.stream>>>(sums, nchunks, prefix);
   QVDG_LAUNCH_CHECK();
