@@ -165,7 +165,9 @@ std::vector<HOp> lower_ops(const qvdg_op* ops, size_t n, uint32_t num_qubits) {
 // Plan, upload and run `ops` on the state (the reference's apply_ops,
 // src/simulator.rs:122-147).
 void apply_program(StateImpl& s, const std::vector<HOp>& ops, const qvdg_options& opt, qvdg_stats* stats) {
-  const Program prog = build_program(target_of(s), ops, opt);
+  // One-shot: a beam search where a pass streams at least 8 GB.
+  const Program prog =
+      build_program(target_of(s), ops, opt, s.n >= 29 ? FusionSearch::Beam : FusionSearch::Lookahead);
   const DeviceUpload dev = upload_program(s, prog, s.work);
   run_program(s, prog, dev, stats);
 }
@@ -487,7 +489,7 @@ qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const
     qvdg_plan* plan = new qvdg_plan();
     plan->device_id = dev;
     try {
-      plan->program = build_program(t, lower_ops(ops, num_ops, num_qubits), opt);
+      plan->program = build_program(t, lower_ops(ops, num_ops, num_qubits), opt, FusionSearch::Thorough);
       plan->program.gates = num_ops;
       // Gate programs and matrices in the plan's precision, one device copy.
       const StageUpload& up = plan->program.upload;
@@ -653,7 +655,7 @@ qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, con
     t.n = num_qubits;
     t.bits = int(precision_bits);
     for (uint32_t q = 0; q < num_qubits; ++q) t.layout.push_back(q);
-    const Program prog = build_program(t, lower_ops(ops, num_ops, num_qubits), opt);
+    const Program prog = build_program(t, lower_ops(ops, num_ops, num_qubits), opt, FusionSearch::Thorough);
     const size_t rows = prog.passes.size();
     if (num_passes) *num_passes = rows;
     if (out) std::memcpy(out, prog.features.data(), std::min(rows, capacity) * kPassFeatures * sizeof(float));

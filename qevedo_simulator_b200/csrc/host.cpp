@@ -114,16 +114,17 @@ namespace {
 // (src/fusion.rs:126-170), on qubit bit masks: an op joins when it touches
 // no blocked qubit and fits; otherwise its qubits become blocked. `pre`:
 // qubits of unfused ops before the seed (they block from the start). The
-// sweep may stop early once the group has max_qubits qubits, all blocked:
-// a later op could then join only if it touched no qubit at all, and
+// sweep may stop early once every qubit of the group is blocked and either
+// the group has max_qubits qubits or every other qubit is blocked too: a
+// later op could then join only if it touched no qubit at all, and
 // `can_stop` says that no op is like that.
-void grow(const FusionInput& in, const std::vector<uint8_t>& done, std::vector<uint8_t>& taken, size_t seed,
-          uint64_t pre, std::vector<size_t>& members, uint64_t& qubits, size_t max_qubits, bool connected_only,
-          bool can_stop) {
+template <class Done>
+void grow(const FusionInput& in, const Done& done, std::vector<uint8_t>& taken, size_t seed, uint64_t pre,
+          std::vector<size_t>& members, uint64_t& qubits, size_t max_qubits, bool connected_only, bool can_stop) {
   uint64_t blocked = pre;
   const size_t n = in.mask.size();
   for (size_t i = seed + 1; i < n; ++i) {
-    if (done[i] || taken[i]) continue;
+    if (done(i) || taken[i]) continue;
     if (connected_only && (qubits & ~blocked) == 0) break;
     const uint64_t m = in.mask[i], fresh = m & ~qubits;
     const bool connected = fresh != m;
@@ -134,7 +135,9 @@ void grow(const FusionInput& in, const std::vector<uint8_t>& done, std::vector<u
       qubits |= m;
     } else {
       blocked |= m;
-      if (can_stop && (qubits & ~blocked) == 0 && size_t(__builtin_popcountll(qubits)) >= max_qubits) break;
+      if (can_stop && (qubits & ~blocked) == 0 &&
+          (size_t(__builtin_popcountll(qubits)) >= max_qubits || (in.all & ~blocked & ~qubits) == 0))
+        break;
     }
   }
 }
@@ -155,6 +158,7 @@ FusionInput fusion_input(const std::vector<HOp>& ops, const std::function<bool(c
     for (auto& c : ops[i].controls) add(c.first);
     in.width[i] = fusable(ops[i]) ? ops[i].width() : SIZE_MAX;
     in.any_empty = in.any_empty || in.mask[i] == 0;
+    in.all |= in.mask[i];
   }
   return in;
 }
@@ -163,6 +167,7 @@ std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_
   const size_t n = in.mask.size();
   const std::vector<uint64_t>& mask = in.mask;
   std::vector<uint8_t> done(n, 0), taken(n, 0);
+  const auto is_done = [&](size_t i) { return done[i] != 0; };
   std::vector<FusedGroup> groups;
   size_t first = 0;
   std::vector<size_t> members, best_members;
@@ -183,8 +188,8 @@ std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_
         uint64_t qubits = mask[s];
         taken[s] = true;
         if (in.width[s] <= max_qubits) {
-          grow(in, done, taken, s, pending, members, qubits, max_qubits, true, false);
-          grow(in, done, taken, s, pending, members, qubits, max_qubits, false, !in.any_empty);
+          grow(in, is_done, taken, s, pending, members, qubits, max_qubits, true, false);
+          grow(in, is_done, taken, s, pending, members, qubits, max_qubits, false, !in.any_empty);
         }
         for (size_t i : members) taken[i] = false;
         if (members.size() > best_members.size()) {
@@ -203,6 +208,98 @@ std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_
     groups.push_back(std::move(g));
   }
   return groups;
+}
+
+namespace {
+
+// A partial fusion of the beam search: the ops it covers (one bit each) and
+// its newest group (earlier ones through the arena's parent links).
+struct BeamNode {
+  std::vector<uint64_t> done;
+  size_t first = 0;    // no uncovered op before this one
+  size_t covered = 0;  // ops covered
+  int64_t last = -1;   // newest group in the arena
+};
+
+struct BeamGroup {
+  int64_t parent;
+  uint32_t offset, count;  // members (ascending) in the member pool
+  uint64_t qubits;
+};
+
+}  // namespace
+
+std::vector<std::vector<FusedGroup>> fuse_groups_beam(const FusionInput& in, size_t max_qubits, size_t lookahead,
+                                                      size_t width) {
+  const size_t n = in.mask.size();
+  std::vector<BeamGroup> arena;
+  std::vector<uint32_t> pool;
+  std::vector<BeamNode> beam(1), next;
+  beam[0].done.assign((n + 63) / 64, 0);
+  std::vector<uint8_t> taken(n, 0);
+  std::vector<size_t> members;
+  while (true) {
+    std::vector<std::vector<FusedGroup>> finished;
+    for (const BeamNode& b : beam) {
+      if (b.covered < n) continue;
+      std::vector<FusedGroup> gs;
+      for (int64_t g = b.last; g >= 0; g = arena[size_t(g)].parent) {
+        FusedGroup f;
+        const BeamGroup& bg = arena[size_t(g)];
+        f.members.assign(pool.begin() + bg.offset, pool.begin() + bg.offset + bg.count);
+        for (uint32_t q = 0; q < 64; ++q)
+          if ((arena[size_t(g)].qubits >> q) & 1) f.qubits.push_back(q);
+        gs.push_back(std::move(f));
+      }
+      std::reverse(gs.begin(), gs.end());
+      finished.push_back(std::move(gs));
+    }
+    if (!finished.empty() || beam.empty()) return finished;
+    next.clear();
+    for (const BeamNode& b : beam) {
+      const auto is_done = [&](size_t i) { return ((b.done[i >> 6] >> (i & 63)) & 1) != 0; };
+      size_t first = b.first;
+      while (first < n && is_done(first)) ++first;
+      uint64_t pending = 0;
+      size_t tried = 0;
+      for (size_t s = first; s < n && tried <= lookahead; ++s) {
+        if (is_done(s)) continue;
+        if (!(in.mask[s] & pending)) {
+          ++tried;
+          members.assign(1, s);
+          uint64_t qubits = in.mask[s];
+          taken[s] = 1;
+          if (in.width[s] <= max_qubits) {
+            grow(in, is_done, taken, s, pending, members, qubits, max_qubits, true, false);
+            grow(in, is_done, taken, s, pending, members, qubits, max_qubits, false, !in.any_empty);
+          }
+          for (size_t i : members) taken[i] = 0;
+          BeamNode c;
+          c.done = b.done;
+          for (size_t i : members) c.done[i >> 6] |= uint64_t(1) << (i & 63);
+          c.first = first;
+          c.covered = b.covered + members.size();
+          std::sort(members.begin(), members.end());
+          arena.push_back({b.last, uint32_t(pool.size()), uint32_t(members.size()), qubits});
+          pool.insert(pool.end(), members.begin(), members.end());
+          c.last = int64_t(arena.size()) - 1;
+          next.push_back(std::move(c));
+        }
+        pending |= in.mask[s];
+      }
+    }
+    // The `width` partial fusions that cover the most ops (earlier ones
+    // first among equals), without repeats of the same covered set.
+    std::stable_sort(next.begin(), next.end(),
+                     [](const BeamNode& x, const BeamNode& y) { return x.covered > y.covered; });
+    beam.clear();
+    for (BeamNode& c : next) {
+      if (beam.size() == width) break;
+      bool repeat = false;
+      for (const BeamNode& k : beam) repeat = repeat || (k.covered == c.covered && k.done == c.done);
+      if (!repeat) beam.push_back(std::move(c));
+    }
+  }
 }
 
 std::vector<FusedGroup> fuse_groups_lookahead(const std::vector<HOp>& ops, size_t max_qubits,

@@ -76,9 +76,18 @@ struct FusionInput {
   std::vector<uint64_t> mask;
   std::vector<size_t> width;
   bool any_empty = false;  // some op touches no qubit
+  uint64_t all = 0;        // every qubit some op touches
 };
 FusionInput fusion_input(const std::vector<HOp>& ops, const std::function<bool(const HOp&)>& fusable);
 std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_qubits, size_t lookahead);
+
+// Beam search over the same growth: each step, every kept partial fusion
+// forms its next group from each of its first lookahead + 1 ready seeds,
+// and the `width` partial fusions that cover the most ops are kept (equal
+// covered sets once). Returns the fusions that finish first, i.e. with the
+// fewest groups the search found.
+std::vector<std::vector<FusedGroup>> fuse_groups_beam(const FusionInput& in, size_t max_qubits, size_t lookahead,
+                                                      size_t width);
 
 // The group's ops as one op (the product matrix on its qubits; a group of one
 // op is that op, controls kept).

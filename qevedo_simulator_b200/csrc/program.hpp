@@ -38,7 +38,14 @@ struct Program {
 
 void pass_features(const Target& t, const PlannedPass& p, const LoweredPass& lp, const StageUpload& up, float* f);
 
-Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt);
+// How hard a tensor-core plain plan searches for fewer passes: the seed
+// lookahead fusions only, plus one beam search, or plus several wider ones.
+// A plan built once and run many times affords the widest search; a
+// one-shot run only where its passes are long enough to pay for it.
+enum class FusionSearch { Lookahead, Beam, Thorough };
+
+Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt,
+                      FusionSearch search);
 
 // Copy the program's gate data to `dst` on `stream` through the state's
 // pinned staging buffer.

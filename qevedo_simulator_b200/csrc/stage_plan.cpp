@@ -171,7 +171,8 @@ Target target_of(const StateImpl& s) {
   return t;
 }
 
-Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt) {
+Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt,
+                      FusionSearch search) {
   Program prog;
   prog.target = t;
   prog.gates = ops.size();
@@ -204,16 +205,37 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       // on a |0...0> state and one swap pass otherwise): the pair with the
       // lowest estimated cost, a pass with k targets on bits 1-3 counting as
       // 1, 1.2, 1.45 or 2.1 clean passes.
-      std::vector<std::vector<FusedGroup>> cand(9);
+      // Fusions: the lookahead ones and the beam searches' (the widest
+      // first, each on its own thread). At 30 qubits (depth-20 grid
+      // circuit, fusion 6) one beam takes 50 passes to 47, the wider ones
+      // to 46; at 32 qubits 52 to 51 and 47.
+      struct BeamConfig {
+        size_t lookahead, width;
+      };
+      std::vector<BeamConfig> beams;
+      if (search == FusionSearch::Thorough) beams = {{16, 32}, {12, 32}, {8, 32}, {6, 32}};
+      if (search != FusionSearch::Lookahead) beams.push_back({8, 8});
+      const size_t nbeam = beams.size(), nlook = 9;
+      std::vector<std::vector<std::vector<FusedGroup>>> found(nbeam + nlook);
+      parallel_for(found.size(), [&](size_t j) {
+        if (j < nbeam) {
+          found[j] = fuse_groups_beam(fin, max_fused, beams[j].lookahead, beams[j].width);
+        } else {
+          const size_t i = nlook - 1 - (j - nbeam);  // the longest lookaheads first
+          found[j].push_back(i == 0 ? groups : fuse_groups_lookahead(fin, max_fused, i));
+        }
+      });
+      // Candidates in a fixed order: lookahead 0-8, then the beams' results.
+      std::vector<std::vector<FusedGroup>> cand;
+      for (size_t i = 0; i < nlook; ++i) cand.push_back(std::move(found[nbeam + nlook - 1 - i][0]));
+      for (size_t j = 0; j < nbeam; ++j)
+        for (auto& f : found[j]) cand.push_back(std::move(f));
       std::vector<double> cost(cand.size());
       std::vector<uint64_t> low_set(cand.size());
       std::vector<uint32_t> at(t.n);  // physical -> logical
       for (uint32_t q = 0; q < t.n; ++q) at[t.layout[q]] = q;
       const uint64_t now = (uint64_t(1) << at[1]) | (uint64_t(1) << at[2]) | (uint64_t(1) << at[3]);
-      // The longest lookaheads first: they take the longest.
-      parallel_for(cand.size(), [&](size_t j) {
-        const size_t i = cand.size() - 1 - j;
-        cand[i] = i == 0 ? groups : fuse_groups_lookahead(fin, max_fused, i);
+      parallel_for(cand.size(), [&](size_t i) {
         std::vector<uint64_t> gm;
         for (const FusedGroup& g : cand[i]) {
           uint64_t m = 0;
@@ -252,7 +274,7 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
             }
         cost[i] = best;
         low_set[i] = best_set;
-      });
+      }, cand.size() >= 8 ? 0u : 1u);
       size_t pick = 0;
       for (size_t i = 1; i < cand.size(); ++i)
         if (cost[i] < cost[pick] - 1e-9) pick = i;

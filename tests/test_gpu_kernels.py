@@ -309,6 +309,21 @@ def test_tensor_core_plain_passes_at_24_qubits(kind):
                 assert ref.max_abs_diff(st) < 1e-6, (kind, fuse)
 
 
+def test_one_shot_tensor_core_run_with_beam_search_at_30_qubits():
+    """A one-shot run of fused 6-qubit tensor-core passes on a state of 29 or
+    more qubits searches its fusion with a beam (below that only the seed
+    lookahead pays for its planning time): the 30-qubit grid circuit matches
+    the plain CUDA-core fusion-4 run to 1e-6."""
+    from qevedo_simulator_b200 import library
+
+    ops = library.random_grid_circuit(5, 6, 8, seed=77).ops()
+    with DeviceState(30, 32) as ref, DeviceState(30, 32) as st:
+        ref.apply_ops(ops, options(4, staged=False))
+        stats = st.apply_ops(ops, options(6, staged=False, math="tensor"))
+        assert stats["passes"] < 0.6 * len(ops)
+        assert ref.max_abs_diff(st) < 1e-6
+
+
 def test_tensor_core_plain_plans_relabel_low_bits():
     """Tensor-core plain plans may first move three qubits onto index bits
     1-3 (the bits whose targets slow the passes down): free on a |0...0>
