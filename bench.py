@@ -62,7 +62,8 @@ def workload_config(n: int, depth: int) -> dict:
         "grid": f"{ROWS}x{COLS}" if n == ROWS * COLS else "custom",
         "gates": "sqrt(X)/sqrt(Y)/sqrt(W) with no repeat + CZ on 4 coupler sets",
         "state_bytes": (1 << n) * 8,
-        "l2": "inputs larger than L2 (8 GiB state vs 126 MB)",
+        "l2": (f"inputs larger than L2 ({(1 << n) * 8 / 2**30:g} GiB state vs 126 MB)" if (1 << n) * 8 > 126e6
+               else f"state ({(1 << n) * 8 / 2**20:g} MiB) fits in L2 (126 MB)"),
         "parallelism": "replicas (one circuit per GPU)",
     }
 

@@ -181,17 +181,32 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+__device__ __forceinline__ void cp_async16_s(uint32_t smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem), "l"(gmem) : "memory");
+}
+
+// prob<T> in fewer instructions: for a complex64 amplitude re*re and im*im
+// are exact in f64 (24-bit significands), so re*re + im*im rounded once, as
+// one fused multiply-add, equals the sum of the two rounded products.
+template <typename T>
+__device__ __forceinline__ double prob_fast(const cplx_t<T>& a) {
+  if constexpr (sizeof(T) == 4) {
+    const double re = double(a.x), im = double(a.y);
+    return __fma_rn(re, re, __dmul_rn(im, im));
+  } else {
+    return prob<T>(a);
+  }
+}
+
 // p of the amplitudes of one 16-byte read, in index order.
 template <typename T>
-__device__ __forceinline__ double fold16(double s, const float4& v);
-template <>
-__device__ __forceinline__ double fold16<float>(double s, const float4& v) {
-  s = __dadd_rn(s, prob<float>(make_float2(v.x, v.y)));
-  return __dadd_rn(s, prob<float>(make_float2(v.z, v.w)));
-}
-template <>
-__device__ __forceinline__ double fold16<double>(double s, const float4& v) {
-  return __dadd_rn(s, prob<double>(*reinterpret_cast<const double2*>(&v)));
+__device__ __forceinline__ void probs16(const float4& v, double* p) {
+  if constexpr (sizeof(T) == 4) {
+    p[0] = prob_fast<float>(make_float2(v.x, v.y));
+    p[1] = prob_fast<float>(make_float2(v.z, v.w));
+  } else {
+    p[0] = prob<double>(*reinterpret_cast<const double2*>(&v));
+  }
 }
 
 template <typename T>
@@ -209,8 +224,25 @@ __global__ void __launch_bounds__(32) k_chunk_sums(const cplx_t<T>* __restrict__
   // Windows of the warp's first chunk (no later chunk is longer).
   const uint64_t windows = (umin64(chunk_len, len - chunk0 * chunk_len) + kPerWin - 1) / kPerWin;
   const unsigned char* src0 = reinterpret_cast<const unsigned char*>(psi);
+  const int half = lane >> 4, sub = lane & 15;
+  // Every chunk of the warp whole (all but a state shorter than one chunk):
+  // a lane's copies are then one pointer and one shared address apart.
+  const bool whole = (chunk0 + uint64_t(live)) * chunk_len <= len;
+  const unsigned char* lane_src = src0 + (chunk0 + uint64_t(half)) * chunk_len * kAmp + sub * 16;
+  const uint64_t lane_step = 2 * chunk_len * kAmp;
+  const uint32_t lane_dst = static_cast<uint32_t>(__cvta_generic_to_shared(&sbuf[0][half * kSumRow + sub * 16]));
   auto issue = [&](uint64_t w, int stage) {
-    const int half = lane >> 4, sub = lane & 15;
+    if (whole) {
+      const unsigned char* src = lane_src + w * kSumWindow;
+      uint32_t dst = lane_dst + uint32_t(stage) * kSumStageBytes;
+      if (live == 32) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) cp_async16_s(dst + uint32_t(r) * 2 * kSumRow, src + r * lane_step);
+      } else {
+        for (int r = 0; 2 * r + half < live; ++r) cp_async16_s(dst + uint32_t(r) * 2 * kSumRow, src + r * lane_step);
+      }
+      return;
+    }
     for (int r = 0; r < 16; ++r) {
       const int c = 2 * r + half;
       if (c >= live) break;
@@ -242,11 +274,15 @@ __global__ void __launch_bounds__(32) k_chunk_sums(const cplx_t<T>* __restrict__
       const float4* row = reinterpret_cast<const float4*>(&sbuf[w % kSumStages][lane * kSumRow]);
       const uint64_t n = umin64(kPerWin, my_end - pos);
       if (n == uint64_t(kPerWin)) {
+        // The probabilities first (independent of the sum), then the chain.
+        double p[kPerWin];
 #pragma unroll
-        for (int j = 0; j < kPerWin / kPerRead; ++j) s = fold16<T>(s, row[j]);
+        for (int j = 0; j < kPerWin / kPerRead; ++j) probs16<T>(row[j], p + j * kPerRead);
+#pragma unroll
+        for (int j = 0; j < kPerWin; ++j) s = __dadd_rn(s, p[j]);
       } else {
         const cplx_t<T>* amps = reinterpret_cast<const cplx_t<T>*>(row);
-        for (uint64_t j = 0; j < n; ++j) s = __dadd_rn(s, prob<T>(amps[j]));
+        for (uint64_t j = 0; j < n; ++j) s = __dadd_rn(s, prob_fast<T>(amps[j]));
       }
     }
     __syncwarp();
@@ -324,14 +360,21 @@ __global__ void k_active(const uint64_t* __restrict__ bounds, uint64_t nchunks, 
 }
 
 // Pass 2: one warp per chunk that holds shots (src/measure.rs:134-167). The
-// warp computes the chunk's probabilities a window at a time (coalesced, the
-// next window while the current one is folded) into shared memory, and lane
-// 0 folds them in index order exactly as the reference does: one
-// sequential f64 sum from prefix[chunk], emitting an index while the next
-// target is below the running sum.
+// warp streams the chunk's amplitudes through shared memory with cp.async
+// (windows of 2 KB, two ahead of the fold). For each window the lanes
+// compute the probabilities, eight each, with each block of eight's last
+// nonzero position; lane 0 then folds them in index order exactly as the
+// reference does: one sequential f64 sum from prefix[chunk], emitting an
+// index while the next target is below the running sum. Lane 0 adds eight
+// probabilities at a time and checks the target once against the eighth
+// sum: the running sum never decreases (p >= +0, and adding +0 changes
+// nothing), so a target at or above it emits nothing in those eight, and
+// only a block that emits is redone one probability at a time (the same
+// additions, so the same sums). Lane 0's work per amplitude is then one
+// addition of the chain.
 constexpr int kWalkWarps = 4;
-constexpr int kWalkPerLane = 8;
-constexpr int kWalkWindow = 32 * kWalkPerLane;
+constexpr int kWalkStages = 3;
+constexpr int kWalkBytes = 2048;  // per window
 
 template <typename T>
 __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(const cplx_t<T>* __restrict__ psi, uint64_t len,
@@ -341,7 +384,12 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(const cplx_t<T>* __res
                                                           const uint64_t* __restrict__ bounds, size_t shots,
                                                           const double* __restrict__ targets,
                                                           uint64_t* __restrict__ out) {
-  __shared__ double sp[kWalkWarps][2][kWalkWindow];
+  constexpr int kAmp = int(sizeof(cplx_t<T>));
+  constexpr int kPerWin = kWalkBytes / kAmp;  // 256 or 128 amplitudes
+  constexpr int kBlocks = kPerWin / 8;        // blocks of eight per window
+  __shared__ __align__(16) unsigned char raw[kWalkWarps][kWalkStages][kWalkBytes];
+  __shared__ __align__(16) double pw[kWalkWarps][kPerWin];
+  __shared__ int8_t last_in[kWalkWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t a = blockIdx.x * kWalkWarps + warp;
   if (a >= *num_active) return;
@@ -350,27 +398,78 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(const cplx_t<T>* __res
   const uint64_t end = umin64(chunk_len, len - base);
   const uint64_t hi = umin64(bounds[chunk + 1], shots);
   uint64_t shot = bounds[chunk];
+  if (shot >= hi) return;  // the whole warp: no shot lands here
   uint64_t last_nonzero = base;
   double cumulative = prefix[chunk];
-  auto fill = [&](uint64_t pos, int buf) {
+  const uint64_t windows = (end + kPerWin - 1) / kPerWin;
+  const uint64_t end_b = end * kAmp;
+  const unsigned char* src0 = reinterpret_cast<const unsigned char*>(psi + base);
+  auto issue = [&](uint64_t w, int stage) {
 #pragma unroll
-    for (int e = 0; e < kWalkPerLane; ++e) {
-      const uint64_t off = pos + uint64_t(lane + 32 * e);
-      sp[warp][buf][lane + 32 * e] = off < end ? prob<T>(psi[base + off]) : 0.0;
+    for (int i = 0; i < kWalkBytes / 512; ++i) {
+      const uint64_t off_b = w * kWalkBytes + uint64_t(i * 32 + lane) * 16;
+      unsigned char* dst = &raw[warp][stage][(i * 32 + lane) * 16];
+      if (off_b + 16 <= end_b)
+        cp_async16(dst, src0 + off_b);
+      else if (off_b < end_b)  // one complex64 left (a state of one amplitude)
+        *reinterpret_cast<cplx_t<T>*>(dst) = *reinterpret_cast<const cplx_t<T>*>(src0 + off_b);
     }
   };
-  bool walking = shot < hi;
-  if (walking) fill(0, 0);
-  __syncwarp();
-  int buf = 0;
-  for (uint64_t pos = 0; walking && pos < end; pos += kWalkWindow) {
-    if (pos + kWalkWindow < end) fill(pos + kWalkWindow, buf ^ 1);
+  for (int st = 0; st < kWalkStages - 1; ++st) {
+    if (uint64_t(st) < windows) issue(uint64_t(st), st);
+    cp_async_commit();
+  }
+  for (uint64_t w = 0; w < windows; ++w) {
+    const uint64_t ahead = w + kWalkStages - 1;
+    if (ahead < windows) issue(ahead, int(ahead % kWalkStages));
+    cp_async_commit();
+    cp_async_wait<kWalkStages - 1>();  // window w has landed
+    __syncwarp();
+    const uint64_t pos = w * kPerWin;
+    const int n = int(umin64(kPerWin, end - pos));
+    // Lane b: the probabilities of block b (0 past the window's end) and the
+    // position of its last nonzero one (-1: none).
+    if (lane < kBlocks) {
+      const cplx_t<T>* amps = reinterpret_cast<const cplx_t<T>*>(&raw[warp][w % kWalkStages][0]);
+      const int j0 = lane * 8;
+      double p[8];
+      if (j0 + 8 <= n) {
+        const float4* v = reinterpret_cast<const float4*>(amps + j0);
+#pragma unroll
+        for (int r = 0; r < 8 * kAmp / 16; ++r) probs16<T>(v[r], p + r * (16 / kAmp));
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) p[j] = j0 + j < n ? prob_fast<T>(amps[j0 + j]) : 0.0;
+      }
+      int last = -1;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        pw[warp][j0 + j] = p[j];
+        last = p[j] != 0.0 ? j : last;
+      }
+      last_in[warp][lane] = int8_t(last);
+    }
+    __syncwarp();
     if (lane == 0) {
       double next = targets[shot];  // shot < hi here
-      for (int j0 = 0; j0 < kWalkWindow && shot < hi; j0 += 8) {
+      for (int j0 = 0; j0 < n && shot < hi; j0 += 8) {
         double p[8];
+        const double2* v = reinterpret_cast<const double2*>(&pw[warp][j0]);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) p[j] = sp[warp][buf][j0 + j];
+        for (int r = 0; r < 4; ++r) {
+          const double2 x = v[r];
+          p[2 * r] = x.x;
+          p[2 * r + 1] = x.y;
+        }
+        double c8 = cumulative;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) c8 = __dadd_rn(c8, p[j]);
+        if (!(next < c8)) {  // no emission among these eight
+          cumulative = c8;
+          const int last = last_in[warp][j0 >> 3];
+          if (last >= 0) last_nonzero = base + pos + uint64_t(j0 + last);
+          continue;
+        }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           if (p[j] == 0.0 || shot == hi) continue;
@@ -385,10 +484,11 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(const cplx_t<T>* __res
         }
       }
     }
-    walking = __shfl_sync(0xffffffffu, shot < hi ? 1 : 0, 0) != 0;
+    const bool walking = __shfl_sync(0xffffffffu, shot < hi ? 1 : 0, 0) != 0;
     __syncwarp();
-    buf ^= 1;
+    if (!walking) break;
   }
+  cp_async_wait<0>();  // no copy outlives the kernel's shared memory
   if (lane == 0)
     for (; shot < hi; ++shot) out[shot] = umin64(last_nonzero, len - 1);
 }
