@@ -165,7 +165,7 @@ std::vector<HOp> lower_ops(const qvdg_op* ops, size_t n, uint32_t num_qubits) {
 // Plan, upload and run `ops` on the state (the reference's apply_ops,
 // src/simulator.rs:122-147).
 void apply_program(StateImpl& s, const std::vector<HOp>& ops, const qvdg_options& opt, qvdg_stats* stats) {
-  // One-shot: a beam search where a pass streams at least 8 GB.
+  // One-shot: narrow beam searches where a pass streams at least 8 GB.
   const Program prog =
       build_program(target_of(s), ops, opt, s.n >= 29 ? FusionSearch::Beam : FusionSearch::Lookahead);
   const DeviceUpload dev = upload_program(s, prog, s.work);

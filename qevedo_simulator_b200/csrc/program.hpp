@@ -39,7 +39,7 @@ struct Program {
 void pass_features(const Target& t, const PlannedPass& p, const LoweredPass& lp, const StageUpload& up, float* f);
 
 // How hard a tensor-core plain plan searches for fewer passes: the seed
-// lookahead fusions only, plus one beam search, or plus several wider ones.
+// lookahead fusions only, plus narrow beam searches, or plus wider ones too.
 // A plan built once and run many times affords the widest search; a
 // one-shot run only where its passes are long enough to pay for it.
 enum class FusionSearch { Lookahead, Beam, Thorough };

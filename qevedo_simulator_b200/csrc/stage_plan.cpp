@@ -207,14 +207,18 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       // 1, 1.2, 1.45 or 2.1 clean passes.
       // Fusions: the lookahead ones and the beam searches' (the widest
       // first, each on its own thread). At 30 qubits (depth-20 grid
-      // circuit, fusion 6) one beam takes 50 passes to 47, the wider ones
-      // to 46; at 32 qubits 52 to 51 and 47.
+      // circuit, fusion 6) the narrow beams take 50 passes to 47, the wide
+      // ones to 45; at 32 qubits 52 to 50 and 47.
       struct BeamConfig {
         size_t lookahead, width;
       };
       std::vector<BeamConfig> beams;
-      if (search == FusionSearch::Thorough) beams = {{16, 32}, {12, 32}, {8, 32}, {6, 32}};
-      if (search != FusionSearch::Lookahead) beams.push_back({8, 8});
+      if (search == FusionSearch::Thorough) {
+        beams = {{24, 32}, {16, 32}, {12, 32}, {8, 32}, {6, 32}};
+        if (ops.size() <= 2000) beams.insert(beams.begin(), {24, 64});  // its time grows with the groups
+      }
+      if (search != FusionSearch::Lookahead)
+        for (size_t l : {16, 6}) beams.push_back({l, 8});
       const size_t nbeam = beams.size(), nlook = 9;
       std::vector<std::vector<std::vector<FusedGroup>>> found(nbeam + nlook);
       parallel_for(found.size(), [&](size_t j) {
