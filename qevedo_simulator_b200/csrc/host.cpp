@@ -118,28 +118,45 @@ namespace {
 // the group has max_qubits qubits or every other qubit is blocked too: a
 // later op could then join only if it touched no qubit at all, and
 // `can_stop` says that no op is like that.
+//
+// With in.commute, a diagonal op is blocked only by skipped non-diagonal
+// ops (`blocked`): diagonal ops commute, so it may move ahead of skipped
+// diagonal ones (`blocked_diag`, which still block non-diagonal ops). The
+// stop rule then looks at `blocked` alone.
 template <class Done>
 void grow(const FusionInput& in, const Done& done, std::vector<uint8_t>& taken, size_t seed, uint64_t pre,
-          std::vector<size_t>& members, uint64_t& qubits, size_t max_qubits, bool connected_only, bool can_stop) {
-  uint64_t blocked = pre;
+          uint64_t pre_diag, std::vector<size_t>& members, uint64_t& qubits, size_t max_qubits,
+          bool connected_only, bool can_stop) {
+  uint64_t blocked = pre, blocked_diag = pre_diag;
   const size_t n = in.mask.size();
   for (size_t i = seed + 1; i < n; ++i) {
     if (done(i) || taken[i]) continue;
     if (connected_only && (qubits & ~blocked) == 0) break;
+    const bool diag = in.commute && in.diag[i];
     const uint64_t m = in.mask[i], fresh = m & ~qubits;
     const bool connected = fresh != m;
     const bool fits = in.width[i] <= max_qubits && size_t(__builtin_popcountll(qubits | m)) <= max_qubits;
-    if (!(m & blocked) && fits && (connected || !connected_only)) {
+    if (!(m & (diag ? blocked : blocked | blocked_diag)) && fits && (connected || !connected_only)) {
       taken[i] = true;
       members.push_back(i);
       qubits |= m;
     } else {
-      blocked |= m;
+      (diag ? blocked_diag : blocked) |= m;
       if (can_stop && (qubits & ~blocked) == 0 &&
           (size_t(__builtin_popcountll(qubits)) >= max_qubits || (in.all & ~blocked & ~qubits) == 0))
         break;
     }
   }
+}
+
+// Whether a seed at `mask` may start a group ahead of the unfused ops
+// before it (`pending`, and `pending_diag` for diagonal ones in commute
+// mode), and those ops' qubits updated with op s.
+inline bool ready(const FusionInput& in, size_t s, uint64_t pending, uint64_t pending_diag) {
+  return !(in.mask[s] & (in.commute && in.diag[s] ? pending : pending | pending_diag));
+}
+inline void hold(const FusionInput& in, size_t s, uint64_t& pending, uint64_t& pending_diag) {
+  (in.commute && in.diag[s] ? pending_diag : pending) |= in.mask[s];
 }
 
 }  // namespace
@@ -157,10 +174,24 @@ FusionInput fusion_input(const std::vector<HOp>& ops, const std::function<bool(c
     for (uint32_t q : ops[i].targets) add(q);
     for (auto& c : ops[i].controls) add(c.first);
     in.width[i] = fusable(ops[i]) ? ops[i].width() : SIZE_MAX;
+    in.diag.push_back(ops[i].diagonal ? 1 : 0);
     in.any_empty = in.any_empty || in.mask[i] == 0;
     in.all |= in.mask[i];
   }
   return in;
+}
+
+bool diagonal_runs(const FusionInput& in) {
+  uint64_t last_diag = 0;  // qubits whose latest op is diagonal
+  for (size_t i = 0; i < in.mask.size(); ++i) {
+    if (in.diag[i]) {
+      if (in.mask[i] & last_diag) return true;
+      last_diag |= in.mask[i];
+    } else {
+      last_diag &= ~in.mask[i];
+    }
+  }
+  return false;
 }
 
 std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_qubits, size_t lookahead) {
@@ -177,19 +208,19 @@ std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_
     // Seeds: the first unfused op, then up to `lookahead` later ones that
     // no unfused earlier op holds back; keep the seed whose group takes the
     // most ops (ties: the earliest).
-    uint64_t pending = 0, best_qubits = 0;
+    uint64_t pending = 0, pending_diag = 0, best_qubits = 0;
     size_t tried = 0;
     best_members.clear();
     for (size_t s = first; s < n && tried <= lookahead; ++s) {
       if (done[s]) continue;
-      if (!(mask[s] & pending)) {
+      if (ready(in, s, pending, pending_diag)) {
         ++tried;
         members.assign(1, s);
         uint64_t qubits = mask[s];
         taken[s] = true;
         if (in.width[s] <= max_qubits) {
-          grow(in, is_done, taken, s, pending, members, qubits, max_qubits, true, false);
-          grow(in, is_done, taken, s, pending, members, qubits, max_qubits, false, !in.any_empty);
+          grow(in, is_done, taken, s, pending, pending_diag, members, qubits, max_qubits, true, false);
+          grow(in, is_done, taken, s, pending, pending_diag, members, qubits, max_qubits, false, !in.any_empty);
         }
         for (size_t i : members) taken[i] = false;
         if (members.size() > best_members.size()) {
@@ -197,7 +228,7 @@ std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_
           best_qubits = qubits;
         }
       }
-      pending |= mask[s];
+      hold(in, s, pending, pending_diag);
     }
     FusedGroup g;
     g.members = best_members;
@@ -260,18 +291,18 @@ std::vector<std::vector<FusedGroup>> fuse_groups_beam(const FusionInput& in, siz
       const auto is_done = [&](size_t i) { return ((b.done[i >> 6] >> (i & 63)) & 1) != 0; };
       size_t first = b.first;
       while (first < n && is_done(first)) ++first;
-      uint64_t pending = 0;
+      uint64_t pending = 0, pending_diag = 0;
       size_t tried = 0;
       for (size_t s = first; s < n && tried <= lookahead; ++s) {
         if (is_done(s)) continue;
-        if (!(in.mask[s] & pending)) {
+        if (ready(in, s, pending, pending_diag)) {
           ++tried;
           members.assign(1, s);
           uint64_t qubits = in.mask[s];
           taken[s] = 1;
           if (in.width[s] <= max_qubits) {
-            grow(in, is_done, taken, s, pending, members, qubits, max_qubits, true, false);
-            grow(in, is_done, taken, s, pending, members, qubits, max_qubits, false, !in.any_empty);
+            grow(in, is_done, taken, s, pending, pending_diag, members, qubits, max_qubits, true, false);
+            grow(in, is_done, taken, s, pending, pending_diag, members, qubits, max_qubits, false, !in.any_empty);
           }
           for (size_t i : members) taken[i] = 0;
           BeamNode c;
@@ -285,7 +316,7 @@ std::vector<std::vector<FusedGroup>> fuse_groups_beam(const FusionInput& in, siz
           c.last = int64_t(arena.size()) - 1;
           next.push_back(std::move(c));
         }
-        pending |= in.mask[s];
+        hold(in, s, pending, pending_diag);
       }
     }
     // The `width` partial fusions that cover the most ops (earlier ones

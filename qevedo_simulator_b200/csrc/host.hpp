@@ -75,9 +75,17 @@ std::vector<FusedGroup> fuse_groups_lookahead(const std::vector<HOp>& ops, size_
 struct FusionInput {
   std::vector<uint64_t> mask;
   std::vector<size_t> width;
-  bool any_empty = false;  // some op touches no qubit
-  uint64_t all = 0;        // every qubit some op touches
+  std::vector<uint8_t> diag;  // the op is diagonal
+  bool any_empty = false;     // some op touches no qubit
+  uint64_t all = 0;           // every qubit some op touches
+  // Diagonal ops commute with each other: with `commute` a diagonal op may
+  // join a group ahead of skipped diagonal ops on its qubits (only skipped
+  // non-diagonal ones hold it back), and seed one.
+  bool commute = false;
 };
+// Whether some qubit meets two diagonal ops with no other op between them
+// (only then does commute change a fusion).
+bool diagonal_runs(const FusionInput& in);
 FusionInput fusion_input(const std::vector<HOp>& ops, const std::function<bool(const HOp&)>& fusable);
 std::vector<FusedGroup> fuse_groups_lookahead(const FusionInput& in, size_t max_qubits, size_t lookahead);
 

@@ -219,21 +219,34 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       }
       if (search != FusionSearch::Lookahead)
         for (size_t l : {16, 6}) beams.push_back({l, 8});
-      const size_t nbeam = beams.size(), nlook = 9;
-      std::vector<std::vector<std::vector<FusedGroup>>> found(nbeam + nlook);
-      parallel_for(found.size(), [&](size_t j) {
+      // Each search in up to two families: the fusion as the reference
+      // orders ops, and, where some qubit meets two diagonal ops in a row
+      // (QFT's controlled phases), with diagonal ops free to commute
+      // (45 instead of 68 passes for the 30-qubit QFT at fusion 6).
+      FusionInput fin_c = fin;
+      fin_c.commute = true;
+      std::vector<const FusionInput*> families = {&fin};
+      if (diagonal_runs(fin)) families.push_back(&fin_c);
+      const size_t nbeam = beams.size(), nlook = 9, per = nbeam + nlook;
+      std::vector<std::vector<std::vector<FusedGroup>>> found(per * families.size());
+      parallel_for(found.size(), [&](size_t t) {
+        const size_t j = t % per;
+        const FusionInput& in = *families[t / per];
         if (j < nbeam) {
-          found[j] = fuse_groups_beam(fin, max_fused, beams[j].lookahead, beams[j].width);
+          found[t] = fuse_groups_beam(in, max_fused, beams[j].lookahead, beams[j].width);
         } else {
           const size_t i = nlook - 1 - (j - nbeam);  // the longest lookaheads first
-          found[j].push_back(i == 0 ? groups : fuse_groups_lookahead(fin, max_fused, i));
+          found[t].push_back(i == 0 && t < per ? groups : fuse_groups_lookahead(in, max_fused, i));
         }
       });
-      // Candidates in a fixed order: lookahead 0-8, then the beams' results.
+      // Candidates in a fixed order: per family, lookahead 0-8, then the
+      // beams' results.
       std::vector<std::vector<FusedGroup>> cand;
-      for (size_t i = 0; i < nlook; ++i) cand.push_back(std::move(found[nbeam + nlook - 1 - i][0]));
-      for (size_t j = 0; j < nbeam; ++j)
-        for (auto& f : found[j]) cand.push_back(std::move(f));
+      for (size_t f = 0; f < families.size(); ++f) {
+        for (size_t i = 0; i < nlook; ++i) cand.push_back(std::move(found[f * per + nbeam + nlook - 1 - i][0]));
+        for (size_t j = 0; j < nbeam; ++j)
+          for (auto& g : found[f * per + j]) cand.push_back(std::move(g));
+      }
       std::vector<double> cost(cand.size());
       std::vector<uint64_t> low_set(cand.size());
       std::vector<uint32_t> at(t.n);  // physical -> logical
