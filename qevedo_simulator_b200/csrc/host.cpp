@@ -1,8 +1,12 @@
 // Host gate algebra and greedy fusion (see host.hpp for the reference map).
 #include "host.hpp"
 
+#include <unistd.h>
+
+#include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <exception>
 #include <mutex>
 #include <stdexcept>
@@ -267,8 +271,6 @@ std::vector<std::vector<FusedGroup>> fuse_groups_beam(const FusionInput& in, siz
   std::vector<uint32_t> pool;
   std::vector<BeamNode> beam(1), next;
   beam[0].done.assign((n + 63) / 64, 0);
-  std::vector<uint8_t> taken(n, 0);
-  std::vector<size_t> members;
   while (true) {
     std::vector<std::vector<FusedGroup>> finished;
     for (const BeamNode& b : beam) {
@@ -286,8 +288,19 @@ std::vector<std::vector<FusedGroup>> fuse_groups_beam(const FusionInput& in, siz
       finished.push_back(std::move(gs));
     }
     if (!finished.empty() || beam.empty()) return finished;
-    next.clear();
-    for (const BeamNode& b : beam) {
+    // Every kept partial fusion's children, on the pool's threads; merged
+    // in the nodes' order, so the result does not depend on timing.
+    struct Child {
+      BeamNode node;
+      std::vector<size_t> members;  // ascending
+      uint64_t qubits;
+    };
+    std::vector<std::vector<Child>> kids(beam.size());
+    parallel_for(beam.size(), [&](size_t bi) {
+      const BeamNode& b = beam[bi];
+      thread_local std::vector<uint8_t> taken;  // all 0 between uses
+      if (taken.size() < n) taken.resize(n, 0);
+      std::vector<size_t> members;
       const auto is_done = [&](size_t i) { return ((b.done[i >> 6] >> (i & 63)) & 1) != 0; };
       size_t first = b.first;
       while (first < n && is_done(first)) ++first;
@@ -305,20 +318,28 @@ std::vector<std::vector<FusedGroup>> fuse_groups_beam(const FusionInput& in, siz
             grow(in, is_done, taken, s, pending, pending_diag, members, qubits, max_qubits, false, !in.any_empty);
           }
           for (size_t i : members) taken[i] = 0;
-          BeamNode c;
-          c.done = b.done;
-          for (size_t i : members) c.done[i >> 6] |= uint64_t(1) << (i & 63);
-          c.first = first;
-          c.covered = b.covered + members.size();
+          Child c;
+          c.node.done = b.done;
+          for (size_t i : members) c.node.done[i >> 6] |= uint64_t(1) << (i & 63);
+          c.node.first = first;
+          c.node.covered = b.covered + members.size();
+          c.node.last = b.last;  // the parent's newest group, until merged
           std::sort(members.begin(), members.end());
-          arena.push_back({b.last, uint32_t(pool.size()), uint32_t(members.size()), qubits});
-          pool.insert(pool.end(), members.begin(), members.end());
-          c.last = int64_t(arena.size()) - 1;
-          next.push_back(std::move(c));
+          c.members = members;
+          c.qubits = qubits;
+          kids[bi].push_back(std::move(c));
         }
         hold(in, s, pending, pending_diag);
       }
-    }
+    });
+    next.clear();
+    for (auto& ks : kids)
+      for (Child& c : ks) {
+        arena.push_back({c.node.last, uint32_t(pool.size()), uint32_t(c.members.size()), c.qubits});
+        pool.insert(pool.end(), c.members.begin(), c.members.end());
+        c.node.last = int64_t(arena.size()) - 1;
+        next.push_back(std::move(c.node));
+      }
     // The `width` partial fusions that cover the most ops (earlier ones
     // first among equals), without repeats of the same covered set.
     std::stable_sort(next.begin(), next.end(),
@@ -464,31 +485,121 @@ std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
   return fused;
 }
 
+namespace {
+
+// A fork-join pool of host threads. parallel_for posts a job and runs its
+// indices itself; idle workers take indices of any posted job. A caller
+// whose indices are all taken helps other jobs until its own finish, so a
+// task that itself calls parallel_for (the beam searches' steps inside the
+// planner's candidate tasks) cannot deadlock. Workers spin briefly before
+// sleeping, so the short jobs of consecutive search steps find them awake.
+struct PoolJob {
+  const std::function<void(size_t)>* f = nullptr;
+  size_t n = 0;
+  std::atomic<size_t> next{0};
+  std::atomic<size_t> done{0};
+  std::mutex error_mutex;
+  std::exception_ptr error;
+
+  // Runs index i of this job (taken by the caller).
+  void run(size_t i) {
+    try {
+      (*f)(i);
+    } catch (...) {
+      std::lock_guard<std::mutex> lock(error_mutex);
+      if (!error) error = std::current_exception();
+    }
+    done.fetch_add(1, std::memory_order_release);
+  }
+};
+
+class WorkerPool {
+ public:
+  explicit WorkerPool(unsigned workers) {
+    for (unsigned t = 0; t < workers; ++t) std::thread([this] { work(); }).detach();
+  }
+
+  void run(PoolJob& job) {
+    {
+      std::lock_guard<std::mutex> lock(m_);
+      jobs_.push_back(&job);
+      maybe_work_.store(true, std::memory_order_release);
+    }
+    cv_.notify_all();
+    for (size_t i; (i = job.next.fetch_add(1)) < job.n;) job.run(i);
+    while (job.done.load(std::memory_order_acquire) < job.n)
+      if (!(maybe_work_.load(std::memory_order_acquire) && help())) std::this_thread::yield();
+    std::lock_guard<std::mutex> lock(m_);
+    jobs_.erase(std::find(jobs_.begin(), jobs_.end(), &job));
+  }
+
+ private:
+  // Runs one index of any posted job; false when none is left (and then
+  // marks the pool as without work until the next post).
+  bool help() {
+    PoolJob* job = nullptr;
+    size_t i = 0;
+    {
+      std::lock_guard<std::mutex> lock(m_);
+      for (PoolJob* j : jobs_) {
+        if (j->next.load(std::memory_order_relaxed) >= j->n) continue;
+        i = j->next.fetch_add(1);
+        if (i < j->n) {
+          job = j;
+          break;
+        }
+      }
+      if (!job) maybe_work_.store(false, std::memory_order_release);
+    }
+    if (!job) return false;
+    job->run(i);
+    return true;
+  }
+
+  void work() {
+    for (;;) {
+      if (help()) continue;
+      // Spin (tens of microseconds) without the lock for the next post.
+      for (int k = 0; k < 2000 && !maybe_work_.load(std::memory_order_acquire); ++k) std::this_thread::yield();
+      if (maybe_work_.load(std::memory_order_acquire)) continue;
+      std::unique_lock<std::mutex> lock(m_);
+      cv_.wait(lock, [&] { return maybe_work_.load(std::memory_order_acquire); });
+    }
+  }
+
+  std::mutex m_;
+  std::condition_variable cv_;
+  std::vector<PoolJob*> jobs_;
+  std::atomic<bool> maybe_work_{false};  // a posted job may have indices left
+};
+
+// The process's pool, made again in a forked child (which inherits no
+// threads; the old pool is left alone, its mutex possibly held).
+WorkerPool& pool() {
+  static std::mutex init;
+  static WorkerPool* pool = nullptr;
+  static pid_t owner = 0;
+  std::lock_guard<std::mutex> lock(init);
+  if (!pool || owner != getpid()) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    pool = new WorkerPool(std::min(16u, hw) - 1);  // never freed: workers live as long as the process
+    owner = getpid();
+  }
+  return *pool;
+}
+
+}  // namespace
+
 void parallel_for(size_t n, const std::function<void(size_t)>& f, unsigned threads) {
-  if (threads == 0) threads = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
-  threads = unsigned(std::min<size_t>(threads, n));
-  if (threads <= 1) {
+  if (threads == 1 || n <= 1 || std::thread::hardware_concurrency() <= 1) {
     for (size_t i = 0; i < n; ++i) f(i);
     return;
   }
-  std::atomic<size_t> next{0};
-  std::exception_ptr error;
-  std::mutex error_mutex;
-  auto work = [&] {
-    for (size_t i; (i = next.fetch_add(1)) < n;) {
-      try {
-        f(i);
-      } catch (...) {
-        std::lock_guard<std::mutex> lock(error_mutex);
-        if (!error) error = std::current_exception();
-      }
-    }
-  };
-  std::vector<std::thread> pool;
-  for (unsigned t = 1; t < threads; ++t) pool.emplace_back(work);
-  work();
-  for (std::thread& t : pool) t.join();
-  if (error) std::rethrow_exception(error);
+  PoolJob job;
+  job.f = &f;
+  job.n = n;
+  pool().run(job);
+  if (job.error) std::rethrow_exception(job.error);
 }
 
 std::vector<HOp> fuse(const std::vector<HOp>& ops, size_t max_qubits) {

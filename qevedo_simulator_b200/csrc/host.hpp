@@ -106,8 +106,9 @@ std::vector<HOp> fuse_where(const std::vector<HOp>& ops, size_t max_qubits,
                             const std::function<bool(const HOp&)>& fusable);
 std::vector<HOp> fuse(const std::vector<HOp>& ops, size_t max_qubits);
 
-// f(0) .. f(n - 1) on up to `threads` host threads (0: the hardware's
-// count, at most 16); the first exception thrown is rethrown here.
+// f(0) .. f(n - 1) on the calling thread and the process's pool of host
+// threads (at most 16 in all; `threads` = 1 runs them here, in order); the
+// first exception thrown is rethrown here. Calls may nest.
 void parallel_for(size_t n, const std::function<void(size_t)>& f, unsigned threads = 0);
 
 }  // namespace qvdg
