@@ -336,7 +336,10 @@ def run_ours(args, rank: int, world: int):
     plain_s = float(np.mean(plain_times))
     plain_info = plain.info()
     # Roofline of the dominant kernel of the tuned plan (the pass kind with
-    # the most device time): algorithmic bytes per launch / mean launch time.
+    # the most device time): algorithmic bytes per launch / mean launch time,
+    # over its whole-state launches. The zero-start passes (kind 4: the first
+    # passes of a run from |0...0>, over the subspace of the qubits touched
+    # so far) are reported apart.
     sec = np.concatenate(pass_t)
     byt = np.concatenate(pass_b)
     kind = np.concatenate(pass_k)
@@ -406,7 +409,10 @@ def run_ours(args, rank: int, world: int):
                       "staged": staged, "math": math_name,
                       "chosen_by": "learned cost model, judged against the greedy default" if fixed is None
                       else "--plan", "candidates_s": {k: round(v, 5) for k, v in candidates.items()},
-                      "pass_ms": [round(float(x) * 1e3, 3) for x in pass_t[-1]]},
+                      "pass_ms": [round(float(x) * 1e3, 3) for x in pass_t[-1]],
+                      "zero_start": {"passes": int(np.sum(pass_k[-1] == 4)),
+                                     "ms": round(float(np.sum(pass_t[-1][pass_k[-1] == 4])) * 1e3, 3),
+                                     "bytes": float(np.sum(pass_b[-1][pass_k[-1] == 4]))}},
             "plain": {"s": plain_s, "passes": plain_info["passes"], "kernels": plain_info["kernels"]},
             "tuned_over_plain": step / plain_s,
             "max_amp_err_vs_c128": err,

@@ -225,7 +225,9 @@ qvdg_status qvdg_state_layout(const qvdg_state* state, uint32_t* layout);
 
 /* Device address and byte size of the amplitude buffer (interleaved complex
  * in the state's precision, physical order), for callers that keep data on
- * the device. The pointer stays valid until the state is destroyed. */
+ * the device. The pointer stays valid until the state is destroyed. The
+ * caller may write through it: the state then no longer counts as |0...0>
+ * (which lets runs skip work) until the next qvdg_state_zero. */
 qvdg_status qvdg_state_device_buffer(const qvdg_state* state, void** pointer, size_t* bytes);
 
 /* Block the host until the state's stream is idle. */
@@ -355,9 +357,10 @@ qvdg_status qvdg_set_pass_timing(qvdg_state* state, int32_t enabled);
 
 /* Per-pass device seconds, algorithmic bytes and kind (1 staged tile pass,
  * 0 single-gate pass, 2 single-gate pass on the tensor cores, 3 the same
- * through a shared-memory stage for gates on index bits 1-3) of the last
- * gate run; `*count` receives the number of
- * passes, at most `capacity` entries are written. */
+ * through a shared-memory stage for gates on index bits 1-3, 4 a zero-start
+ * pass: run from |0...0>, it skips the amplitudes of qubits no earlier pass
+ * touched, which are zero) of the last gate run; `*count` receives the
+ * number of passes, at most `capacity` entries are written. */
 qvdg_status qvdg_pass_times(const qvdg_state* state, double* seconds, double* bytes, int32_t* staged,
                             size_t capacity, size_t* count);
 

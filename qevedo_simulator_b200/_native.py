@@ -313,7 +313,8 @@ class DeviceState:
         """(seconds, bytes, kind) per pass of the last gate run; kind 1 is a
         staged tile pass, 0 a single-gate pass, 2 a single-gate pass on the
         tensor cores, 3 the same through a shared-memory stage (gates on
-        index bits 1-3)."""
+        index bits 1-3), 4 a zero-start pass (run from |0...0>, it skips the
+        still-zero amplitudes of qubits no earlier pass touched)."""
         count = ct.c_size_t()
         check(lib().qvdg_pass_times(self._h, None, None, None, 0, ct.byref(count)))
         n = count.value

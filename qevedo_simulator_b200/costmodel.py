@@ -185,9 +185,10 @@ class CostModel:
         return self.rank(ops, num_qubits, cands)[0]
 
 
-def measure_plan(ops, num_qubits: int, opts, state: DeviceState, repeats: int = 2):
-    """(best device seconds, per-pass seconds) of one plan on `state`."""
-    best, passes = math.inf, None
+def measure_plan(ops, num_qubits: int, opts, state: DeviceState, repeats: int = 2, kinds: bool = False):
+    """(best device seconds, per-pass seconds[, per-pass kinds]) of one plan
+    run from |0...0> on `state`."""
+    best, passes, kind = math.inf, None, None
     with Plan(ops, num_qubits, state.precision_bits, opts) as plan:
         state.set_pass_timing(True)
         for _ in range(repeats):
@@ -195,9 +196,10 @@ def measure_plan(ops, num_qubits: int, opts, state: DeviceState, repeats: int = 
             s = state.execute(plan)
             if s["gate_seconds"] < best:
                 best = s["gate_seconds"]
-                passes = state.pass_times()[0].copy()
+                sec, _, k = state.pass_times()
+                passes, kind = sec.copy(), k.copy()
         state.set_pass_timing(False)
-    return best, passes
+    return (best, passes, kind) if kinds else (best, passes)
 
 
 def collect(op_lists, num_qubits: int, cands=None, repeats: int = 2):
@@ -208,11 +210,12 @@ def collect(op_lists, num_qubits: int, cands=None, repeats: int = 2):
         for ops in op_lists:
             for _, opts in cands or candidates():
                 feats = plan_features(ops, num_qubits, opts)
-                _, passes = measure_plan(ops, num_qubits, opts, st, repeats)
+                _, passes, kind = measure_plan(ops, num_qubits, opts, st, repeats, kinds=True)
                 if passes is None or len(passes) != feats.shape[0]:
                     continue
-                xs.append(feats)
-                ts.append(time_target(passes, num_qubits))
+                full = kind != 4  # zero-start passes move less than their features describe
+                xs.append(feats[full])
+                ts.append(time_target(passes[full], num_qubits))
     return np.concatenate(xs), np.concatenate(ts)
 
 

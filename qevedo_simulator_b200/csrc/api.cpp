@@ -462,6 +462,7 @@ qvdg_status qvdg_state_device_buffer(const qvdg_state* st, void** pointer, size_
     const StateImpl& s = impl(st);
     if (pointer) *pointer = s.amp;
     if (bytes) *bytes = s.amp_bytes;
+    s.zero_state = false;  // the caller may write through the pointer
   });
 }
 

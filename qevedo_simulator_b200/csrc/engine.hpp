@@ -45,7 +45,10 @@ struct StateImpl {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   std::vector<uint32_t> layout;  // logical -> physical
-  bool zero_state = false;       // |0...0> since the last zero(): a relabel costs no data movement
+  // |0...0> since the last zero(): a relabel costs no data movement and a
+  // program may run its zero-start passes. Mutable: handing out the device
+  // buffer (through a const handle) clears it, as the caller may write.
+  mutable bool zero_state = false;
   DeviceScratch work;            // device workspace (uploads, reductions, sampling)
   DeviceScratch work2;
   HostScratch host;              // pinned staging

@@ -34,6 +34,12 @@ struct Program {
   uint64_t gates = 0, kernels = 0, stages = 0;
   double bytes = 0.0;
   std::vector<float> features;  // kPassFeatures per pass
+  // Passes for a run that starts from |0...0>: until every qubit has been
+  // in some pass, the amplitudes with an untouched qubit set are zero and
+  // stay zero, so pass i (i < zero_passes.size()) may take those qubits as
+  // controls that must be 0 and move only 2^-c of the state.
+  std::vector<LoweredPass> zero_passes;
+  std::vector<double> zero_pass_bytes;
 };
 
 void pass_features(const Target& t, const PlannedPass& p, const LoweredPass& lp, const StageUpload& up, float* f);

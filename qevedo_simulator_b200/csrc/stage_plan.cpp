@@ -394,6 +394,44 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     prog.pass_bytes.push_back(b);
     prog.bytes += b;
   }
+  // Zero-start passes: each plain pass of the prefix in which some qubit
+  // is still untouched, with those qubits as controls of value 0 (the
+  // amplitudes they would select are zero before the pass and after it).
+  // On the 30-qubit grid circuit the first passes then move a few MB each
+  // instead of 17 GB.
+  uint64_t support = 0;  // logical qubits touched so far
+  const uint64_t every = t.n >= 64 ? ~uint64_t(0) : (uint64_t(1) << t.n) - 1;
+  for (const PlannedPass& p : passes) {
+    if (p.staged || p.block || p.ops.size() != 1) break;
+    for (uint32_t q : p.ops[0].targets) support |= uint64_t(1) << q;
+    for (auto& c : p.ops[0].controls) support |= uint64_t(1) << c.first;
+    if (support == every) break;
+    // The untouched qubits, lowest physical bit first. A tensor-core pass
+    // keeps at least 2^13 amplitudes selected, so that it stays on the
+    // tensor cores and gives the full pass's results exactly: the lowest
+    // untouched qubits stay free (contiguous accesses).
+    std::vector<uint32_t> idle;
+    for (uint32_t q = 0; q < t.n; ++q)
+      if (!((support >> q) & 1)) idle.push_back(q);
+    std::sort(idle.begin(), idle.end(), [&](uint32_t x, uint32_t y) { return tt.layout[x] < tt.layout[y]; });
+    size_t skip = 0;
+    if (plain_tc_eligible(tt, p, prog.cfg)) {
+      const size_t cap = t.n - 13 - std::min<size_t>(t.n - 13, p.ops[0].controls.size());
+      skip = idle.size() > cap ? idle.size() - cap : 0;
+    }
+    if (skip == idle.size()) {  // nothing to save
+      prog.zero_passes.push_back(prog.passes[prog.zero_passes.size()]);
+      prog.zero_pass_bytes.push_back(prog.pass_bytes[prog.zero_pass_bytes.size()]);
+      continue;
+    }
+    PlannedPass v = p;
+    for (size_t j = skip; j < idle.size(); ++j) v.ops[0].controls.push_back({idle[j], false});
+    PlainTcBlob vb;
+    const bool tc = plain_tc_eligible(tt, v, prog.cfg);
+    if (tc) vb = plain_tc_blob(tt, v.ops[0]);
+    prog.zero_passes.push_back(lower_pass(tt, v, prog.cfg, prog.upload, tc ? &vb : nullptr));
+    prog.zero_pass_bytes.push_back(2.0 * state_bytes / double(uint64_t(1) << v.ops[0].controls.size()));
+  }
   return prog;
 }
 
@@ -462,12 +500,15 @@ void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_s
     }
   }
   QVDG_CUDA(cudaEventRecord(s.ev_start, s.stream));
+  // From |0...0> the zero-start passes run where they exist.
+  const size_t zero = s.zero_state ? p.zero_passes.size() : 0;
+  auto pass = [&](size_t i) -> const LoweredPass& { return i < zero ? p.zero_passes[i] : p.passes[i]; };
   // The passes' layout (a relabel pass is timed with them).
   relabel_to(s, p.run_layout.empty() ? p.target.layout : p.run_layout);
   s.zero_state = false;
   for (size_t i = 0; i < p.passes.size(); ++i) {
     if (timing) QVDG_CUDA(cudaEventRecord(s.pass_events[i], s.stream));
-    launch_pass(s, p.passes[i], dev);
+    launch_pass(s, pass(i), dev);
   }
   if (timing) QVDG_CUDA(cudaEventRecord(s.pass_events[p.passes.size()], s.stream));
   QVDG_CUDA(cudaEventRecord(s.ev_stop, s.stream));
@@ -492,20 +533,24 @@ void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_s
       float t = 0.f;
       QVDG_CUDA(cudaEventElapsedTime(&t, s.pass_events[i], s.pass_events[i + 1]));
       s.pass_seconds.push_back(double(t) * 1e-3);
-      const LoweredPass& lp = p.passes[i];
+      const LoweredPass& lp = pass(i);
       int kind = lp.staged ? 1 : 0;
       if (!lp.staged && lp.plain.tensor)
         kind = dense_tc_staged(s.n, lp.plain.targets, lp.plain.controls.size()) ? 3 : 2;
+      if (i < zero && p.zero_pass_bytes[i] < p.pass_bytes[i]) kind = 4;  // a zero-start pass
       s.pass_kinds.push_back(kind);
     }
     s.pass_bytes = p.pass_bytes;
+    for (size_t i = 0; i < zero; ++i) s.pass_bytes[i] = p.zero_pass_bytes[i];
   }
   if (stats) {
+    double bytes = p.bytes;
+    for (size_t i = 0; i < zero; ++i) bytes += p.zero_pass_bytes[i] - p.pass_bytes[i];
     stats->kernels += p.kernels;
     stats->passes += p.passes.size();
     stats->stages += p.stages;
     stats->gate_seconds += ms * 1e-3;
-    stats->bytes += p.bytes;
+    stats->bytes += bytes;
   }
 }
 

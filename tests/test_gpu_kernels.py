@@ -309,6 +309,36 @@ def test_tensor_core_plain_passes_at_24_qubits(kind):
                 assert ref.max_abs_diff(st) < 1e-6, (kind, fuse)
 
 
+@pytest.mark.parametrize("kind", ["grid", "qft", "mixed"])
+def test_zero_start_passes_match_full_passes(kind):
+    """Run from |0...0> (after zero()), a plan's first passes take every
+    qubit that no pass has touched yet as a control of value 0: those
+    amplitudes are zero and stay zero. The result equals, exactly, the same
+    plan run on |0...0> loaded as amplitudes (every pass over the whole
+    state), for CUDA-core and tensor-core plans, and the zero-start run
+    moves fewer bytes."""
+    from qevedo_simulator_b200 import Plan, library
+
+    n = 21
+    if kind == "grid":
+        ops = library.random_grid_circuit(3, 7, 10, seed=8).ops()
+    elif kind == "qft":
+        ops = library.qft(n).ops()
+    else:
+        ops = library.mixed_ops(n, 6, seed=9)
+    basis = np.zeros(2 ** n, dtype=np.complex128)
+    basis[0] = 1.0
+    for opts in (options(4, staged=False), options(5, staged=False, math="tensor"),
+                 options(6, staged=False, math="tensor")):
+        with Plan(ops, n, 32, opts) as plan, DeviceState(n, 32) as a, DeviceState(n, 32) as b:
+            a.zero()
+            sa = a.execute(plan)
+            b.set_amplitudes(basis)
+            sb = b.execute(plan)
+            assert a.max_abs_diff(b) == 0.0, (kind, opts.max_fused_qubits, opts.math)
+            assert sa["bytes"] < sb["bytes"], (sa, sb)
+
+
 def test_qft_plans_with_commuting_diagonal_gates():
     """The 22-qubit QFT as a reusable tensor-core plan at fusion 5 and 6,
     whose fusion lets controlled phases commute past each other (and beam
