@@ -246,11 +246,16 @@ qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const
 /* Free a plan (NULL is accepted). */
 qvdg_status qvdg_plan_destroy(qvdg_plan* plan);
 
-/* Gates, fused kernels, passes, stages and algorithmic bytes of a plan. */
+/* Gates, fused kernels, passes, stages and algorithmic bytes of a plan (as
+ * run from |0...0>, whole passes counted). */
 qvdg_status qvdg_plan_info(const qvdg_plan* plan, qvdg_stats* stats);
 
-/* Apply a plan to a state of its size, precision and layout (the execution
- * half of apply_ops, src/simulator.rs:122-147). */
+/* Apply a plan to a state of its size and precision, in any layout (the
+ * execution half of apply_ops, src/simulator.rs:122-147). A tensor-core
+ * plain plan may hold two fusions: the one cheapest from |0...0>, run on a
+ * state still |0...0> since its last qvdg_state_zero (its first passes skip
+ * the amplitudes of untouched qubits), and the one cheapest for any other
+ * state. */
 qvdg_status qvdg_plan_execute(qvdg_state* state, const qvdg_plan* plan, qvdg_stats* stats);
 
 /* ---- Learned cost model ------------------------------------------------
@@ -261,7 +266,9 @@ qvdg_status qvdg_plan_execute(qvdg_state* state, const qvdg_plan* plan, qvdg_sta
 #define QVDG_PASS_FEATURES 32
 
 /* Features of every pass the planner builds for `ops` on a `num_qubits`
- * state under `options` (host only: no device work). `out` receives at most
+ * state under `options` (host only: no device work), for a state other than
+ * |0...0> (whole passes; a plan run from |0...0> may pick another fusion and
+ * skips the amplitudes of untouched qubits). `out` receives at most
  * `capacity` rows of QVDG_PASS_FEATURES floats; `*num_passes` the number of
  * passes. */
 qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "batch.hpp"
@@ -28,6 +29,12 @@ struct qvdg_plan {
   qvdg::DeviceUpload dev;
   void* device = nullptr;  // owned copy of the gate programs and matrices
   int device_id = 0;
+  // The plan for states other than |0...0>, where the fusion scored from
+  // |0...0> (its zero-start passes) differs from the one scored for any
+  // state; run by qvdg_plan_execute on such states.
+  std::unique_ptr<qvdg::Program> general;
+  qvdg::DeviceUpload general_dev;
+  void* general_device = nullptr;
 };
 
 namespace qvdg {
@@ -162,12 +169,39 @@ std::vector<HOp> lower_ops(const qvdg_op* ops, size_t n, uint32_t num_qubits) {
   return out;
 }
 
+// A plan's gate programs and matrices in its precision, one device copy
+// owned by the plan.
+void upload_plan(const Program& p, uint32_t precision_bits, void** device, DeviceUpload* dev) {
+  const StageUpload& up = p.upload;
+  auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t gate_bytes = up.gates.size() * sizeof(TileGate);
+  const size_t mat_bytes = up.mats.size() * (precision_bits == 32 ? 4 : 8);
+  std::vector<char> h(align(gate_bytes) + align(mat_bytes) + align(up.tc.size()) + 256, 0);
+  if (gate_bytes) std::memcpy(h.data(), up.gates.data(), gate_bytes);
+  if (precision_bits == 32) {
+    float* f = reinterpret_cast<float*>(h.data() + align(gate_bytes));
+    for (size_t i = 0; i < up.mats.size(); ++i) f[i] = float(up.mats[i]);
+  } else if (mat_bytes) {
+    std::memcpy(h.data() + align(gate_bytes), up.mats.data(), mat_bytes);
+  }
+  if (!up.tc.empty()) std::memcpy(h.data() + align(gate_bytes) + align(mat_bytes), up.tc.data(), up.tc.size());
+  if (cudaMalloc(device, h.size()) != cudaSuccess) {
+    cudaGetLastError();
+    *device = nullptr;
+    throw Error(QVDG_ERR_OUT_OF_MEMORY, "cannot allocate the plan's device memory");
+  }
+  QVDG_CUDA(cudaMemcpy(*device, h.data(), h.size(), cudaMemcpyHostToDevice));
+  dev->gates = static_cast<const TileGate*>(*device);
+  dev->mats = static_cast<const char*>(*device) + align(gate_bytes);
+  dev->tc = static_cast<const uint8_t*>(*device) + align(gate_bytes) + align(mat_bytes);
+}
+
 // Plan, upload and run `ops` on the state (the reference's apply_ops,
 // src/simulator.rs:122-147).
 void apply_program(StateImpl& s, const std::vector<HOp>& ops, const qvdg_options& opt, qvdg_stats* stats) {
   // One-shot: narrow beam searches where a pass streams at least 8 GB.
-  const Program prog =
-      build_program(target_of(s), ops, opt, s.n >= 29 ? FusionSearch::Beam : FusionSearch::Lookahead);
+  const Program prog = build_program(target_of(s), ops, opt,
+                                     s.n >= 29 ? FusionSearch::Beam : FusionSearch::Lookahead, s.zero_state);
   const DeviceUpload dev = upload_program(s, prog, s.work);
   run_program(s, prog, dev, stats);
 }
@@ -490,31 +524,20 @@ qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const
     qvdg_plan* plan = new qvdg_plan();
     plan->device_id = dev;
     try {
-      plan->program = build_program(t, lower_ops(ops, num_ops, num_qubits), opt, FusionSearch::Thorough);
+      const std::vector<HOp> hops = lower_ops(ops, num_ops, num_qubits);
+      plan->program = build_program(t, hops, opt, FusionSearch::Thorough, true);
       plan->program.gates = num_ops;
-      // Gate programs and matrices in the plan's precision, one device copy.
-      const StageUpload& up = plan->program.upload;
-      auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
-      const size_t gate_bytes = up.gates.size() * sizeof(TileGate);
-      const size_t mat_bytes = up.mats.size() * (precision_bits == 32 ? 4 : 8);
-      std::vector<char> h(align(gate_bytes) + align(mat_bytes) + align(up.tc.size()) + 256, 0);
-      if (gate_bytes) std::memcpy(h.data(), up.gates.data(), gate_bytes);
-      if (precision_bits == 32) {
-        float* f = reinterpret_cast<float*>(h.data() + align(gate_bytes));
-        for (size_t i = 0; i < up.mats.size(); ++i) f[i] = float(up.mats[i]);
-      } else if (mat_bytes) {
-        std::memcpy(h.data() + align(gate_bytes), up.mats.data(), mat_bytes);
+      upload_plan(plan->program, precision_bits, &plan->device, &plan->dev);
+      // Tensor-core plain plans pick their fusion by the cost from |0...0>;
+      // the pick for any other state is kept beside it where it differs.
+      if (!opt.staged && opt.math == QVDG_MATH_TENSOR && opt.max_fused_qubits >= 5 && num_qubits >= 13) {
+        Program general = build_program(t, hops, opt, FusionSearch::Thorough, false);
+        if (general.features != plan->program.features || general.run_layout != plan->program.run_layout) {
+          general.gates = num_ops;
+          plan->general = std::make_unique<Program>(std::move(general));
+          upload_plan(*plan->general, precision_bits, &plan->general_device, &plan->general_dev);
+        }
       }
-      if (!up.tc.empty()) std::memcpy(h.data() + align(gate_bytes) + align(mat_bytes), up.tc.data(), up.tc.size());
-      if (cudaMalloc(&plan->device, h.size()) != cudaSuccess) {
-        cudaGetLastError();
-        plan->device = nullptr;
-        throw Error(QVDG_ERR_OUT_OF_MEMORY, "cannot allocate the plan's device memory");
-      }
-      QVDG_CUDA(cudaMemcpy(plan->device, h.data(), h.size(), cudaMemcpyHostToDevice));
-      plan->dev.gates = static_cast<const TileGate*>(plan->device);
-      plan->dev.mats = static_cast<const char*>(plan->device) + align(gate_bytes);
-      plan->dev.tc = static_cast<const uint8_t*>(plan->device) + align(gate_bytes) + align(mat_bytes);
     } catch (...) {
       qvdg_plan_destroy(plan);
       throw;
@@ -526,6 +549,7 @@ qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const
 qvdg_status qvdg_plan_destroy(qvdg_plan* plan) {
   if (!plan) return QVDG_OK;
   if (plan->device) cudaFree(plan->device);
+  if (plan->general_device) cudaFree(plan->general_device);
   delete plan;
   return QVDG_OK;
 }
@@ -552,7 +576,10 @@ qvdg_status qvdg_plan_execute(qvdg_state* st, const qvdg_plan* plan, qvdg_stats*
     // A state in another layout is relabelled first (free on |0...0>).
     require(plan->device_id == s.device, "the plan lives on another device");
     if (stats) stats->gates += plan->program.gates;
-    run_program(s, plan->program, plan->dev, stats);
+    if (plan->general && !s.zero_state)
+      run_program(s, *plan->general, plan->general_dev, stats);
+    else
+      run_program(s, plan->program, plan->dev, stats);
   });
 }
 
@@ -656,7 +683,8 @@ qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, con
     t.n = num_qubits;
     t.bits = int(precision_bits);
     for (uint32_t q = 0; q < num_qubits; ++q) t.layout.push_back(q);
-    const Program prog = build_program(t, lower_ops(ops, num_ops, num_qubits), opt, FusionSearch::Thorough);
+    // The program for any state: the cost model predicts whole passes.
+    const Program prog = build_program(t, lower_ops(ops, num_ops, num_qubits), opt, FusionSearch::Thorough, false);
     const size_t rows = prog.passes.size();
     if (num_passes) *num_passes = rows;
     if (out) std::memcpy(out, prog.features.data(), std::min(rows, capacity) * kPassFeatures * sizeof(float));

@@ -50,8 +50,11 @@ void pass_features(const Target& t, const PlannedPass& p, const LoweredPass& lp,
 // one-shot run only where its passes are long enough to pay for it.
 enum class FusionSearch { Lookahead, Beam, Thorough };
 
+// `from_zero`: score tensor-core plain candidates by their cost from
+// |0...0> (zero-start passes), the usual start of a run; plans built once
+// assume it too, and still run on any state.
 Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt,
-                      FusionSearch search);
+                      FusionSearch search, bool from_zero);
 
 // Copy the program's gate data to `dst` on `stream` through the state's
 // pinned staging buffer.

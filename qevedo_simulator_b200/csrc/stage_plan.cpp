@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <functional>
 #include <cstring>
 #include <string>
@@ -172,7 +173,7 @@ Target target_of(const StateImpl& s) {
 }
 
 Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt,
-                      FusionSearch search) {
+                      FusionSearch search, bool from_zero) {
   Program prog;
   prog.target = t;
   prog.gates = ops.size();
@@ -252,6 +253,23 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       std::vector<uint32_t> at(t.n);  // physical -> logical
       for (uint32_t q = 0; q < t.n; ++q) at[t.layout[q]] = q;
       const uint64_t now = (uint64_t(1) << at[1]) | (uint64_t(1) << at[2]) | (uint64_t(1) << at[3]);
+      // From |0...0> the passes before every qubit has been touched move
+      // 2^(touched - n) of the state (zero-start passes; at least 2^13
+      // amplitudes, plus a launch's worth): each pass's cost is scaled by
+      // that share. At 30 qubits two 45-pass fusions of the grid circuit
+      // spend 11 and 7 passes that way.
+      const uint64_t every = t.n >= 64 ? ~uint64_t(0) : (uint64_t(1) << t.n) - 1;
+      auto shares = [&](const std::vector<uint64_t>& gm) {
+        std::vector<double> f(gm.size(), 1.0);
+        uint64_t touched = 0;
+        for (size_t k = 0; from_zero && k < gm.size(); ++k) {
+          touched |= gm[k];
+          if (touched == every) break;
+          f[k] = std::ldexp(1.0, std::max(__builtin_popcountll(touched), 13) - int(t.n)) + 0.005;
+        }
+        return f;
+      };
+      auto weight = [](int low) { return low == 0 ? 1.0 : (low == 1 ? 1.2 : (low == 2 ? 1.45 : 2.1)); };
       parallel_for(cand.size(), [&](size_t i) {
         std::vector<uint64_t> gm;
         for (const FusedGroup& g : cand[i]) {
@@ -259,12 +277,10 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
           for (uint32_t q : g.qubits) m |= uint64_t(1) << q;
           gm.push_back(m);
         }
+        const std::vector<double> f = shares(gm);
         auto eval = [&](uint64_t s) {
           double c = 0.0;
-          for (uint64_t m : gm) {
-            const int low = __builtin_popcountll(m & s);
-            c += low == 0 ? 1.0 : (low == 1 ? 1.2 : (low == 2 ? 1.45 : 2.1));
-          }
+          for (size_t k = 0; k < gm.size(); ++k) c += weight(__builtin_popcountll(gm[k] & s)) * f[k];
           return c;
         };
         // Triples among the 12 qubits in the fewest groups (the cost grows
@@ -296,14 +312,18 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       for (size_t i = 1; i < cand.size(); ++i)
         if (cost[i] < cost[pick] - 1e-9) pick = i;
       // Relabel only where it saves at least 1.5 passes (it costs one when
-      // the state is not |0...0>).
+      // the state is not |0...0>), or any saving for a one-shot run on
+      // |0...0>, where it is free.
       auto eval_now = [&](const std::vector<FusedGroup>& gs) {
-        double c = 0.0;
+        std::vector<uint64_t> gm;
         for (const FusedGroup& g : gs) {
-          int low = 0;
-          for (uint32_t q : g.qubits) low += ((now >> q) & 1) ? 1 : 0;
-          c += low == 0 ? 1.0 : (low == 1 ? 1.2 : (low == 2 ? 1.45 : 2.1));
+          uint64_t m = 0;
+          for (uint32_t q : g.qubits) m |= uint64_t(1) << q;
+          gm.push_back(m);
         }
+        const std::vector<double> f = shares(gm);
+        double c = 0.0;
+        for (size_t k = 0; k < gm.size(); ++k) c += weight(__builtin_popcountll(gm[k] & now)) * f[k];
         return c;
       };
       size_t keep = 0;
@@ -315,7 +335,7 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
           keep_cost = c;
         }
       }
-      if (cost[pick] > keep_cost - 1.5) {
+      if (cost[pick] > keep_cost - (search == FusionSearch::Thorough || !from_zero ? 1.5 : 1e-9)) {
         pick = keep;
         low_set[pick] = now;
       }

@@ -313,10 +313,12 @@ def test_tensor_core_plain_passes_at_24_qubits(kind):
 def test_zero_start_passes_match_full_passes(kind):
     """Run from |0...0> (after zero()), a plan's first passes take every
     qubit that no pass has touched yet as a control of value 0: those
-    amplitudes are zero and stay zero. The result equals, exactly, the same
-    plan run on |0...0> loaded as amplitudes (every pass over the whole
-    state), for CUDA-core and tensor-core plans, and the zero-start run
-    moves fewer bytes."""
+    amplitudes are zero and stay zero. For plans without a fusion search
+    (CUDA-core fusion 4, tensor-core fusion 4) the result equals, exactly,
+    the same plan run on |0...0> loaded as amplitudes (every pass over the
+    whole state), and the zero-start run moves fewer bytes. Tensor-core
+    fusion-6 plans pick their fusion by the cost from |0...0> and keep the
+    general pick for other states: both runs match complex128 to 1e-6."""
     from qevedo_simulator_b200 import Plan, library
 
     n = 21
@@ -328,15 +330,20 @@ def test_zero_start_passes_match_full_passes(kind):
         ops = library.mixed_ops(n, 6, seed=9)
     basis = np.zeros(2 ** n, dtype=np.complex128)
     basis[0] = 1.0
-    for opts in (options(4, staged=False), options(5, staged=False, math="tensor"),
-                 options(6, staged=False, math="tensor")):
-        with Plan(ops, n, 32, opts) as plan, DeviceState(n, 32) as a, DeviceState(n, 32) as b:
-            a.zero()
-            sa = a.execute(plan)
-            b.set_amplitudes(basis)
-            sb = b.execute(plan)
-            assert a.max_abs_diff(b) == 0.0, (kind, opts.max_fused_qubits, opts.math)
-            assert sa["bytes"] < sb["bytes"], (sa, sb)
+    with DeviceState(n, 64) as ref:
+        ref.zero()
+        ref.apply_ops(ops, options(4, staged=False))
+        for opts, exact in ((options(4, staged=False), True), (options(4, staged=False, math="tensor"), True),
+                            (options(6, staged=False, math="tensor"), False)):
+            with Plan(ops, n, 32, opts) as plan, DeviceState(n, 32) as a, DeviceState(n, 32) as b:
+                a.zero()
+                sa = a.execute(plan)
+                b.set_amplitudes(basis)
+                sb = b.execute(plan)
+                if exact:
+                    assert a.max_abs_diff(b) == 0.0, (kind, opts.max_fused_qubits, opts.math)
+                    assert sa["bytes"] < sb["bytes"], (sa, sb)
+                assert ref.max_abs_diff(a) < 1e-6 and ref.max_abs_diff(b) < 1e-6, (kind, opts.max_fused_qubits)
 
 
 def test_qft_plans_with_commuting_diagonal_gates():
