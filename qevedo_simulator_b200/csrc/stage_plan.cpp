@@ -419,10 +419,11 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
   // amplitudes they would select are zero before the pass and after it).
   // On the 30-qubit grid circuit the first passes then move a few MB each
   // instead of 17 GB.
+  // Only programs meant to run from |0...0> get them.
   uint64_t support = 0;  // logical qubits touched so far
   const uint64_t every = t.n >= 64 ? ~uint64_t(0) : (uint64_t(1) << t.n) - 1;
   for (const PlannedPass& p : passes) {
-    if (p.staged || p.block || p.ops.size() != 1) break;
+    if (!from_zero || p.staged || p.block || p.ops.size() != 1) break;
     for (uint32_t q : p.ops[0].targets) support |= uint64_t(1) << q;
     for (auto& c : p.ops[0].controls) support |= uint64_t(1) << c.first;
     if (support == every) break;
