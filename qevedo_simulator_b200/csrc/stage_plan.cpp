@@ -191,21 +191,22 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     // as its product matrix.
     // The groups' product matrices are independent: built on host threads.
     const bool gates = opt.math == QVDG_MATH_GATES;
-    // Tensor-core plain plans of 5-6 qubit groups seed each group among the
-    // next few ready ops: the fusions with 1-8 candidate seeds are scored by
-    // their passes, a pass with targets on index bits 1-3 counting as the
-    // 1.2-2.1 clean passes it takes on the tensor-core kernels, and the
-    // cheapest is kept (50 passes instead of 55 on the 30-qubit grid circuit
-    // at fusion 6, 64 instead of 70 at fusion 5; at fusion 4 the seeds would
-    // add passes). Other plain plans keep the reference's greedy fusion.
+    // Tensor-core plain plans of 5-6 qubit groups search their fusion: the
+    // reference's greedy one, seed-lookahead variants and beam searches over
+    // the seeds, each scored by its passes (a pass with targets on index
+    // bits 1-3 counting as the 1.2-2.1 clean passes it takes on the
+    // tensor-core kernels, and from |0...0> by the share of the state it
+    // moves); 45 passes instead of 55 on the 30-qubit grid circuit at fusion
+    // 6 (at fusion 4 the searches would add passes). Other plain plans keep
+    // the reference's greedy fusion.
     const FusionInput fin = fusion_input(ops, [](const HOp&) { return true; });
     std::vector<FusedGroup> groups = fuse_groups_lookahead(fin, max_fused, 0);
     if (opt.math == QVDG_MATH_TENSOR && max_fused >= 5 && t.n >= 13) {
-      // Candidate fusions (seed lookahead 0-8) and, for each, the three
-      // qubits to place on physical bits 1-3 (a relabel that costs nothing
-      // on a |0...0> state and one swap pass otherwise): the pair with the
-      // lowest estimated cost, a pass with k targets on bits 1-3 counting as
-      // 1, 1.2, 1.45 or 2.1 clean passes.
+      // Candidate fusions and, for each, the three qubits to place on
+      // physical bits 1-3 (a relabel that costs nothing on a |0...0> state
+      // and one swap pass otherwise): the pair with the lowest estimated
+      // cost, a pass with k targets on bits 1-3 counting as 1, 1.2, 1.45 or
+      // 2.1 clean passes.
       // Fusions: the lookahead ones and the beam searches' (the widest
       // first, each on its own thread). At 30 qubits (depth-20 grid
       // circuit, fusion 6) the narrow beams take 50 passes to 47, the wide
