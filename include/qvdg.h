@@ -274,6 +274,25 @@ qvdg_status qvdg_plan_execute(qvdg_state* state, const qvdg_plan* plan, qvdg_sta
 qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
                                const qvdg_options* options, float* out, size_t capacity, size_t* num_passes);
 
+/* The ops a plain plan's passes apply, in order, on logical qubits (host
+ * only): each fused group as its product matrix, a pass applied gate by gate
+ * as its member gates. The fusion is the one a plan picks for a state
+ * other than |0...0> (from_zero = 0) or for |0...0> (from_zero != 0).
+ * Reference: fuse (src/fusion.rs:63-170), which returns the greedy fusion's
+ * ops the same way. Op i has num_targets[i] targets and num_controls[i]
+ * controls; their qubits (targets, then controls) follow one another in
+ * `qubits`, with 0 for targets and the required value for controls in
+ * `control_values`, and its 4^k complex entries (row-major, interleaved
+ * re/im) in `matrices`. `*num_fused`, `*num_qubit_entries` and
+ * `*num_matrix_doubles` receive the sizes; with `capacity` below the
+ * number of ops, only the sizes are written. Plain plans only
+ * (options->staged = 0). */
+qvdg_status qvdg_plan_fused_ops(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                                const qvdg_options* options, int32_t from_zero, uint32_t* num_targets,
+                                uint32_t* num_controls, uint32_t* qubits, uint8_t* control_values, double* matrices,
+                                size_t capacity, size_t* num_fused, size_t* num_qubit_entries,
+                                size_t* num_matrix_doubles);
+
 /* An MLP with two hidden ReLU layers of `hidden` units and one linear
  * output, trained and evaluated by this library's own CUDA kernels (fp32,
  * on the current device). Parameters, in order: W1 (hidden x inputs), b1,

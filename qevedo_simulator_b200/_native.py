@@ -73,6 +73,11 @@ _SIGNATURES = {
     "qvdg_plan_features": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(QvdgOp), ct.c_size_t,
                                       ct.POINTER(QvdgOptions), ct.POINTER(ct.c_float), ct.c_size_t,
                                       ct.POINTER(ct.c_size_t)]),
+    "qvdg_plan_fused_ops": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(QvdgOp), ct.c_size_t,
+                                       ct.POINTER(QvdgOptions), ct.c_int32, ct.POINTER(ct.c_uint32),
+                                       ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint8),
+                                       ct.POINTER(ct.c_double), ct.c_size_t, ct.POINTER(ct.c_size_t),
+                                       ct.POINTER(ct.c_size_t), ct.POINTER(ct.c_size_t)]),
     "qvdg_mlp_create": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.c_uint64, ct.POINTER(_P)]),
     "qvdg_mlp_destroy": (ct.c_int, [_P]),
     "qvdg_mlp_num_params": (ct.c_int, [_P, ct.POINTER(ct.c_size_t)]),

@@ -72,6 +72,39 @@ def plan_features(ops, num_qubits: int, opts, precision_bits: int = 32) -> np.nd
     return rows[:count.value]
 
 
+def fused_ops(ops, num_qubits: int, opts, precision_bits: int = 32, from_zero: bool = False) -> list:
+    """The ops a plain plan's passes apply, in order (host only): each fused
+    group as one Op with its product matrix, on logical qubits; the fusion
+    a plan picks for a general state, or for |0...0> with `from_zero`."""
+    from .circuit import Op
+
+    packed = PackedOps(ops)
+    nf, nq, nm = ct.c_size_t(), ct.c_size_t(), ct.c_size_t()
+    args = (num_qubits, precision_bits, packed.array, packed.count, ct.byref(opts), 1 if from_zero else 0)
+    check(lib().qvdg_plan_fused_ops(*args, None, None, None, None, None, 0, ct.byref(nf), ct.byref(nq),
+                                    ct.byref(nm)))
+    k = np.zeros(max(nf.value, 1), dtype=np.uint32)
+    c = np.zeros(max(nf.value, 1), dtype=np.uint32)
+    q = np.zeros(max(nq.value, 1), dtype=np.uint32)
+    v = np.zeros(max(nq.value, 1), dtype=np.uint8)
+    m = np.zeros(max(nm.value, 2), dtype=np.float64)
+    u32 = ct.POINTER(ct.c_uint32)
+    check(lib().qvdg_plan_fused_ops(*args, k.ctypes.data_as(u32), c.ctypes.data_as(u32), q.ctypes.data_as(u32),
+                                    v.ctypes.data_as(ct.POINTER(ct.c_uint8)), m.ctypes.data_as(ct.POINTER(ct.c_double)),
+                                    nf.value, ct.byref(nf), ct.byref(nq), ct.byref(nm)))
+    out, qi, mi = [], 0, 0
+    cm = m.view(np.complex128)
+    for i in range(nf.value):
+        t, cc = int(k[i]), int(c[i])
+        targets = [int(x) for x in q[qi:qi + t]]
+        controls = [(int(q[qi + t + j]), bool(v[qi + t + j])) for j in range(cc)]
+        d = 1 << t
+        out.append(Op(targets, controls, cm[mi:mi + d * d].reshape(d, d).copy()))
+        qi += t + cc
+        mi += d * d
+    return out
+
+
 def time_target(seconds: np.ndarray, num_qubits: int) -> np.ndarray:
     """log(seconds per 2^24 amplitudes)."""
     return np.log(np.maximum(seconds, 1e-9) / 2.0 ** (num_qubits - 24)).astype(np.float32)

@@ -691,6 +691,54 @@ qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, con
   });
 }
 
+qvdg_status qvdg_plan_fused_ops(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                                const qvdg_options* options, int32_t from_zero, uint32_t* num_targets,
+                                uint32_t* num_controls, uint32_t* qubits, uint8_t* control_values, double* matrices,
+                                size_t capacity, size_t* num_fused, size_t* num_qubit_entries,
+                                size_t* num_matrix_doubles) {
+  return guarded([&] {
+    require(precision_bits == 32 || precision_bits == 64, "precision must be 32 or 64 bits");
+    require(num_qubits >= 1 && num_qubits <= 40, "a state needs 1 to 40 qubits");
+    qvdg_options opt;
+    qvdg_default_options(&opt);
+    if (options) opt = *options;
+    Target t;
+    t.n = num_qubits;
+    t.bits = int(precision_bits);
+    for (uint32_t q = 0; q < num_qubits; ++q) t.layout.push_back(q);
+    std::vector<HOp> fused;
+    build_program(t, lower_ops(ops, num_ops, num_qubits), opt, FusionSearch::Thorough, from_zero != 0, &fused);
+    size_t nq = 0, nm = 0;
+    for (const HOp& f : fused) {
+      nq += f.targets.size() + f.controls.size();
+      nm += 2 * f.matrix.a.size();
+    }
+    if (num_fused) *num_fused = fused.size();
+    if (num_qubit_entries) *num_qubit_entries = nq;
+    if (num_matrix_doubles) *num_matrix_doubles = nm;
+    if (fused.empty() || capacity < fused.size()) return;  // sizes only
+    require(num_targets && num_controls && qubits && control_values && matrices, "null output array");
+    size_t qi = 0, mi = 0;
+    for (size_t i = 0; i < fused.size(); ++i) {
+      const HOp& f = fused[i];
+      num_targets[i] = uint32_t(f.targets.size());
+      num_controls[i] = uint32_t(f.controls.size());
+      for (uint32_t q : f.targets) {
+        qubits[qi] = q;
+        control_values[qi++] = 0;
+      }
+      for (auto& c : f.controls) {
+        qubits[qi] = c.first;
+        control_values[qi++] = c.second ? 1 : 0;
+      }
+      for (const C& x : f.matrix.a) {
+        matrices[mi++] = x.re;
+        matrices[mi++] = x.im;
+      }
+    }
+  });
+}
+
 qvdg_status qvdg_mlp_create(uint32_t inputs, uint32_t hidden, uint64_t seed, qvdg_mlp** out) {
   return guarded([&] {
     require(out != nullptr, "null output handle");

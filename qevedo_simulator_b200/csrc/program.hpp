@@ -53,8 +53,11 @@ enum class FusionSearch { Lookahead, Beam, Thorough };
 // `from_zero`: score tensor-core plain candidates by their cost from
 // |0...0> (zero-start passes), the usual start of a run; plans built once
 // assume it too, and still run on any state.
+// `fused` (optional): receives the ops of a plain plan's passes in order,
+// on logical qubits (each fused group as its product matrix, or, for a pass
+// applied gate by gate, its member gates).
 Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt,
-                      FusionSearch search, bool from_zero);
+                      FusionSearch search, bool from_zero, std::vector<HOp>* fused = nullptr);
 
 // Copy the program's gate data to `dst` on `stream` through the state's
 // pinned staging buffer.

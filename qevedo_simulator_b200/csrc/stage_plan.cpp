@@ -173,7 +173,7 @@ Target target_of(const StateImpl& s) {
 }
 
 Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt,
-                      FusionSearch search, bool from_zero) {
+                      FusionSearch search, bool from_zero, std::vector<HOp>* fused) {
   Program prog;
   prog.target = t;
   prog.gates = ops.size();
@@ -387,6 +387,10 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       p.ops[0] = fuse_group(ops, groups[products[j]]);
       if (plain_tc_eligible(rt, p, prog.cfg)) blobs[products[j]] = plain_tc_blob(rt, p.ops[0]);
     }, wide ? 0u : 1u);
+  }
+  if (fused) {
+    if (opt.staged) throw Error(QVDG_ERR_INVALID, "fused ops exist for plain plans only");
+    for (const PlannedPass& p : passes) fused->insert(fused->end(), p.ops.begin(), p.ops.end());
   }
   // Passes are lowered on the layout they run with.
   Target run_target = t;

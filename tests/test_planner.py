@@ -1,0 +1,51 @@
+"""The planner's fused programs against the naive oracle (host only): every
+plain plan's passes, read back as ops (qvdg_plan_fused_ops, the counterpart
+of the reference's `fuse`, src/fusion.rs:63-170), applied in order to a
+random state give the circuit's own result. This covers the greedy fusion,
+the seed-lookahead and beam searches, the commuting-diagonal family (QFT,
+controlled phases) and both scorings (for a general state, and from
+|0...0>)."""
+
+import numpy as np
+import pytest
+
+from conftest import random_state
+from qevedo_simulator_b200 import costmodel, library, options
+
+
+def _circuit(kind: str, n: int):
+    if kind == "grid":
+        return library.random_grid_circuit(3, 5, 10, seed=21).ops()
+    if kind == "qft":
+        return library.qft(n).ops()
+    if kind == "mixed":
+        return library.mixed_ops(n, 5, seed=22)
+    return library.random_gate_circuit(n, 160, seed=23).ops()
+
+
+@pytest.mark.parametrize("kind", ["grid", "qft", "mixed", "random"])
+def test_fused_programs_equal_the_circuit(oracle, kind):
+    n = 15 if kind == "grid" else 14
+    ops = _circuit(kind, n)
+    psi = random_state(np.random.Generator(np.random.PCG64(40)), n)
+    expected = oracle.naive_apply_ops(psi, ops)
+    plans = [options(4, staged=False), options(5, staged=False, math="tensor"),
+             options(6, staged=False, math="tensor"), options(5, staged=False, math="gates")]
+    for opts in plans:
+        for from_zero in (False, True):
+            fused = costmodel.fused_ops(ops, n, opts, from_zero=from_zero)
+            assert len(fused) <= len(ops)
+            assert all(len(f.targets) <= opts.max_fused_qubits for f in fused if f.matrix.shape[0] > 1)
+            got = oracle.naive_apply_ops(psi, fused)
+            err = np.max(np.abs(got - expected))
+            assert err < 1e-10, (kind, opts.max_fused_qubits, opts.math, from_zero, err)
+        # The general-state fusion is the one the cost model's features describe.
+        rows = costmodel.plan_features(ops, n, opts)
+        if opts.math != 2:
+            assert rows.shape[0] == len(costmodel.fused_ops(ops, n, opts))
+
+
+def test_fused_ops_of_an_empty_circuit_and_staged_plans():
+    assert costmodel.fused_ops([], 14, options(6, staged=False, math="tensor")) == []
+    with pytest.raises(ValueError, match="plain plans only"):
+        costmodel.fused_ops(library.qft(14).ops(), 14, options(4, staged=True))
