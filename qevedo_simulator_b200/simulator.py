@@ -103,28 +103,49 @@ def count_outcomes(outcomes: np.ndarray, measures, num_clbits: int) -> dict:
     return dict(sorted(out.items()))
 
 
-def statevector(circuit: Circuit, *, precision: str = "double", max_fused_qubits: int = 4, staged: bool = True,
-                tile_qubits: int = 0, math: str = "fp32") -> np.ndarray:
+def _as_circuit(circuit) -> Circuit:
+    """A Circuit, or OpenQASM 2/3 text parsed into one (the reference's
+    `run` and `statevector` take either)."""
+    if isinstance(circuit, str):
+        from . import qasm
+
+        return qasm.parse(circuit)
+    return circuit
+
+
+def statevector(circuit: Circuit | str, *, precision: str = "double", max_fused_qubits: int = 4,
+                staged: bool = True, tile_qubits: int = 0, math: str = "fp32",
+                threads: int | str | None = None) -> np.ndarray:
     """The final state of a circuit without measurements, as complex128 in
     logical order (index bit q = qubit q). Double precision by default, as
-    the reference's `statevector` (python/src/lib.rs:686-718)."""
+    the reference's `statevector` (python/src/lib.rs:686-718). `threads`
+    is accepted for the reference's signature; host planning uses the
+    library's own thread pool."""
+    circuit = _as_circuit(circuit)
     ops = circuit.ops()
     with _native.DeviceState(circuit.num_qubits, _precision_bits(precision)) as st:
         st.apply_ops(ops, _native.options(max_fused_qubits, staged, tile_qubits, math=math))
         return st.amplitudes()
 
 
-def run(circuit: Circuit, shots: int = 1024, *, backend: str = "auto", seed: int | None = None,
-        precision: str = "single", max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0,
+def run(circuit: Circuit | str, shots: int = 1024, *, backend: str = "auto", seed: int | None = None,
+        precision: str = "single", max_bond_dimension: int = 256, truncation_threshold: float = 1e-16,
+        threads: int | str | None = None, max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0,
         math: str = "fp32", state: _native.DeviceState | None = None) -> RunResult:
-    """Sample `shots` shots of `circuit` on the device state vector.
+    """Sample `shots` shots of `circuit` (a Circuit or OpenQASM 2/3 text) on
+    the device state vector.
 
     `seed` seeds the uniforms (numpy PCG64; the reference seeds rand_pcg's
     Pcg64, whose streams this engine does not reproduce). Given the same
     uniforms, every outcome is bit-identical to the reference sampler's. A
     caller may pass a reusable `state` of the right size and precision.
+    `max_bond_dimension` and `truncation_threshold` (the reference's MPS
+    settings) and `threads` are accepted for the reference's signature
+    (python/python/qevedo/simulator/__init__.py:96-106) and do not affect
+    the state vector; host planning uses the library's own thread pool.
     """
     _check_backend(backend)
+    circuit = _as_circuit(circuit)
     bits = _precision_bits(precision)
     rng = np.random.Generator(np.random.PCG64(seed))
     opts = _native.options(max_fused_qubits, staged, tile_qubits, math=math)

@@ -197,3 +197,23 @@ def test_relative_phase_toffolis_follow_qelib1(oracle):
     assert max_distance(state(oracle, direct), state(oracle, parsed)) < 1e-12
     redefined = parse("OPENQASM 2.0;\ngate rccx a,b,c { ccx a,b,c; }\nqreg q[3];\nrccx q[0], q[1], q[2];")
     assert len(redefined._instructions) == 1
+
+
+def test_run_and_statevector_take_the_reference_arguments():
+    """`run` and `statevector` accept what the reference's Python wrappers
+    accept (python/python/qevedo/simulator/__init__.py:96-106, :141): a
+    Circuit or OpenQASM text, and the `threads` (and, for `run`, MPS)
+    keywords, which do not change the state-vector result."""
+    import inspect
+
+    from qevedo_simulator_b200 import simulator
+
+    run_params = inspect.signature(simulator.run).parameters
+    for name, default in (("backend", "auto"), ("seed", None), ("precision", "single"),
+                          ("max_bond_dimension", 256), ("truncation_threshold", 1e-16), ("threads", None)):
+        assert run_params[name].default == default, name
+    sv_params = inspect.signature(simulator.statevector).parameters
+    assert sv_params["threads"].default is None and sv_params["precision"].default == "double"
+    c = simulator._as_circuit('OPENQASM 2.0;\ninclude "qelib1.inc";\nqreg q[2];\ncreg c[2];\n'
+                              'h q[0];\ncx q[0],q[1];\nmeasure q -> c;')
+    assert (c.num_qubits, c.num_clbits, c.gate_count) == (2, 2, 2)
