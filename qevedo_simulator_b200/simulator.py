@@ -24,7 +24,10 @@ BACKENDS = ("auto", "statevector")
 @dataclass
 class RunResult:
     """Counts per classical bitstring (classical bit 0 on the right, Qiskit's
-    convention) and run statistics (src/simulator.rs:70-101)."""
+    convention) and run statistics (src/simulator.rs:70-101), with the
+    binding's fields (python/src/lib.rs:409-477): `fidelity`,
+    `max_bond_dimension` and `peak_active_qubits` belong to the MPS and
+    near-Clifford backends and are None here."""
 
     counts: dict
     backend: str = "statevector"
@@ -34,6 +37,12 @@ class RunResult:
     gate_seconds: float = 0.0
     measure_seconds: float = 0.0
     stats: dict = field(default_factory=dict)
+    fidelity: float | None = None
+    max_bond_dimension: int | None = None
+    peak_active_qubits: int | None = None
+
+    def __repr__(self) -> str:
+        return f'RunResult(backend="{self.backend}", {len(self.counts)} outcomes)'
 
 
 def _precision_bits(precision: str) -> int:

@@ -217,3 +217,11 @@ def test_run_and_statevector_take_the_reference_arguments():
     c = simulator._as_circuit('OPENQASM 2.0;\ninclude "qelib1.inc";\nqreg q[2];\ncreg c[2];\n'
                               'h q[0];\ncx q[0],q[1];\nmeasure q -> c;')
     assert (c.num_qubits, c.num_clbits, c.gate_count) == (2, 2, 2)
+
+
+def test_run_result_has_the_binding_fields():
+    from qevedo_simulator_b200.simulator import RunResult
+
+    r = RunResult(counts={"00": 3, "11": 5})
+    assert (r.backend, r.fidelity, r.max_bond_dimension, r.peak_active_qubits) == ("statevector", None, None, None)
+    assert repr(r) == 'RunResult(backend="statevector", 2 outcomes)'
