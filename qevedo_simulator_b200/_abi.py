@@ -82,19 +82,25 @@ class PackedOps:
     """Ops laid out as a contiguous qvdg_op array; owns every buffer the
     structs point into, so it must outlive the call it is passed to."""
 
-    def __init__(self, ops):
-        n = len(ops)
-        qubits, values, mats, ks, cs = [], [], [], [], []
-        for op in ops:
-            t, ctl = op.targets, op.controls
-            ks.append(len(t))
-            cs.append(len(ctl))
-            qubits += t
-            values += [0] * len(t)
-            for q, v in ctl:
-                qubits.append(q)
-                values.append(1 if v else 0)
-            mats.append(op.matrix)
+    def __init__(self, ops=None, *, parts=None):
+        """From ops (targets, controls [(qubit, value)], matrix), or from
+        `parts` = (target counts, control counts, qubits with targets first,
+        their values, matrices) already laid out."""
+        if parts is None:
+            qubits, values, mats, ks, cs = [], [], [], [], []
+            for op in ops:
+                t, ctl = op.targets, op.controls
+                ks.append(len(t))
+                cs.append(len(ctl))
+                qubits += t
+                values += [0] * len(t)
+                for q, v in ctl:
+                    qubits.append(q)
+                    values.append(1 if v else 0)
+                mats.append(op.matrix)
+        else:
+            ks, cs, qubits, values, mats = parts
+        n = len(ks)
         ks = np.array(ks or [0], dtype=np.uint32)
         cs = np.array(cs or [0], dtype=np.uint32)
         if n:

@@ -189,6 +189,35 @@ def _named_matrix(name: str, params: tuple) -> np.ndarray:
     return hit
 
 
+def packed_gate_ops(instructions):
+    """The ops of the "gate" instructions, as gate_op lowers them, laid out
+    for the C ABI in one pass (no Op objects in between)."""
+    from ._abi import PackedOps
+
+    ks, cs, qubits, values, mats = [], [], [], [], []
+    for ins in instructions:
+        if ins[0] != "gate":
+            continue
+        gate, qs = ins[1], ins[2]
+        form = _CONTROLLED.get(gate.name)
+        if form is not None:
+            nc = form[0]
+            ks.append(len(qs) - nc)
+            cs.append(nc)
+            qubits += qs[nc:]
+            qubits += qs[:nc]
+            values += [0] * (len(qs) - nc)
+            values += [1] * nc
+            mats.append(_named_matrix(form[1], gate.params))
+        else:
+            ks.append(len(qs))
+            cs.append(0)
+            qubits += qs
+            values += [0] * len(qs)
+            mats.append(gate.matrix() if gate.name == "unitary" else _named_matrix(gate.name, gate.params))
+    return PackedOps(parts=(ks, cs, qubits, values, mats))
+
+
 def gate_op(gate: Gate, qubits) -> Op:
     """simulator::gate_op (src/simulator.rs:106-119): controls stay separate so
     the kernel touches only the controlled part of the state."""

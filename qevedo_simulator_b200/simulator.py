@@ -16,7 +16,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native
-from .circuit import Circuit, Gate, gate_op
+from .circuit import Circuit, Gate, gate_op, packed_gate_ops
 
 BACKENDS = ("auto", "statevector")
 
@@ -166,8 +166,7 @@ def run(circuit: Circuit | str, shots: int = 1024, *, backend: str = "auto", see
         split = terminal_split(circuit)
         result = RunResult(counts={})
         if split is not None:
-            ops = [gate_op(i[1], i[2]) for i in circuit._instructions[:split] if i[0] == "gate"]
-            stats = st.apply_ops(ops, opts)
+            stats = st.apply_packed(packed_gate_ops(circuit._instructions[:split]), opts)
             result.gates, result.kernels, result.passes = stats["gates"], stats["kernels"], stats["passes"]
             result.gate_seconds = stats["gate_seconds"]
             result.stats = stats

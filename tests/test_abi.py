@@ -66,3 +66,28 @@ def test_batch_validation_needs_no_device():
     assert "entangler" in lib.qvdg_last_error().decode()
     assert lib.qvdg_batch_create(arr, 0, None, ct.byref(h)) == 1
     assert lib.qvdg_batch_destroy(None) == 0
+
+
+def test_one_pass_gate_packing_equals_packing_the_ops():
+    """run() packs a circuit's gate instructions for the C ABI in one pass;
+    the arrays equal those of packing gate_op's ops (same counts, qubits,
+    control values, matrices and layout)."""
+    import numpy as np
+
+    from qevedo_simulator_b200 import library
+    from qevedo_simulator_b200._abi import PackedOps
+    from qevedo_simulator_b200.circuit import gate_op, packed_gate_ops
+
+    for c in (library.random_grid_circuit(3, 4, 6, 3), library.qft(9), library.random_gate_circuit(8, 200, 5),
+              library.ghz(5)):
+        ins = c._instructions
+        a = PackedOps([gate_op(i[1], i[2]) for i in ins if i[0] == "gate"])
+        b = packed_gate_ops(ins)
+        assert a.count == b.count
+        for x, y in ((a._q, b._q), (a._v, b._v), (a._m, b._m)):
+            assert np.array_equal(x, y)
+        for f, base in (("targets", "_q"), ("controls", "_q"), ("control_values", "_v"), ("matrix", "_m")):
+            assert np.array_equal(a._ops[f] - np.uint64(getattr(a, base).ctypes.data),
+                                  b._ops[f] - np.uint64(getattr(b, base).ctypes.data)), f
+        for f in ("num_targets", "num_controls"):
+            assert np.array_equal(a._ops[f], b._ops[f]), f
