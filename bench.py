@@ -167,6 +167,34 @@ def cpu_baseline(ops_all, n: int, layers_ops, budget_s: float = 25.0) -> dict:
             "alloc_s": alloc, "engine": "C++ restatement of the reference's AVX2 engine (fusion 4, region_bits 14)"}
 
 
+def device_physical(st) -> np.ndarray:
+    """The device state as it lies in HBM (physical order, its precision)."""
+    from cuda.bindings import runtime as rt
+
+    st.synchronize()
+    ptr, nbytes = st.device_buffer()
+    out = np.empty(1 << st.num_qubits, dtype=np.complex64 if st.precision_bits == 32 else np.complex128)
+    (err,) = rt.cudaMemcpy(out.ctypes.data, ptr, out.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    if err != rt.cudaError_t.cudaSuccess:
+        raise RuntimeError(f"cudaMemcpy failed: {err}")
+    return out
+
+
+def oracle_f64_error(ops, n: int, st) -> float:
+    """max |delta amplitude| of the device state `st` (after `ops` from
+    |0...0>) against the oracle's f64 engine run on the host cores."""
+    from oracle import oracle
+
+    phys = device_physical(st)
+    layout = st.layout()
+    ref = oracle.OracleState(n, 64)
+    try:
+        ref.apply_ops(ops, max_fused=4, region_bits=14)
+        return ref.max_diff_physical(phys, layout)
+    finally:
+        ref.close()
+
+
 def host_cpu_model() -> str:
     try:
         with open("/proc/cpuinfo") as f:
@@ -363,16 +391,13 @@ def run_ours(args, rank: int, world: int):
                 "peak_source": peaks["source"], "bytes_per_launch": per_launch, "avg_launch_s": avg,
                 "traffic_source": "ncu capture of the same kernel at 26 qubits, scaled by amplitudes"
                 if args.traffic is None and dom != 1 else ("--traffic" if args.traffic else None),
-                "launches_per_step": int(dsec.size // max(1, args.steps)),
-                "whole_run_gbs": info["bytes"] / step / 1e9}
-    # Accuracy: tuned complex64 against a complex128 run of the same circuit.
-    err = None
-    if not args.skip_check:
-        st.zero()
-        st.execute(tuned)
-        with DeviceState(n, 64) as ref:
-            ref.apply_ops(ops, options(4, staged=False))
-            err = ref.max_abs_diff(st)
+                "launches_per_step": int(dsec.size // max(1, args.steps))}
+    # Whole run: the bytes every pass of a step moved (zero-start passes at
+    # the share of the state they touch), over the step time.
+    run_bytes = float(np.mean([b.sum() for b in pass_b]))
+    roofline["whole_run_gbs"] = run_bytes / step / 1e9
+    roofline["whole_run_bytes"] = run_bytes
+    roofline["whole_run_zero_start_bytes"] = float(np.mean([b[k == 4].sum() for b, k in zip(pass_b, pass_k)]))
     # End to end through the public API: plan on the host, upload gate data
     # from pinned memory, run, sample SHOTS shots, outcomes back to the host.
     e2e = []
@@ -388,10 +413,15 @@ def run_ours(args, rank: int, world: int):
     e2e_s = max_over_ranks(float(np.mean(e2e)), dist)
     h2d = tuned_upload_bytes(ops) + 8 * SHOTS
     d2h = 8 * SHOTS + 16
-    cpu = None
+    cpu, err = None, None
     if rank == 0 and world == 1 and not args.skip_cpu:
         cpu = cpu_baseline(ops, n, layer_prefix_ops(circuit, n), budget_s=args.cpu_budget)
         cpu["cpu"] = host_cpu_model()
+        if not args.skip_check:
+            # The tuned state against the oracle's f64 engine on the host.
+            st.zero()
+            st.execute(tuned)
+            err = oracle_f64_error(ops, n, st)
     if rank == 0:
         line = {
             "metric": METRIC, "value": step, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -415,7 +445,7 @@ def run_ours(args, rank: int, world: int):
                                      "bytes": float(np.sum(pass_b[-1][pass_k[-1] == 4]))}},
             "plain": {"s": plain_s, "passes": plain_info["passes"], "kernels": plain_info["kernels"]},
             "tuned_over_plain": step / plain_s,
-            "max_amp_err_vs_c128": err,
+            "max_amp_err_vs_oracle_f64": err,
             "gates": info["gates"],
             "wall_s_timed_region": wall,
         }
@@ -505,10 +535,15 @@ def run_precision(args):
 
     out = {"metric": "precision form: seconds, 1M-shot sampling seconds, error vs FP64", "unit": "s",
            "higher_is_better": False, "runs": {}}
-    # Error at 28 qubits (4x7 grid).
+    # Error at 28 qubits (4x7 grid) against the oracle's f64 engine on the
+    # host cores (the reference's fast engine restated, pinned to its naive
+    # simulator).
+    from oracle import oracle
+
     c28 = library.random_grid_circuit(4, 7, DEPTH, SEED)
-    with DeviceState(28, 64) as ref:
-        ref.apply_ops(c28.ops(), options(4, staged=False))
+    ref = oracle.OracleState(28, 64)
+    try:
+        ref.apply_ops(c28.ops(), max_fused=4, region_bits=14)
         errs = {}
         for name, opts in [("plain-tensor-f6", options(6, False, math="tensor")),
                            ("plain-tensor-f5", options(5, False, math="tensor")),
@@ -516,8 +551,10 @@ def run_precision(args):
                            math="tensor")), ("fp32-staged", options(4, True)), ("fp32-plain", options(4, False))]:
             with DeviceState(28, 32) as st:
                 st.apply_ops(c28.ops(), opts)
-                errs[name] = ref.max_abs_diff(st)
-        out["max_amp_err_vs_fp64_28q"] = errs
+                errs[name] = ref.max_diff_physical(device_physical(st), st.layout())
+        out["max_amp_err_vs_oracle_f64_28q"] = errs
+    finally:
+        ref.close()
     rng = np.random.Generator(np.random.PCG64(SEED))
     u = rng.random(1_000_000)
     for label, circuit, bits, plans in [

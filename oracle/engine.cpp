@@ -1204,6 +1204,120 @@ int oracle_sv_layout(void* p, uint32_t* layout) {
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// layout[logical] = physical as a permutation check.
+std::vector<size_t> checked_layout(const uint32_t* layout, size_t n) {
+  std::vector<size_t> v(layout, layout + n);
+  size_t seen = 0;
+  for (size_t q : v) {
+    if (q >= n || (seen >> q & 1)) throw std::runtime_error("layout is not a permutation of the qubits");
+    seen |= size_t(1) << q;
+  }
+  return v;
+}
+
+// Logical -> physical index through a layout, as the OR of per-16-bit-slice
+// tables (a bit permutation maps disjoint bit sets to disjoint bit sets).
+struct IndexMap {
+  std::vector<std::vector<size_t>> tables;
+  explicit IndexMap(const std::vector<size_t>& layout) {
+    const size_t n = layout.size();
+    for (size_t lo = 0; lo < std::max<size_t>(n, 1); lo += 16) {
+      const size_t w = std::min<size_t>(16, n - lo);
+      std::vector<size_t> t(size_t(1) << w, 0);
+      for (size_t v = 0; v < t.size(); ++v)
+        for (size_t b = 0; b < w; ++b) t[v] |= ((v >> b) & 1) << layout[lo + b];
+      tables.push_back(std::move(t));
+    }
+  }
+  size_t operator()(size_t index) const {
+    size_t p = 0;
+    for (size_t s = 0; s < tables.size(); ++s) p |= tables[s][(index >> (16 * s)) & (tables[s].size() - 1)];
+    return p;
+  }
+};
+
+// Interleaved (re, im) value at physical position i of a buffer of either precision.
+inline void read_pair(const void* amps, int bits, size_t i, double& re, double& im) {
+  if (bits == 32) {
+    const float* f = static_cast<const float*>(amps);
+    re = double(f[2 * i]);
+    im = double(f[2 * i + 1]);
+  } else {
+    const double* d = static_cast<const double*>(amps);
+    re = d[2 * i];
+    im = d[2 * i + 1];
+  }
+}
+
+template <class T>
+void set_physical(StateVector<T>& s, const void* amps, int bits) {
+  s.buffer[0] = T(0);
+  const long count = long(s.size());
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < count; ++i) {
+    size_t re, im;
+    double a, b;
+    read_pair(amps, bits, size_t(i), a, b);
+    StateVector<T>::offsets(size_t(i), re, im);
+    s.buffer[re] = T(a);
+    s.buffer[im] = T(b);
+  }
+}
+
+template <class T>
+double max_diff_physical(const StateVector<T>& s, const void* amps, int bits, const std::vector<size_t>& layout) {
+  const IndexMap mine(s.layout), theirs(layout);
+  const long count = long(s.size());
+  double worst = 0.0;
+#pragma omp parallel for schedule(static) reduction(max : worst)
+  for (long i = 0; i < count; ++i) {
+    size_t re, im;
+    StateVector<T>::offsets(mine(size_t(i)), re, im);
+    double a, b;
+    read_pair(amps, bits, theirs(size_t(i)), a, b);
+    const double dr = double(s.buffer[re]) - a, di = double(s.buffer[im]) - b;
+    worst = std::max(worst, std::sqrt(dr * dr + di * di));
+  }
+  return worst;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Sets the layout (layout[logical] = physical) without moving amplitudes;
+// with oracle_sv_set_physical it loads another engine's state as it lies in
+// memory, so that chunk order (the sampler's summation order) is the same.
+int oracle_sv_set_layout(void* p, const uint32_t* layout) {
+  Handle* h = static_cast<Handle*>(p);
+  return guarded([&] { DISPATCH(h, s.layout = checked_layout(layout, s.num_qubits)); });
+}
+
+// Loads 2^n interleaved complex amplitudes in PHYSICAL order, given in
+// `precision_bits` (32: float pairs, 64: double pairs).
+int oracle_sv_set_physical(void* p, const void* amplitudes, int precision_bits) {
+  Handle* h = static_cast<Handle*>(p);
+  return guarded([&] {
+    if (precision_bits != 32 && precision_bits != 64) throw std::runtime_error("precision must be 32 or 64");
+    DISPATCH(h, set_physical(s, amplitudes, precision_bits));
+  });
+}
+
+// max over logical indices of |this state's amplitude - the other's|, the
+// other given as physical-order interleaved amplitudes with its own layout.
+int oracle_sv_max_diff_physical(void* p, const void* amplitudes, int precision_bits, const uint32_t* layout,
+                                double* out) {
+  Handle* h = static_cast<Handle*>(p);
+  return guarded([&] {
+    if (precision_bits != 32 && precision_bits != 64) throw std::runtime_error("precision must be 32 or 64");
+    DISPATCH(h, *out = max_diff_physical(s, amplitudes, precision_bits, checked_layout(layout, s.num_qubits)));
+  });
+}
+
 // Greedy fusion alone (fusion.rs:63-115): writes the number of fused ops and,
 // per fused op, its number of targets and controls.
 int oracle_fuse_shapes(const qvdg_op* ops, size_t num_ops, uint32_t max_fused, size_t* num_fused, uint32_t* widths,

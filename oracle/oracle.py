@@ -58,6 +58,10 @@ def lib():
         L.oracle_naive_apply_op.argtypes = [ct.POINTER(ct.c_double), ct.c_uint32, ct.POINTER(QvdgOp)]
         L.oracle_fuse_shapes.argtypes = [ct.POINTER(QvdgOp), ct.c_size_t, ct.c_uint32, ct.POINTER(ct.c_size_t),
                                          ct.POINTER(ct.c_uint32), ct.c_size_t]
+        L.oracle_sv_set_layout.argtypes = [ct.c_void_p, ct.POINTER(ct.c_uint32)]
+        L.oracle_sv_set_physical.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int]
+        L.oracle_sv_max_diff_physical.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int, ct.POINTER(ct.c_uint32),
+                                                  ct.POINTER(ct.c_double)]
         L.oracle_set_threads.argtypes = [ct.c_int]
         L.oracle_max_threads.restype = ct.c_int
         _lib = L
@@ -181,6 +185,55 @@ class OracleState:
         out = (ct.c_uint32 * max(self.num_qubits, 1))()
         _check(lib().oracle_sv_layout(self._h, out))
         return list(out)[: self.num_qubits]
+
+    def set_layout(self, layout):
+        """layout[logical] = physical, without moving amplitudes."""
+        arr = (ct.c_uint32 * max(self.num_qubits, 1))(*[int(q) for q in layout])
+        _check(lib().oracle_sv_set_layout(self._h, arr))
+
+    def set_physical(self, physical: np.ndarray):
+        """Load interleaved amplitudes in physical order (complex64 or
+        complex128), as another engine holds them in memory."""
+        a = _physical_array(physical, self.num_qubits)
+        _check(lib().oracle_sv_set_physical(self._h, a.ctypes.data_as(ct.c_void_p), _bits_of(a)))
+
+    def max_diff_physical(self, physical: np.ndarray, layout) -> float:
+        """max |this amplitude - the other's| over logical indices, the other
+        state given in physical order with its layout."""
+        a = _physical_array(physical, self.num_qubits)
+        arr = (ct.c_uint32 * max(self.num_qubits, 1))(*[int(q) for q in layout])
+        v = ct.c_double()
+        _check(lib().oracle_sv_max_diff_physical(self._h, a.ctypes.data_as(ct.c_void_p), _bits_of(a), arr,
+                                                 ct.byref(v)))
+        return v.value
+
+
+def _bits_of(a: np.ndarray) -> int:
+    return 32 if a.dtype == np.complex64 else 64
+
+
+def _physical_array(physical: np.ndarray, num_qubits: int) -> np.ndarray:
+    a = np.ascontiguousarray(physical)
+    if a.dtype not in (np.complex64, np.complex128):
+        raise TypeError("expected complex64 or complex128 amplitudes")
+    if a.size != 1 << num_qubits:
+        raise ValueError(f"expected {1 << num_qubits} amplitudes")
+    return a
+
+
+def sample_physical(physical: np.ndarray, layout, uniforms: np.ndarray) -> np.ndarray:
+    """The reference sampler on a state given as it lies in another engine's
+    memory: physical-order amplitudes (complex64 -> a 32-bit state,
+    complex128 -> 64-bit) with layout[logical] = physical, so chunks are
+    summed in the same physical order; outcomes are logical indices."""
+    n = int(physical.size).bit_length() - 1
+    st = OracleState(n, _bits_of(np.asarray(physical)))
+    try:
+        st.set_layout(layout)
+        st.set_physical(physical)
+        return st.sample_unordered(uniforms)
+    finally:
+        st.close()
 
 
 def sample_from_amplitudes(amplitudes: np.ndarray, uniforms: np.ndarray, precision_bits: int) -> np.ndarray:

@@ -60,3 +60,19 @@ def oracle():
 
     o.lib()
     return o
+
+
+def device_physical(st) -> np.ndarray:
+    """A device state's amplitudes as they lie in HBM: physical index order,
+    in the state's own precision (complex64 or complex128), copied with the
+    CUDA runtime after the library's stream has drained."""
+    from cuda.bindings import runtime as rt
+
+    st.synchronize()
+    ptr, nbytes = st.device_buffer()
+    dtype = np.complex64 if st.precision_bits == 32 else np.complex128
+    out = np.empty(1 << st.num_qubits, dtype=dtype)
+    assert nbytes >= out.nbytes
+    (err,) = rt.cudaMemcpy(out.ctypes.data, ptr, out.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    assert err == rt.cudaError_t.cudaSuccess, err
+    return out

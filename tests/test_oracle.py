@@ -218,3 +218,43 @@ def test_measure_collapse(oracle):
     assert st.measure(0, 0.9) == 0  # P(1) = 0.5 <= 0.9 -> outcome 0
     a = st.amplitudes()
     assert abs(a[0] - 1) < 1e-12 and max_distance(a[1:], np.zeros(3)) < 1e-12
+
+
+def test_physical_loads_layouts_and_streamed_differences(oracle):
+    """The oracle reads another engine's state as it lies in memory:
+    physical-order amplitudes with a layout give the same logical state, the
+    same samples as the swapped state, and the streamed max difference
+    equals the logical one; bad layouts are rejected."""
+    rng = np.random.Generator(np.random.PCG64(77))
+    n = 14
+    amps = random_state(rng, n)
+    layout = [int(x) for x in rng.permutation(n)]
+    idx = np.arange(1 << n)
+    phys_index = np.zeros(1 << n, dtype=np.int64)
+    for q in range(n):
+        phys_index |= ((idx >> q) & 1) << layout[q]
+    phys = np.empty_like(amps)
+    phys[phys_index] = amps
+    for bits in (32, 64):
+        st = oracle.OracleState(n, bits)
+        st.set_layout(layout)
+        st.set_physical(phys.astype(np.complex64) if bits == 32 else phys)
+        assert st.layout() == layout
+        got = st.amplitudes()
+        assert max_distance(got, amps) < (1e-7 if bits == 32 else 1e-15)
+        given = phys.astype(np.complex64) if bits == 32 else phys
+        other = amps + 1e-3 * random_state(rng, n)
+        ref = oracle.OracleState(n, 64)
+        ref.set_amplitudes(other)
+        expected = float(np.max(np.abs(other - given[phys_index].astype(np.complex128))))
+        assert abs(ref.max_diff_physical(given, layout) - expected) < 1e-15
+        ref.close()
+        u = rng.random(5000)
+        assert np.array_equal(oracle.sample_physical(given, layout, u), st.sample_unordered(u))
+        st.close()
+    bad = oracle.OracleState(4, 64)
+    with pytest.raises(RuntimeError, match="permutation"):
+        bad.set_layout([0, 1, 1, 3])
+    with pytest.raises(ValueError):
+        bad.set_physical(np.zeros(8, dtype=np.complex128))
+    bad.close()
