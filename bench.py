@@ -278,27 +278,16 @@ def max_over_ranks(value: float, dist, device: str = "cuda") -> float:
 
 
 def choose_tuned(ops, n: int, st, fixed=None):
-    """The tuned plan: the learned cost model's pick among the candidate plans
-    (plain per-gate passes at fusion 2-6 on the CUDA or the tensor cores,
-    staged CUDA-core, staged tensor-core),
-    judged by measurement against the greedy default. Returns (name, options,
-    {candidate: measured seconds}) -- every candidate is measured once so the
-    line shows what the choice was between."""
-    from qevedo_simulator_b200 import costmodel, options
+    """The tuned plan: the library's measured judge (costmodel.tune_settings)
+    over the learned cost model's three best-ranked candidates and the
+    greedy default, with every candidate measured once so the line shows
+    what the choice was between. Returns (name, options, {candidate:
+    measured seconds})."""
+    from qevedo_simulator_b200 import costmodel
 
     if fixed is not None:
         return fixed[0], fixed[1], {}
-    model = costmodel.CostModel.load()
-    ranked = model.rank(ops, n)
-    measured = {}
-    for nm, o in costmodel.candidates():
-        measured[nm] = costmodel.measure_plan(ops, n, o, st, repeats=1)[0]
-    # The model's three picks and the greedy default, judged by measurement.
-    name, opts = "staged-cuda", costmodel.default_options()
-    for nm, o, _ in ranked[:3]:
-        if measured[nm] < measured[name]:
-            name, opts = nm, o
-    return name, opts, measured
+    return costmodel.tune_settings(ops, n, st, every_candidate=True)
 
 
 def run_ours(args, rank: int, world: int):
@@ -398,18 +387,20 @@ def run_ours(args, rank: int, world: int):
     roofline["whole_run_gbs"] = run_bytes / step / 1e9
     roofline["whole_run_bytes"] = run_bytes
     roofline["whole_run_zero_start_bytes"] = float(np.mean([b[k == 4].sum() for b, k in zip(pass_b, pass_k)]))
-    # End to end through the public API: plan on the host, upload gate data
+    # End to end through the public API with its default settings (the
+    # learned planner picks the plan): plan on the host, upload gate data
     # from pinned memory, run, sample SHOTS shots, outcomes back to the host.
     e2e = []
     st.set_pass_timing(False)  # the user's path records no per-pass events
     staged = bool(tuned_opts.staged)
     math_name = {0: "fp32", 1: "tensor", 2: "gates"}[int(tuned_opts.math)]
+    e2e_settings = None
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        run(circuit.copy().measure_all(), SHOTS, seed=7 + i, max_fused_qubits=int(tuned_opts.max_fused_qubits),
-            staged=staged, math=math_name, state=st)
+        res = run(circuit.copy().measure_all(), SHOTS, seed=7 + i, state=st)
         if i >= args.warmup:
             e2e.append(time.perf_counter() - t0)
+        e2e_settings = res.stats.get("settings")
     e2e_s = max_over_ranks(float(np.mean(e2e)), dist)
     h2d = tuned_upload_bytes(ops) + 8 * SHOTS
     d2h = 8 * SHOTS + 16
@@ -431,7 +422,8 @@ def run_ours(args, rank: int, world: int):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "call": f"qevedo_simulator_b200.run(circuit, shots={SHOTS}) on a reused device state"},
+                    "call": f"qevedo_simulator_b200.run(circuit, shots={SHOTS}) on a reused device state, default "
+                            "settings (learned planner)", "plan": e2e_settings},
             "gpu_launches": int(info["passes"]) * args.steps,
             "clocks": clocks.summary(),
             "tuned": {"s": step, "plan": tuned_name, "passes": info["passes"], "stages": info["stages"],

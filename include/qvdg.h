@@ -86,7 +86,12 @@ typedef struct {
    * Small values force many stages on small states (as region_bits 1..4 do in
    * the reference's tests, tests/simulator.rs:256-285). */
   uint32_t tile_qubits;
-  /* QVDG_PLANNER_GREEDY or QVDG_PLANNER_LEARNED. */
+  /* QVDG_PLANNER_GREEDY: plan with the settings given here.
+   * QVDG_PLANNER_LEARNED: build every candidate setting
+   * (qvdg_planner_candidates) and run the one the registered cost model
+   * (qvdg_cost_model_set) predicts fastest; max_fused_qubits, staged,
+   * tile_qubits and math are then only the fallback, used for complex128
+   * states or when no model is registered for the current device. */
   uint32_t planner;
   /* QVDG_MATH_FP32: every gate on the CUDA cores. QVDG_MATH_TENSOR
    * (complex64 only): fused dense gates of 3-6 qubits in staged tiles, or of
@@ -106,6 +111,8 @@ typedef struct {
   uint64_t stages;      /* staged passes */
   double gate_seconds;  /* device time of the gate work (CUDA events) */
   double bytes;         /* algorithmic HBM bytes of the gate work */
+  qvdg_options settings; /* the settings the run's plan was built with (planner = GREEDY: the learned pick
+                          * or the caller's own) */
 } qvdg_stats;
 
 typedef struct qvdg_state qvdg_state;
@@ -293,6 +300,31 @@ qvdg_status qvdg_plan_fused_ops(uint32_t num_qubits, uint32_t precision_bits, co
                                 size_t capacity, size_t* num_fused, size_t* num_qubit_entries,
                                 size_t* num_matrix_doubles);
 
+/* Registers the cost model for the current device, replacing any earlier
+ * one: an MLP of the qvdg_mlp form below with `inputs` = QVDG_PASS_FEATURES
+ * and `hidden` units per hidden layer, given its `count` parameters, that
+ * predicts log(seconds per 2^24 amplitudes) of a pass from its features.
+ * QVDG_PLANNER_LEARNED then ranks candidate plans with it. */
+qvdg_status qvdg_cost_model_set(const float* params, size_t count, uint32_t inputs, uint32_t hidden);
+/* Forgets the current device's cost model (QVDG_PLANNER_LEARNED then falls
+ * back to the given settings). */
+qvdg_status qvdg_cost_model_clear(void);
+
+/* The candidate settings of the learned planner for a precision, in the
+ * order qvdg_plan_choose reports them: `*count` receives their number and
+ * `out` at most `capacity` of them. */
+qvdg_status qvdg_planner_candidates(uint32_t precision_bits, qvdg_options* out, size_t capacity, size_t* count);
+
+/* The learned planner's choice for `ops` on a state of `num_qubits` (host
+ * planning, then one forward of the cost model on the current device): the
+ * chosen settings, and every candidate's predicted seconds (at most
+ * `capacity`, in qvdg_planner_candidates order). from_zero != 0 scores runs
+ * that start from |0...0> (zero-start passes at the share of the state they
+ * move). Fails with QVDG_ERR_INVALID when no model is registered. */
+qvdg_status qvdg_plan_choose(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                             int32_t from_zero, qvdg_options* chosen, double* predicted, size_t capacity,
+                             size_t* num_candidates);
+
 /* An MLP with two hidden ReLU layers of `hidden` units and one linear
  * output, trained and evaluated by this library's own CUDA kernels (fp32,
  * on the current device). Parameters, in order: W1 (hidden x inputs), b1,
@@ -393,6 +425,8 @@ qvdg_status qvdg_pass_times(const qvdg_state* state, double* seconds, double* by
 /* Make `device` the current CUDA device of the calling thread for this
  * library (states and plans are created on the current device). */
 qvdg_status qvdg_set_device(int32_t device);
+/* The calling thread's current CUDA device. */
+qvdg_status qvdg_get_device(int32_t* device);
 
 /* max_i |a_i - b_i| over all logical amplitudes of two states of the same
  * size (any precisions, any layouts), accumulated in double precision on the
@@ -422,7 +456,10 @@ qvdg_status qvdg_max_abs_diff(const qvdg_state* a, const qvdg_state* b, double* 
  *
  * At most 35 qubits; larger states are refused (QVDG_ERR_UNSUPPORTED).
  * The first call on a device looks up the scratch array's address on that
- * device; make that first call before any stream capture. All calls share
+ * device; make that first call before any stream capture. The address is
+ * kept for the life of the process: a caller that resets a device
+ * (cudaDeviceReset) must not call this entry point on it afterwards, as the
+ * kept address would then be stale. All calls share
  * the one array, so calls that overlap on the GPU (from several threads or
  * streams) race: order them, e.g. on one stream. */
 qvdg_status qvdg_bit_probabilities_noalloc(const void* amplitudes, uint32_t num_qubits, uint32_t precision_bits,

@@ -37,10 +37,22 @@ class QvdgStats(ct.Structure):
         ("stages", ct.c_uint64),
         ("gate_seconds", ct.c_double),
         ("bytes", ct.c_double),
+        ("settings", QvdgOptions),
     ]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        out = {name: getattr(self, name) for name, _ in self._fields_ if name != "settings"}
+        out["settings"] = settings_dict(self.settings)
+        return out
+
+
+MATH_NAMES = {0: "fp32", 1: "tensor", 2: "gates"}
+
+
+def settings_dict(o: QvdgOptions) -> dict:
+    """Plan settings as plain values (math by name)."""
+    return {"max_fused_qubits": int(o.max_fused_qubits), "staged": bool(o.staged), "tile_qubits": int(o.tile_qubits),
+            "math": MATH_NAMES.get(int(o.math), str(int(o.math)))}
 
 
 class QvdgLayeredCircuit(ct.Structure):

@@ -54,6 +54,7 @@ _SIGNATURES = {
     "qvdg_plan_info": (ct.c_int, [_P, ct.POINTER(QvdgStats)]),
     "qvdg_plan_execute": (ct.c_int, [_P, _P, ct.POINTER(QvdgStats)]),
     "qvdg_set_device": (ct.c_int, [ct.c_int32]),
+    "qvdg_get_device": (ct.c_int, [ct.POINTER(ct.c_int32)]),
     "qvdg_max_abs_diff": (ct.c_int, [_P, _P, ct.POINTER(ct.c_double)]),
     "qvdg_set_pass_timing": (ct.c_int, [_P, ct.c_int32]),
     "qvdg_pass_times": (ct.c_int, [_P, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), ct.POINTER(ct.c_int32),
@@ -90,6 +91,13 @@ _SIGNATURES = {
                                   ct.c_uint32, ct.c_float, ct.c_uint64, ct.POINTER(ct.c_float)]),
     "qvdg_bit_probabilities_noalloc": (ct.c_int, [_P, ct.c_uint32, ct.c_uint32, _P, ct.POINTER(ct.c_double),
                                                   ct.POINTER(ct.c_double)]),
+    "qvdg_cost_model_set": (ct.c_int, [ct.POINTER(ct.c_float), ct.c_size_t, ct.c_uint32, ct.c_uint32]),
+    "qvdg_cost_model_clear": (ct.c_int, []),
+    "qvdg_planner_candidates": (ct.c_int, [ct.c_uint32, ct.POINTER(QvdgOptions), ct.c_size_t,
+                                           ct.POINTER(ct.c_size_t)]),
+    "qvdg_plan_choose": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(QvdgOp), ct.c_size_t, ct.c_int32,
+                                    ct.POINTER(QvdgOptions), ct.POINTER(ct.c_double), ct.c_size_t,
+                                    ct.POINTER(ct.c_size_t)]),
 }
 
 _lib = None
@@ -144,9 +152,67 @@ def set_device(device: int):
 
 
 MATH = {"fp32": 0, "tensor": 1, "gates": 2}
+PLANNERS = {"greedy": 0, "learned": 1}
+COST_MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "cost_model.npz")
+_models_registered = set()
 
 
-def options(max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0, planner: int = 0,
+def register_cost_model(params, inputs: int, hidden: int):
+    """Register the learned planner's cost model (the MLP parameters) for the
+    current device, replacing any earlier one."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    check(lib().qvdg_cost_model_set(p.ctypes.data_as(ct.POINTER(ct.c_float)), p.size, int(inputs), int(hidden)))
+    _models_registered.add(_current_device())
+
+
+def ensure_cost_model() -> bool:
+    """Register the committed cost model (data/cost_model.npz) for the current
+    device once; False when the file is absent (the learned planner then
+    uses its fallback settings)."""
+    dev = _current_device()
+    if dev in _models_registered:
+        return True
+    if not os.path.exists(COST_MODEL_PATH):
+        return False
+    d = np.load(COST_MODEL_PATH)
+    register_cost_model(d["params"], int(d["inputs"]), int(d["hidden"]))
+    return True
+
+
+def clear_cost_model():
+    check(lib().qvdg_cost_model_clear())
+    _models_registered.discard(_current_device())
+
+
+def _current_device() -> int:
+    d = ct.c_int32()
+    check(lib().qvdg_get_device(ct.byref(d)))
+    return int(d.value)
+
+
+def planner_candidates(precision_bits: int = 32) -> list:
+    """The learned planner's candidate settings, in its reporting order."""
+    n = ct.c_size_t()
+    check(lib().qvdg_planner_candidates(int(precision_bits), None, 0, ct.byref(n)))
+    arr = (QvdgOptions * max(n.value, 1))()
+    check(lib().qvdg_planner_candidates(int(precision_bits), arr, n.value, ct.byref(n)))
+    return [arr[i] for i in range(n.value)]
+
+
+def plan_choose(ops, num_qubits: int, from_zero: bool = True):
+    """(chosen options, [predicted seconds per candidate]) of the learned
+    planner for `ops` on a complex64 state (needs a registered model)."""
+    packed = PackedOps(ops)
+    chosen = QvdgOptions()
+    cands = planner_candidates(32)
+    pred = np.zeros(max(len(cands), 1), dtype=np.float64)
+    n = ct.c_size_t()
+    check(lib().qvdg_plan_choose(int(num_qubits), 32, packed.array, packed.count, 1 if from_zero else 0,
+                                 ct.byref(chosen), as_double_ptr(pred), pred.size, ct.byref(n)))
+    return chosen, pred[:n.value]
+
+
+def options(max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0, planner: int | str = 0,
             math: str = "fp32") -> QvdgOptions:
     """Simulator options (the reference's Options, src/simulator.rs:37-66).
     `math="tensor"` runs fused dense gates on the tensor cores (complex64
@@ -157,7 +223,7 @@ def options(max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0
     o.max_fused_qubits = int(max_fused_qubits)
     o.staged = 1 if staged else 0
     o.tile_qubits = int(tile_qubits)
-    o.planner = int(planner)
+    o.planner = PLANNERS[planner] if isinstance(planner, str) else int(planner)
     o.math = MATH[math]
     return o
 

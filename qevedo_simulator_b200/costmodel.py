@@ -264,6 +264,31 @@ def choose_measured(model: CostModel, ops, num_qubits: int, state: DeviceState, 
     return best[0], best[1], best[2], t_default
 
 
+def tune_settings(ops, num_qubits: int, state: DeviceState, model: CostModel | None = None, top: int = 3,
+                  every_candidate: bool = False):
+    """The measured judge for a plan that will run many times: the model's
+    `top` ranked candidates and the greedy default (the reference's
+    defaults) are each run once from |0...0> on `state`, and the fastest
+    wins. With `every_candidate`, all candidates are measured too, so a
+    caller can see what the choice was between (the judge still picks only
+    among the model's top and the default). Returns (name, options,
+    {candidate name: measured seconds})."""
+    model = model or CostModel.load()
+    cands = dict(candidates())
+    judged = [r[0] for r in model.rank(ops, num_qubits)[:top]] + ["staged-cuda"]
+    measured = {}
+    for name in (list(cands) if every_candidate else list(dict.fromkeys(judged))):
+        measured[name] = measure_plan(ops, num_qubits, cands[name], state, repeats=1)[0]
+    best = min(dict.fromkeys(judged), key=lambda nm: measured[nm])
+    return best, cands[best], measured
+
+
+def tuned_plan(ops, num_qubits: int, state: DeviceState, model: CostModel | None = None, top: int = 3):
+    """(Plan, name, measured seconds) of the judged pick (tune_settings)."""
+    name, opts, measured = tune_settings(ops, num_qubits, state, model, top)
+    return Plan(ops, num_qubits, state.precision_bits, opts), name, measured
+
+
 def _spec(seed: int, qubits, depth):
     rng = np.random.Generator(np.random.PCG64(seed))
     return int(rng.choice(qubits)), int(rng.integers(depth[0], depth[1] + 1))

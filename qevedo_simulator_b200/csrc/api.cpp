@@ -15,6 +15,7 @@
 #include "batch.hpp"
 #include "engine.hpp"
 #include "host.hpp"
+#include "planner.hpp"
 #include "qvdg.h"
 #include "program.hpp"
 #include "stage.hpp"
@@ -35,6 +36,7 @@ struct qvdg_plan {
   std::unique_ptr<qvdg::Program> general;
   qvdg::DeviceUpload general_dev;
   void* general_device = nullptr;
+  qvdg_options settings{};  // what the plan was built with (the learned pick, or the given settings)
 };
 
 namespace qvdg {
@@ -200,10 +202,12 @@ void upload_plan(const Program& p, uint32_t precision_bits, void** device, Devic
 // src/simulator.rs:122-147).
 void apply_program(StateImpl& s, const std::vector<HOp>& ops, const qvdg_options& opt, qvdg_stats* stats) {
   // One-shot: narrow beam searches where a pass streams at least 8 GB.
-  const Program prog = build_program(target_of(s), ops, opt,
-                                     s.n >= 29 ? FusionSearch::Beam : FusionSearch::Lookahead, s.zero_state);
+  qvdg_options chosen;
+  const Program prog = choose_program(target_of(s), ops, opt, s.n >= 29 ? FusionSearch::Beam : FusionSearch::Lookahead,
+                                      s.zero_state, &chosen);
   const DeviceUpload dev = upload_program(s, prog, s.work);
   run_program(s, prog, dev, stats);
+  if (stats) stats->settings = chosen;
 }
 
 // One op as a single plain pass (StateVector::apply, src/state.rs:181-198).
@@ -525,7 +529,8 @@ qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const
     plan->device_id = dev;
     try {
       const std::vector<HOp> hops = lower_ops(ops, num_ops, num_qubits);
-      plan->program = build_program(t, hops, opt, FusionSearch::Thorough, true);
+      plan->program = choose_program(t, hops, opt, FusionSearch::Thorough, true, &plan->settings);
+      opt = plan->settings;
       plan->program.gates = num_ops;
       upload_plan(plan->program, precision_bits, &plan->device, &plan->dev);
       // Tensor-core plain plans pick their fusion by the cost from |0...0>;
@@ -564,6 +569,7 @@ qvdg_status qvdg_plan_info(const qvdg_plan* plan, qvdg_stats* stats) {
     stats->stages = p.stages;
     stats->gate_seconds = 0.0;
     stats->bytes = p.bytes;
+    stats->settings = plan->settings;
   });
 }
 
@@ -580,6 +586,7 @@ qvdg_status qvdg_plan_execute(qvdg_state* st, const qvdg_plan* plan, qvdg_stats*
       run_program(s, *plan->general, plan->general_dev, stats);
     else
       run_program(s, plan->program, plan->dev, stats);
+    if (stats) stats->settings = plan->settings;
   });
 }
 
@@ -603,6 +610,15 @@ qvdg_status qvdg_pass_times(const qvdg_state* st, double* seconds, double* bytes
 
 qvdg_status qvdg_set_device(int32_t device) {
   return guarded([&] { QVDG_CUDA(cudaSetDevice(device)); });
+}
+
+qvdg_status qvdg_get_device(int32_t* device) {
+  return guarded([&] {
+    require(device != nullptr, "null output");
+    int d = 0;
+    QVDG_CUDA(cudaGetDevice(&d));
+    *device = d;
+  });
 }
 
 qvdg_status qvdg_max_abs_diff(const qvdg_state* a, const qvdg_state* b, double* out) {
@@ -688,6 +704,58 @@ qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, con
     const size_t rows = prog.passes.size();
     if (num_passes) *num_passes = rows;
     if (out) std::memcpy(out, prog.features.data(), std::min(rows, capacity) * kPassFeatures * sizeof(float));
+  });
+}
+
+qvdg_status qvdg_cost_model_set(const float* params, size_t count, uint32_t inputs, uint32_t hidden) {
+  return guarded([&] {
+    require(params != nullptr, "null parameters");
+    int dev = 0;
+    QVDG_CUDA(cudaGetDevice(&dev));
+    set_cost_model(dev, params, count, inputs, hidden);
+  });
+}
+
+qvdg_status qvdg_cost_model_clear(void) {
+  return guarded([&] {
+    int dev = 0;
+    QVDG_CUDA(cudaGetDevice(&dev));
+    clear_cost_model(dev);
+  });
+}
+
+qvdg_status qvdg_planner_candidates(uint32_t precision_bits, qvdg_options* out, size_t capacity, size_t* count) {
+  return guarded([&] {
+    require(precision_bits == 32 || precision_bits == 64, "precision must be 32 or 64 bits");
+    const std::vector<qvdg_options> c = learned_candidates(int(precision_bits));
+    if (count) *count = c.size();
+    for (size_t i = 0; out && i < c.size() && i < capacity; ++i) out[i] = c[i];
+  });
+}
+
+qvdg_status qvdg_plan_choose(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                             int32_t from_zero, qvdg_options* chosen, double* predicted, size_t capacity,
+                             size_t* num_candidates) {
+  return guarded([&] {
+    require(precision_bits == 32, "the cost model ranks complex64 plans only");
+    require(num_qubits >= 1 && num_qubits <= 40, "a state needs 1 to 40 qubits");
+    int dev = 0;
+    QVDG_CUDA(cudaGetDevice(&dev));
+    require(has_cost_model(dev), "no cost model is registered for this device");
+    Target t;
+    t.n = num_qubits;
+    t.bits = int(precision_bits);
+    QVDG_CUDA(cudaDeviceGetAttribute(&t.sms, cudaDevAttrMultiProcessorCount, dev));
+    for (uint32_t q = 0; q < num_qubits; ++q) t.layout.push_back(q);
+    qvdg_options opt;
+    qvdg_default_options(&opt);
+    opt.planner = QVDG_PLANNER_LEARNED;
+    qvdg_options pick;
+    std::vector<double> sec;
+    choose_program(t, lower_ops(ops, num_ops, num_qubits), opt, FusionSearch::Thorough, from_zero != 0, &pick, &sec);
+    if (chosen) *chosen = pick;
+    if (num_candidates) *num_candidates = sec.size();
+    for (size_t i = 0; predicted && i < sec.size() && i < capacity; ++i) predicted[i] = sec[i];
   });
 }
 

@@ -18,7 +18,7 @@ import numpy as np
 from . import _native
 from .circuit import Circuit, Gate, gate_op, packed_gate_ops
 
-BACKENDS = ("auto", "statevector")
+BACKENDS = ("auto", "statevector", "state_vector")
 
 
 @dataclass
@@ -114,33 +114,81 @@ def count_outcomes(outcomes: np.ndarray, measures, num_clbits: int) -> dict:
 
 def _as_circuit(circuit) -> Circuit:
     """A Circuit, or OpenQASM 2/3 text parsed into one (the reference's
-    `run` and `statevector` take either)."""
+    `run` and `statevector` take either; anything else is a TypeError, as
+    the reference's binding raises)."""
     if isinstance(circuit, str):
         from . import qasm
 
         return qasm.parse(circuit)
+    if not isinstance(circuit, Circuit):
+        raise TypeError(f"expected a Circuit or OpenQASM text, not {type(circuit).__name__}")
     return circuit
 
 
-def statevector(circuit: Circuit | str, *, precision: str = "double", max_fused_qubits: int = 4,
-                staged: bool = True, tile_qubits: int = 0, math: str = "fp32",
-                threads: int | str | None = None) -> np.ndarray:
+_THREAD_PLACEMENTS = ("pcores", "pthreads", "cores", "allcores", "all")
+
+
+def _check_threads(threads):
+    """The reference's thread setting (python/src/lib.rs:574-594): None, a
+    thread count (0 meaning 1), or a placement name; anything else is a
+    ValueError with the reference's message. Host planning here uses the
+    library's own thread pool, so a valid value changes nothing."""
+    if threads is None:
+        return
+    if isinstance(threads, int) and not isinstance(threads, bool) and threads >= 0:
+        return
+    if not isinstance(threads, str):
+        raise ValueError("threads must be a number or a placement name")
+    if threads not in _THREAD_PLACEMENTS:
+        raise ValueError(f"unknown thread placement `{threads}` (pcores, pthreads, cores, all)")
+
+
+def plan_options(max_fused_qubits: int | None = None, staged: bool | None = None, tile_qubits: int = 0,
+                 math: str | None = None, planner: str | None = None) -> _native.QvdgOptions:
+    """Planner settings for a run. With none of max_fused_qubits, staged and
+    math given, the learned planner picks among its candidate plans by the
+    committed cost model's predicted time (complex64 states; the reference's
+    defaults, fusion 4 with staged tiles, are its fallback and run for
+    complex128). Giving any of them plans greedily with those settings, as
+    the reference's Options do (src/simulator.rs:37-66)."""
+    if planner is None:
+        planner = "learned" if max_fused_qubits is None and staged is None and math is None else "greedy"
+    if planner not in _native.PLANNERS:
+        raise ValueError('planner must be "learned" or "greedy"')
+    return _native.options(4 if max_fused_qubits is None else max_fused_qubits, True if staged is None else staged,
+                           tile_qubits, planner=planner, math="fp32" if math is None else math)
+
+
+def _with_model(opts: _native.QvdgOptions) -> _native.QvdgOptions:
+    """Registers the committed cost model on the current device when the
+    learned planner will run (a device call, so not in plan_options)."""
+    if opts.planner == _native.PLANNERS["learned"]:
+        _native.ensure_cost_model()
+    return opts
+
+
+def statevector(circuit: Circuit | str, *, precision: str = "double", max_fused_qubits: int | None = None,
+                staged: bool | None = None, tile_qubits: int = 0, math: str | None = None,
+                planner: str | None = None, threads: int | str | None = None) -> np.ndarray:
     """The final state of a circuit without measurements, as complex128 in
     logical order (index bit q = qubit q). Double precision by default, as
-    the reference's `statevector` (python/src/lib.rs:686-718). `threads`
-    is accepted for the reference's signature; host planning uses the
-    library's own thread pool."""
+    the reference's `statevector` (python/src/lib.rs:686-718). Planner
+    settings as in `plan_options`. `threads` is checked as the reference
+    does; host planning uses the library's own thread pool."""
+    _check_threads(threads)
     circuit = _as_circuit(circuit)
     ops = circuit.ops()
+    opts = plan_options(max_fused_qubits, staged, tile_qubits, math, planner)
     with _native.DeviceState(circuit.num_qubits, _precision_bits(precision)) as st:
-        st.apply_ops(ops, _native.options(max_fused_qubits, staged, tile_qubits, math=math))
+        st.apply_ops(ops, _with_model(opts))
         return st.amplitudes()
 
 
 def run(circuit: Circuit | str, shots: int = 1024, *, backend: str = "auto", seed: int | None = None,
         precision: str = "single", max_bond_dimension: int = 256, truncation_threshold: float = 1e-16,
-        threads: int | str | None = None, max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0,
-        math: str = "fp32", state: _native.DeviceState | None = None) -> RunResult:
+        threads: int | str | None = None, max_fused_qubits: int | None = None, staged: bool | None = None,
+        tile_qubits: int = 0, math: str | None = None, planner: str | None = None,
+        state: _native.DeviceState | None = None) -> RunResult:
     """Sample `shots` shots of `circuit` (a Circuit or OpenQASM 2/3 text) on
     the device state vector.
 
@@ -152,14 +200,18 @@ def run(circuit: Circuit | str, shots: int = 1024, *, backend: str = "auto", see
     settings) and `threads` are accepted for the reference's signature
     (python/python/qevedo/simulator/__init__.py:96-106) and do not affect
     the state vector; host planning uses the library's own thread pool.
+    Planner settings as in `plan_options`: by default the learned planner
+    picks the plan; `result.stats["settings"]` says which.
     """
     _check_backend(backend)
+    _check_threads(threads)
     circuit = _as_circuit(circuit)
     bits = _precision_bits(precision)
     rng = np.random.Generator(np.random.PCG64(seed))
-    opts = _native.options(max_fused_qubits, staged, tile_qubits, math=math)
+    opts = plan_options(max_fused_qubits, staged, tile_qubits, math, planner)
     own = state is None
     st = state or _native.DeviceState(circuit.num_qubits, bits)
+    _with_model(opts)
     try:
         if not own:
             st.zero()

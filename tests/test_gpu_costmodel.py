@@ -96,3 +96,44 @@ def test_learned_planner_beats_the_greedy_default_on_held_out_circuits():
             picked += p
             default += dsec
     assert picked < default
+
+
+def test_learned_planner_on_the_product_path(oracle):
+    """The committed cost model, registered in the library: its choice
+    (qvdg_plan_choose, host planning and one forward of the device MLP over
+    every candidate's passes) equals the Python ranking of the same model;
+    a plan built with planner="learned" carries that choice; run() and
+    statevector() with default settings run the learned pick and match the
+    naive oracle; with the model cleared the fallback settings run."""
+    from qevedo_simulator_b200 import Plan, _native, options, run, statevector
+    from qevedo_simulator_b200._abi import settings_dict
+
+    n = 20
+    c = library.random_grid_circuit(4, 5, 12, seed=3)
+    ops = c.ops()
+    assert _native.ensure_cost_model()
+    chosen, pred = _native.plan_choose(ops, n, from_zero=False)
+    model = costmodel.CostModel.load()
+    by_name = {name: sec for name, _, sec in model.rank(ops, n)}
+    names = [name for name, _ in costmodel.candidates()]
+    assert len(pred) == len(names)
+    for name, p in zip(names, pred):
+        assert p == pytest.approx(by_name[name], rel=1e-5), name
+    assert settings_dict(chosen) == settings_dict(dict(costmodel.candidates())[names[int(np.argmin(pred))]])
+    pick0, _ = _native.plan_choose(ops, n, from_zero=True)
+    with Plan(ops, n, 32, options(planner="learned")) as plan:
+        assert plan.info()["settings"] == settings_dict(pick0)
+    expected = oracle.naive_statevector(ops, n)
+    assert np.abs(statevector(c, precision="single") - expected).max() <= 1e-6
+    cand = [settings_dict(o) for o in _native.planner_candidates(32)]
+    res = run(c.copy().measure_all(), 200, seed=1)
+    assert res.stats["settings"] in cand and sum(res.counts.values()) == 200
+    from qevedo_simulator_b200 import DeviceState
+
+    try:
+        _native.clear_cost_model()  # run() would register it again; the C ABI alone falls back
+        with DeviceState(n, 32) as st:
+            stats = st.apply_ops(ops, options(planner="learned"))
+        assert stats["settings"] == {"max_fused_qubits": 4, "staged": True, "tile_qubits": 0, "math": "fp32"}
+    finally:
+        _native.ensure_cost_model()
