@@ -1,51 +1,35 @@
-"""Reading OpenQASM 2 and 3 programs into circuits.
+"""OpenQASM 2 and 3 programs read into circuits.
 
-The front end of the reference's `qvd::qasm::parse` (src/qasm.rs) for the
-state-vector engine: registers (`qreg`/`creg`, `qubit`/`bit`), the gates of
-`qelib1.inc` / `stdgates.inc` (natively where the circuit builder has the
-gate, as exact unitaries for `csx`, `cu3`, `cu`, `c3x`, `c3sqrtx`, `c4x`, and
-through their `qelib1.inc` definitions for `rccx` / `rc3x`), gate
-definitions (expanded where called), parameter expressions, broadcasting
-over registers and ranges, measure, reset, barrier, `gphase` (ignored), the
-modifiers `inv @`, `ctrl(n) @`, `negctrl(n) @` and integer `pow(k) @`, and
-`if` on one classical bit with Pauli-only bodies (read as classical
-feedback). Anything else that needs classical state is rejected with the
-line and column of the statement (QasmError).
+The state-vector engine's reader for the programs the reference's
+`qvd::qasm::parse` (src/qasm.rs) takes: registers (`qreg`/`creg`,
+`qubit`/`bit`), the `qelib1.inc` / `stdgates.inc` gates, user gate
+definitions, parameter expressions, broadcasting over registers and ranges,
+`measure` (both forms), `reset`, `barrier`, `gphase` (a global phase, so
+dropped), the modifiers `inv @`, `ctrl(n) @`, `negctrl(n) @` and integer
+`pow(k) @`, and `if` on one classical bit whose bodies apply Pauli gates
+(lowered to classical feedback). Statements that need classical state the
+engine does not keep are refused with their line and column (QasmError).
+
+Design: one regular expression built from a token table splits the text;
+expressions are parsed by precedence climbing into closures over the gate
+parameters; statements are dispatched by keyword through a table; gate
+applications are lowered straight to the circuit's instructions, with a
+modified gate or a modified definition turned into one unitary. The user
+visible error messages and the instruction forms are the reference's.
 """
 
 from __future__ import annotations
 
+import bisect
 import math
-from dataclasses import dataclass, field
+import operator
+import re
+from dataclasses import dataclass
+from typing import Callable
 
 import numpy as np
 
 from .circuit import Circuit, Gate, _controlled
-
-# Definitions of the relative-phase Toffolis, as in qelib1.inc; a program may
-# redefine them.
-_PRELUDE = """
-gate rccx a,b,c
-{
-  u2(0,pi) c; u1(pi/4) c; cx b, c; u1(-pi/4) c; cx a, c;
-  u1(pi/4) c; cx b, c; u1(-pi/4) c; u2(0,pi) c;
-}
-gate rc3x a,b,c,d
-{
-  u2(0,pi) d; u1(pi/4) d; cx c,d; u1(-pi/4) d; u2(0,pi) d;
-  cx a,d; u1(pi/4) d; cx b,d; u1(-pi/4) d; cx a,d;
-  u1(pi/4) d; cx b,d; u1(-pi/4) d; u2(0,pi) d;
-  u1(pi/4) d; cx c,d; u1(-pi/4) d; u2(0,pi) d;
-}
-"""
-
-# Statement keywords that need classical state the engine does not model.
-_UNSUPPORTED = {"else", "for", "while", "def", "defcal", "defcalgrammar", "cal", "let", "const", "input", "output",
-                "int", "uint", "float", "angle", "bool", "complex", "duration", "stretch", "delay", "box", "return",
-                "break", "continue", "end", "extern", "array", "opaque", "pragma"}
-
-_SYMBOLS2 = {"->", "**", "==", "!="}
-_SYMBOLS1 = set(";,()[]{}=+-*/^@:<>!&|%~$")
 
 
 class QasmError(ValueError):
@@ -56,727 +40,726 @@ class QasmError(ValueError):
         self.line, self.column, self.message = line, column, message
 
 
-@dataclass
-class _Tok:
-    kind: str  # "id", "num", "str", "sym", "end"
-    value: object
-    line: int
-    column: int
+# ------------------------------------------------------------------ tokens
+# (kind, pattern), tried in this order at every position.
+_TOKEN_TABLE = (
+    ("space", r"\s+"),
+    ("comment", r"//[^\n]*|/\*.*?\*/"),
+    ("open_comment", r"/\*"),
+    ("number", r"(?:\d[\d_]*(?:\.[\d_]*)?|\.\d[\d_]*)(?:[eE][+-]?\d+)?"),
+    ("name", r"[^\W\d]\w*"),
+    ("string", r"\"[^\"\n]*\"|'[^'\n]*'"),
+    ("open_string", r"[\"']"),
+    ("symbol", r"->|\*\*|==|!=|[;,()\[\]{}=+\-*/^@:<>!&|%~$]"),
+)
+_SCANNER = re.compile("|".join(f"(?P<{kind}>{pattern})" for kind, pattern in _TOKEN_TABLE), re.S)
 
 
-def _lex(src: str) -> list:
-    toks, i, line, col = [], 0, 1, 1
-    n = len(src)
+@dataclass(frozen=True)
+class _Token:
+    kind: str  # "name", "number", "string", "symbol" or "end"
+    text: str
+    pos: int
 
-    def adv(k):
-        nonlocal i, line, col
-        for _ in range(k):
-            if src[i] == "\n":
-                line, col = line + 1, 1
-            else:
-                col += 1
-            i += 1
-
-    while i < n:
-        c = src[i]
-        sl, sc = line, col
-        if c.isspace():
-            adv(1)
-        elif src.startswith("//", i):
-            while i < n and src[i] != "\n":
-                adv(1)
-        elif src.startswith("/*", i):
-            j = src.find("*/", i + 2)
-            if j < 0:
-                raise QasmError(sl, sc, "unterminated comment")
-            adv(j + 2 - i)
-        elif c.isalpha() or c == "_":
-            j = i
-            while j < n and (src[j].isalnum() or src[j] == "_"):
-                j += 1
-            toks.append(_Tok("id", src[i:j], sl, sc))
-            adv(j - i)
-        elif c.isdigit() or (c == "." and i + 1 < n and src[i + 1].isdigit()):
-            j = i
-            while j < n and (src[j].isdigit() or src[j] in "._"):
-                j += 1
-            if j < n and src[j] in "eE":
-                k = j + 1
-                if k < n and src[k] in "+-":
-                    k += 1
-                if k < n and src[k].isdigit():
-                    j = k
-                    while j < n and src[j].isdigit():
-                        j += 1
-            text = src[i:j].replace("_", "")
-            try:
-                value = float(text)
-            except ValueError:
-                raise QasmError(sl, sc, f"invalid number `{text}`") from None
-            toks.append(_Tok("num", value, sl, sc))
-            adv(j - i)
-        elif c in "\"'":
-            j = i + 1
-            while j < n and src[j] != c and src[j] != "\n":
-                j += 1
-            if j >= n or src[j] != c:
-                raise QasmError(sl, sc, "unterminated string")
-            toks.append(_Tok("str", src[i + 1:j], sl, sc))
-            adv(j + 1 - i)
-        elif src[i:i + 2] in _SYMBOLS2:
-            toks.append(_Tok("sym", src[i:i + 2], sl, sc))
-            adv(2)
-        elif c in _SYMBOLS1:
-            toks.append(_Tok("sym", c, sl, sc))
-            adv(1)
-        else:
-            raise QasmError(sl, sc, f"unexpected character `{c}`")
-    toks.append(_Tok("end", None, line, col))
-    return toks
+    @property
+    def number(self) -> float:
+        return float(self.text.replace("_", ""))
 
 
-def _describe(t: _Tok) -> str:
-    if t.kind == "end":
-        return "the end of the program"
-    if t.kind == "num":
-        return f"number `{t.value:g}`"
-    return f"`{t.value}`"
+class _Tokens:
+    """The tokens of one source text and a cursor over them."""
 
+    def __init__(self, text: str):
+        self.text = text
+        self.line_starts = [0] + [m.end() for m in re.finditer("\n", text)]
+        self.items: list[_Token] = []
+        pos = 0
+        while pos < len(text):
+            m = _SCANNER.match(text, pos)
+            if m is None:
+                self.fail_at(pos, f"unexpected character `{text[pos]}`")
+            kind = m.lastgroup
+            if kind == "open_comment":
+                self.fail_at(pos, "unterminated comment")
+            if kind == "open_string":
+                self.fail_at(pos, "unterminated string")
+            if kind == "number":
+                try:
+                    float(m.group().replace("_", ""))
+                except ValueError:
+                    self.fail_at(pos, f"invalid number `{m.group()}`")
+            if kind == "string":
+                self.items.append(_Token("string", m.group()[1:-1], pos))
+            elif kind not in ("space", "comment"):
+                self.items.append(_Token(kind, m.group(), pos))
+            pos = m.end()
+        self.items.append(_Token("end", "", len(text)))
+        self.at = 0
+
+    # positions and errors
+    def where(self, pos: int) -> tuple:
+        line = bisect.bisect_right(self.line_starts, pos)
+        return line, pos - self.line_starts[line - 1] + 1
+
+    def fail_at(self, pos: int, message: str):
+        raise QasmError(*self.where(pos), message)
+
+    def fail(self, tok: _Token, message: str):
+        self.fail_at(tok.pos, message)
+
+    @staticmethod
+    def describe(tok: _Token) -> str:
+        if tok.kind == "end":
+            return "the end of the program"
+        if tok.kind == "number":
+            return f"number `{tok.number:g}`"
+        return f"`{tok.text}`"
+
+    # the cursor
+    def peek(self) -> _Token:
+        return self.items[self.at]
+
+    def take(self) -> _Token:
+        tok = self.items[self.at]
+        self.at = min(self.at + 1, len(self.items) - 1)
+        return tok
+
+    def at_symbol(self, text: str) -> bool:
+        tok = self.items[self.at]
+        return tok.kind == "symbol" and tok.text == text
+
+    def at_name(self, text: str) -> bool:
+        tok = self.items[self.at]
+        return tok.kind == "name" and tok.text == text
+
+    def at_end(self) -> bool:
+        return self.items[self.at].kind == "end"
+
+    def accept(self, text: str) -> bool:
+        if self.at_symbol(text):
+            self.take()
+            return True
+        return False
+
+    def require(self, text: str) -> _Token:
+        tok = self.take()
+        if tok.kind != "symbol" or tok.text != text:
+            self.fail(tok, f"expected `{text}`, found {self.describe(tok)}")
+        return tok
+
+    def name(self) -> _Token:
+        tok = self.take()
+        if tok.kind != "name":
+            self.fail(tok, f"expected a name, found {self.describe(tok)}")
+        return tok
+
+    def index(self) -> int:
+        tok = self.take()
+        if tok.kind != "number" or tok.number < 0 or tok.number != int(tok.number):
+            self.fail(tok, f"expected a non-negative integer, found {self.describe(tok)}")
+        return int(tok.number)
+
+    def skip_past(self, text: str):
+        while not self.at_symbol(text) and not self.at_end():
+            self.take()
+        self.require(text)
+
+
+# ------------------------------------------------------------- expressions
+Expr = Callable[[dict], float]
 
 _CONSTANTS = {"pi": math.pi, "π": math.pi, "tau": math.tau, "τ": math.tau, "euler": math.e, "ℇ": math.e}
 _FUNCTIONS = {"sin": math.sin, "cos": math.cos, "tan": math.tan, "exp": math.exp, "ln": math.log, "sqrt": math.sqrt,
               "arcsin": math.asin, "asin": math.asin, "arccos": math.acos, "acos": math.acos, "arctan": math.atan,
               "atan": math.atan}
+# Infix operators: symbol -> (binding power, right associative, function).
+_INFIX = {"+": (10, False, operator.add), "-": (10, False, operator.sub), "*": (20, False, operator.mul),
+          "/": (20, False, operator.truediv), "^": (30, True, math.pow), "**": (30, True, math.pow)}
+# A sign binds tighter than every infix operator (-2^2 is (-2)^2, as in the
+# reference's grammar).
+_PREFIX_POWER = 40
 
 
-def _eval(expr, env: dict) -> float:
-    kind = expr[0]
-    if kind == "num":
-        return expr[1]
-    if kind == "name":
-        _, name, tok = expr
-        if name in _CONSTANTS:
-            return _CONSTANTS[name]
-        if name in env:
-            return env[name]
-        raise QasmError(tok.line, tok.column, f"unknown parameter `{name}`")
-    if kind == "neg":
-        return -_eval(expr[1], env)
-    if kind == "bin":
-        op, a, b = expr[1], _eval(expr[2], env), _eval(expr[3], env)
-        if op == "+":
-            return a + b
-        if op == "-":
-            return a - b
-        if op == "*":
-            return a * b
-        if op == "/":
-            return a / b
-        return math.pow(a, b)
-    _, name, arg, tok = expr  # call
-    if name not in _FUNCTIONS:
-        raise QasmError(tok.line, tok.column, f"unknown function `{name}`")
-    return _FUNCTIONS[name](_eval(arg, env))
+def _expression(toks: _Tokens, min_power: int = 0) -> Expr:
+    """Precedence climbing over _INFIX; the result evaluates in an
+    environment of parameter values."""
+    left = _primary(toks)
+    while True:
+        tok = toks.peek()
+        entry = _INFIX.get(tok.text) if tok.kind == "symbol" else None
+        if entry is None or entry[0] < min_power:
+            return left
+        power, right_assoc, fn = entry
+        toks.take()
+        right = _expression(toks, power if right_assoc else power + 1)
+        left = (lambda f, a, b: lambda env: f(a(env), b(env)))(fn, left, right)
 
 
-def _builtin(name: str, p: list):
-    """(Gate, arity) for a built-in gate name, None if unknown; raises
-    ValueError (message) on a wrong parameter count. src/qasm.rs:1377-1435."""
-
-    def need(k):
-        if len(p) != k:
-            raise ValueError(f"`{name}` takes {k} parameters, given {len(p)}")
-
-    simple = {"id": "id", "i": "id", "h": "h", "x": "x", "y": "y", "z": "z", "s": "s", "sdg": "sdg", "t": "t",
-              "tdg": "tdg", "sx": "sx", "sxdg": "sxdg", "CX": "cx", "cx": "cx", "cnot": "cx", "cy": "cy",
-              "cz": "cz", "ch": "ch", "swap": "swap", "ccx": "ccx", "toffoli": "ccx", "cswap": "cswap",
-              "fredkin": "cswap"}
-    one = {"rx": "rx", "ry": "ry", "rz": "rz", "p": "p", "u1": "p", "phase": "p", "cp": "cp", "cu1": "cp",
-           "cphase": "cp", "crx": "crx", "cry": "cry", "crz": "crz", "rzz": "rzz", "rxx": "rxx"}
-    if name in simple:
-        need(0)
-        g = Gate(simple[name])
-        return g, g.arity
-    if name in one:
-        need(1)
-        g = Gate(one[name], (float(p[0]),))
-        return g, g.arity
-    if name == "u0":
-        need(1)
-        return Gate("id"), 1
-    if name == "u2":
-        need(2)
-        return Gate("u", (math.pi / 2, float(p[0]), float(p[1]))), 1
-    if name in ("U", "u", "u3"):
-        need(3)
-        return Gate("u", tuple(float(v) for v in p)), 1
-    x = Gate("x").matrix()
-    sx = Gate("sx").matrix()
-    if name == "csx":
-        need(0)
-        return Gate("unitary", (), _controlled(sx, 1, 1)), 2
-    if name == "cu3":
-        need(3)
-        return Gate("unitary", (), _controlled(Gate("u", tuple(p)).matrix(), 1, 1)), 2
-    if name == "cu":
-        need(4)
-        u = Gate("u", tuple(p[:3])).matrix() * complex(math.cos(p[3]), math.sin(p[3]))
-        return Gate("unitary", (), _controlled(u, 1, 1)), 2
-    if name == "c3x":
-        need(0)
-        return Gate("unitary", (), _controlled(x, 3, 7)), 4
-    if name == "c4x":
-        need(0)
-        return Gate("unitary", (), _controlled(x, 4, 15)), 5
-    if name == "c3sqrtx":
-        need(0)
-        return Gate("unitary", (), _controlled(sx, 3, 7)), 4
-    return None
+def _primary(toks: _Tokens) -> Expr:
+    tok = toks.take()
+    if tok.kind == "symbol" and tok.text in "+-" and len(tok.text) == 1:
+        inner = _expression(toks, _PREFIX_POWER)
+        return inner if tok.text == "+" else (lambda env: -inner(env))
+    if tok.kind == "number":
+        value = tok.number
+        return lambda env: value
+    if tok.kind == "symbol" and tok.text == "(":
+        inner = _expression(toks)
+        toks.require(")")
+        return inner
+    if tok.kind == "name":
+        if toks.accept("("):
+            arg = _expression(toks)
+            toks.require(")")
+            return _function_call(toks, tok, arg)
+        return _variable(toks, tok)
+    toks.fail(tok, f"expected an expression, found {toks.describe(tok)}")
 
 
-def _apply(state: np.ndarray, m: np.ndarray, qubits: list) -> np.ndarray:
-    """m on `qubits` (matrix index bit j = qubits[j]) of a small state vector."""
-    k = len(qubits)
-    n = int(state.size).bit_length() - 1
-    t = state.reshape([2] * n)
-    axes = [n - 1 - q for q in reversed(qubits)]  # tensor axis of index bit
-    t = np.moveaxis(t, axes, range(k))
-    t = (m @ t.reshape(1 << k, -1)).reshape(t.shape)
-    return np.moveaxis(t, range(k), axes).reshape(-1)
+def _function_call(toks: _Tokens, tok: _Token, arg: Expr) -> Expr:
+    def call(env):
+        fn = _FUNCTIONS.get(tok.text)
+        if fn is None:
+            toks.fail(tok, f"unknown function `{tok.text}`")
+        return fn(arg(env))
+
+    return call
+
+
+def _variable(toks: _Tokens, tok: _Token) -> Expr:
+    def value(env):
+        if tok.text in _CONSTANTS:
+            return _CONSTANTS[tok.text]
+        if tok.text in env:
+            return env[tok.text]
+        toks.fail(tok, f"unknown parameter `{tok.text}`")
+
+    return value
+
+
+# ------------------------------------------------------------ gate library
+def _gate_library():
+    """name -> (parameter count, maker(params) -> (Gate, arity)) for the
+    gates of qelib1.inc and stdgates.inc (src/qasm.rs:1377-1435), with the
+    ones the circuit builder lacks as exact controlled unitaries."""
+
+    def named(kind):
+        def make(p):
+            g = Gate(kind, tuple(float(v) for v in p))
+            return g, g.arity
+
+        return make
+
+    def controlled(base, controls):
+        return lambda p: (Gate("unitary", (), _controlled(base(p), controls, (1 << controls) - 1)), controls + 1)
+
+    table = {}
+    for kind, aliases in (("id", ("id", "i")), ("h", ("h",)), ("x", ("x",)), ("y", ("y",)), ("z", ("z",)),
+                          ("s", ("s",)), ("sdg", ("sdg",)), ("t", ("t",)), ("tdg", ("tdg",)), ("sx", ("sx",)),
+                          ("sxdg", ("sxdg",)), ("cx", ("CX", "cx", "cnot")), ("cy", ("cy",)), ("cz", ("cz",)),
+                          ("ch", ("ch",)), ("swap", ("swap",)), ("ccx", ("ccx", "toffoli")),
+                          ("cswap", ("cswap", "fredkin"))):
+        for alias in aliases:
+            table[alias] = (0, named(kind))
+    for kind, aliases in (("rx", ("rx",)), ("ry", ("ry",)), ("rz", ("rz",)), ("p", ("p", "u1", "phase")),
+                          ("cp", ("cp", "cu1", "cphase")), ("crx", ("crx",)), ("cry", ("cry",)), ("crz", ("crz",)),
+                          ("rzz", ("rzz",)), ("rxx", ("rxx",))):
+        for alias in aliases:
+            table[alias] = (1, named(kind))
+    table["u0"] = (1, lambda p: (Gate("id"), 1))
+    table["u2"] = (2, lambda p: named("u")([math.pi / 2, p[0], p[1]]))
+    for alias in ("U", "u", "u3"):
+        table[alias] = (3, named("u"))
+    x, sx = (lambda p: Gate("x").matrix()), (lambda p: Gate("sx").matrix())
+    table["csx"] = (0, controlled(sx, 1))
+    table["cu3"] = (3, controlled(lambda p: Gate("u", tuple(p)).matrix(), 1))
+    table["cu"] = (4, controlled(lambda p: Gate("u", tuple(p[:3])).matrix() * complex(math.cos(p[3]),
+                                                                                        math.sin(p[3])), 1))
+    table["c3x"] = (0, controlled(x, 3))
+    table["c4x"] = (0, controlled(x, 4))
+    table["c3sqrtx"] = (0, controlled(sx, 3))
+    return table
+
+
+_LIBRARY = _gate_library()
+
+# The relative-phase Toffolis through their qelib1.inc definitions (a
+# program may redefine them).
+_PRELUDE = """
+gate rccx a,b,c { u2(0,pi) c; u1(pi/4) c; cx b,c; u1(-pi/4) c; cx a,c; u1(pi/4) c; cx b,c; u1(-pi/4) c;
+                  u2(0,pi) c; }
+gate rc3x a,b,c,d { u2(0,pi) d; u1(pi/4) d; cx c,d; u1(-pi/4) d; u2(0,pi) d; cx a,d; u1(pi/4) d; cx b,d;
+                    u1(-pi/4) d; cx a,d; u1(pi/4) d; cx b,d; u1(-pi/4) d; u2(0,pi) d; u1(pi/4) d; cx c,d;
+                    u1(-pi/4) d; u2(0,pi) d; }
+"""
+
+# Keywords of statements that need classical state the engine does not keep.
+_REFUSED = {"else", "for", "while", "def", "defcal", "defcalgrammar", "cal", "let", "const", "input", "output",
+            "int", "uint", "float", "angle", "bool", "complex", "duration", "stretch", "delay", "box", "return",
+            "break", "continue", "end", "extern", "array", "opaque", "pragma"}
+_MODIFIERS = ("inv", "ctrl", "negctrl", "pow")
+_PAULI_BITS = {"x": 1, "z": 2, "y": 3}  # X = 1, Z = 2, Y = X.Z up to phase
+_PAULI_LETTER = {1: "X", 2: "Z", 3: "Y"}
+
+
+def _embed(m: np.ndarray, qubits: list, k: int) -> np.ndarray:
+    """`m` (matrix index bit j = qubits[j]) as a 2^k x 2^k matrix."""
+    idx = np.arange(1 << k)
+    sub = np.zeros_like(idx)
+    rest = idx.copy()
+    for j, q in enumerate(qubits):
+        sub |= ((idx >> q) & 1) << j
+        rest &= ~(1 << q)
+    return np.where(rest[:, None] == rest[None, :], m[sub[:, None], sub[None, :]], 0)
+
+
+def _unitary(instructions: list, k: int) -> np.ndarray:
+    """The product of gate instructions on qubits 0..k-1 (first applied first)."""
+    u = np.eye(1 << k, dtype=np.complex128)
+    for _, gate, qubits in instructions:
+        u = _embed(gate.matrix(), qubits, k) @ u
+    return u
+
+
+# ---------------------------------------------------------------- programs
+@dataclass
+class _Operand:
+    register: _Token
+    indices: list | None  # None: the whole register
 
 
 @dataclass
-class _Call:
-    modifiers: list
-    name: str
-    params: list
-    args: list  # names, or ("idx", token position) for indexed operands
-    tok: _Tok
+class _Application:
+    modifiers: list  # ("inv",) | ("pow", Expr, tok) | ("ctrl"|"negctrl", count)
+    name: _Token
+    params: list  # of Expr
+    operands: list  # of _Operand
 
 
 @dataclass
 class _Definition:
-    params: list
-    qubits: list
-    body: list
+    params: list  # names
+    qubits: list  # names
+    body: list  # of _Application
 
 
-@dataclass
 class _Program:
-    qubits: int = 0
-    clbits: int = 0
-    qregs: dict = field(default_factory=dict)
-    cregs: dict = field(default_factory=dict)
-    gates: dict = field(default_factory=dict)
-    ins: list = field(default_factory=list)
+    """Registers, definitions and the instructions emitted so far."""
 
+    def __init__(self, definitions: dict | None = None):
+        self.qubits = self.clbits = 0
+        self.qregs: dict = {}
+        self.cregs: dict = {}
+        self.definitions = dict(definitions or {})
+        self.out: list = []
 
-class _Parser:
-    def __init__(self, toks, program):
-        self.toks, self.at, self.p = toks, 0, program
+    def read(self, text: str):
+        toks = _Tokens(text)
+        while not toks.at_end():
+            _statement(self, toks)
 
-    # -- tokens
-    def peek(self):
-        return self.toks[self.at]
-
-    def next(self):
-        t = self.toks[self.at]
-        if self.at + 1 < len(self.toks):
-            self.at += 1
-        return t
-
-    def err(self, t, msg):
-        raise QasmError(t.line, t.column, msg)
-
-    def is_sym(self, s):
-        t = self.peek()
-        return t.kind == "sym" and t.value == s
-
-    def is_word(self, w):
-        t = self.peek()
-        return t.kind == "id" and t.value == w
-
-    def expect(self, s):
-        t = self.next()
-        if not (t.kind == "sym" and t.value == s):
-            self.err(t, f"expected `{s}`, found {_describe(t)}")
-        return t
-
-    def ident(self):
-        t = self.next()
-        if t.kind != "id":
-            self.err(t, f"expected a name, found {_describe(t)}")
-        return t.value, t
-
-    def integer(self):
-        t = self.next()
-        if t.kind != "num" or t.value < 0 or t.value != int(t.value):
-            self.err(t, f"expected a non-negative integer, found {_describe(t)}")
-        return int(t.value)
-
-    # -- program
-    def program(self):
-        while self.peek().kind != "end":
-            self.statement()
-
-    def statement(self):
-        t = self.peek()
-        if t.kind != "id":
-            self.err(t, f"expected a statement, found {_describe(t)}")
-        w = t.value
-        if w == "OPENQASM":
-            self.next()
-            v = self.next()
-            if v.kind != "num" or not 2.0 <= v.value < 4.0:
-                self.err(v, "only OpenQASM 2 and 3 are supported")
-            self.expect(";")
-        elif w == "include":
-            self.next()
-            f = self.next()
-            if f.kind != "str":
-                self.err(f, "expected a file name")
-            if f.value not in ("qelib1.inc", "stdgates.inc"):
-                self.err(f, f"cannot include `{f.value}`: only qelib1.inc and stdgates.inc are built in")
-            self.expect(";")
-        elif w in ("qreg", "creg"):
-            self.next()
-            name, at = self.ident()
-            self.expect("[")
-            size = self.integer()
-            self.expect("]")
-            self.expect(";")
-            self.declare(w == "qreg", name, size, at)
-        elif w in ("qubit", "bit"):
-            self.next()
-            size = 1
-            if self.is_sym("["):
-                self.next()
-                size = self.integer()
-                self.expect("]")
-            name, at = self.ident()
-            if self.is_sym("="):
-                self.err(at, "initialising classical bits is not supported")
-            self.expect(";")
-            self.declare(w == "qubit", name, size, at)
-        elif w == "gate":
-            self.definition()
-        elif w == "if":
-            self.conditional()
-        elif w == "measure":
-            self.next()
-            qs = self.operand(True)
-            if not self.is_sym("->"):
-                self.err(t, "a measurement must store its result (`measure q -> c;` or `c = measure q;`)")
-            self.next()
-            cs = self.operand(False)
-            self.expect(";")
-            self.measure(qs, cs, t)
-        elif w == "reset":
-            self.next()
-            qs = self.operand(True)
-            self.expect(";")
-            for q in qs:
-                self.p.ins.append(("reset", q))
-        elif w == "barrier":
-            self.next()
-            qs = []
-            while not self.is_sym(";"):
-                qs.extend(self.operand(True))
-                if self.is_sym(","):
-                    self.next()
-            self.expect(";")
-            self.p.ins.append(("barrier", qs or list(range(self.p.qubits))))
-        elif w == "gphase":
-            while not self.is_sym(";") and self.peek().kind != "end":
-                self.next()
-            self.expect(";")
-        elif w in _UNSUPPORTED:
-            self.err(t, f"`{w}` is not supported (the simulator runs gates, measurements and resets only)")
-        else:
-            save = self.at
-            self.next()
-            if self.is_sym("[") or self.is_sym("="):
-                self.at = save
-                cs = self.operand(False)
-                self.expect("=")
-                kw, at = self.ident()
-                if kw != "measure":
-                    self.err(at, "assigning classical values other than measurements is not supported")
-                qs = self.operand(True)
-                self.expect(";")
-                self.measure(qs, cs, t)
-            else:
-                self.at = save
-                call = self.call()
-                self.expect(";")
-                self.top_level_call(call)
-
-    def declare(self, quantum, name, size, at):
-        if name in self.p.qregs or name in self.p.cregs:
-            self.err(at, f"`{name}` is already declared")
+    # registers
+    def declare(self, toks, quantum: bool, name: _Token, size: int):
+        if name.text in self.qregs or name.text in self.cregs:
+            toks.fail(name, f"`{name.text}` is already declared")
         if quantum:
-            self.p.qregs[name] = (self.p.qubits, size)
-            self.p.qubits += size
+            self.qregs[name.text] = (self.qubits, size)
+            self.qubits += size
         else:
-            self.p.cregs[name] = (self.p.clbits, size)
-            self.p.clbits += size
+            self.cregs[name.text] = (self.clbits, size)
+            self.clbits += size
 
-    def measure(self, qs, cs, at):
-        if len(qs) != len(cs):
-            self.err(at, f"measuring {len(qs)} qubits into {len(cs)} bits")
-        for q, c in zip(qs, cs):
-            self.p.ins.append(("measure", q, c))
-
-    def operand(self, quantum):
-        name, at = self.ident()
-        regs = self.p.qregs if quantum else self.p.cregs
-        if name not in regs:
-            self.err(at, f"unknown {'qubit' if quantum else 'classical bit'} register `{name}`")
-        first, size = regs[name]
-        if not self.is_sym("["):
+    def resolve(self, toks, operand: _Operand, quantum: bool) -> list:
+        regs = self.qregs if quantum else self.cregs
+        reg = operand.register
+        if reg.text not in regs:
+            toks.fail(reg, f"unknown {'qubit' if quantum else 'classical bit'} register `{reg.text}`")
+        first, size = regs[reg.text]
+        if operand.indices is None:
             return list(range(first, first + size))
-        self.next()
-        start = self.integer()
-        idx = [start]
-        if self.is_sym(":"):
-            self.next()
-            second = self.integer()
-            step, end = 1, second
-            if self.is_sym(":"):
-                self.next()
-                step, end = second, self.integer()
-            if step == 0:
-                self.err(at, "a range step must be positive")
-            idx = list(range(start, end + 1, step))
-        self.expect("]")
-        for i in idx:
+        for i in operand.indices:
             if i >= size:
-                self.err(at, f"index {i} is out of range for `{name}` of size {size}")
-        return [first + i for i in idx]
+                toks.fail(reg, f"index {i} is out of range for `{reg.text}` of size {size}")
+        return [first + i for i in operand.indices]
 
-    # -- expressions: + -, * /, ^ ** (right associative), unary minus
-    def expression(self):
-        left = self.term()
-        while self.is_sym("+") or self.is_sym("-"):
-            op = self.next().value
-            left = ("bin", op, left, self.term())
-        return left
-
-    def term(self):
-        left = self.power()
-        while self.is_sym("*") or self.is_sym("/"):
-            op = self.next().value
-            left = ("bin", op, left, self.power())
-        return left
-
-    def power(self):
-        base = self.unary()
-        if self.is_sym("^") or self.is_sym("**"):
-            self.next()
-            return ("bin", "^", base, self.power())
-        return base
-
-    def unary(self):
-        if self.is_sym("-"):
-            self.next()
-            return ("neg", self.unary())
-        if self.is_sym("+"):
-            self.next()
-            return self.unary()
-        t = self.next()
-        if t.kind == "num":
-            return ("num", t.value)
-        if t.kind == "sym" and t.value == "(":
-            e = self.expression()
-            self.expect(")")
-            return e
-        if t.kind == "id":
-            if self.is_sym("("):
-                self.next()
-                arg = self.expression()
-                self.expect(")")
-                return ("call", t.value, arg, t)
-            return ("name", t.value, t)
-        self.err(t, f"expected an expression, found {_describe(t)}")
-
-    # -- gate calls
-    def call(self):
-        mods = []
-        while True:
-            t = self.peek()
-            if t.kind != "id" or t.value not in ("inv", "ctrl", "negctrl", "pow"):
-                break
-            save = self.at
-            self.next()
-            arg = None
-            if self.is_sym("("):
-                self.next()
-                arg = self.expression()
-                self.expect(")")
-            if not self.is_sym("@"):
-                self.at = save
-                break
-            self.next()
-            if t.value == "inv":
-                mods.append(("inv",))
-            elif t.value == "pow":
-                if arg is None:
-                    self.err(t, "`pow` needs an exponent")
-                mods.append(("pow", arg, t))
-            else:
-                count = 1
-                if arg is not None:
-                    x = _eval(arg, {})
-                    if x < 1 or x != int(x):
-                        self.err(t, "a control count must be a positive integer")
-                    count = int(x)
-                mods.append((t.value, count))
-        name, at = self.ident()
-        params = []
-        if self.is_sym("("):
-            self.next()
-            if not self.is_sym(")"):
-                while True:
-                    params.append(self.expression())
-                    if self.is_sym(","):
-                        self.next()
-                    else:
-                        break
-            self.expect(")")
-        args = []
-        while not self.is_sym(";") and not self.is_sym("}") and self.peek().kind != "end":
-            start = self.at
-            arg, _ = self.ident()
-            if self.is_sym("["):
-                while not self.is_sym("]") and self.peek().kind != "end":
-                    self.next()
-                self.expect("]")
-                arg = ("idx", start)
-            args.append(arg)
-            if self.is_sym(","):
-                self.next()
-            else:
-                break
-        return _Call(mods, name, params, args, at)
-
-    def top_level_call(self, call):
-        operands = []
-        for a in call.args:
-            if isinstance(a, tuple):
-                save = self.at
-                self.at = a[1]
-                operands.append(self.operand(True))
-                self.at = save
-            else:
-                if a not in self.p.qregs:
-                    self.err(call.tok, f"unknown qubit register `{a}`")
-                first, size = self.p.qregs[a]
-                operands.append(list(range(first, first + size)))
-        width = max([len(o) for o in operands if len(o) != 1] or [1])
-        if any(len(o) not in (1, width) for o in operands):
-            self.err(call.tok, "registers of different sizes cannot be broadcast together")
-        params = [_eval(e, {}) for e in call.params]
+    # gates
+    def apply(self, toks, app: _Application):
+        """A top-level application, broadcast over register operands."""
+        groups = [self.resolve(toks, o, True) for o in app.operands]
+        width = max([len(g) for g in groups if len(g) != 1] or [1])
+        if any(len(g) not in (1, width) for g in groups):
+            toks.fail(app.name, "registers of different sizes cannot be broadcast together")
+        values = [e({}) for e in app.params]
         for i in range(width):
-            qubits = [o[0] if len(o) == 1 else o[i] for o in operands]
+            qubits = [g[0] if len(g) == 1 else g[i] for g in groups]
             if len(set(qubits)) != len(qubits):
-                self.err(call.tok, f"`{call.name}` is applied to the same qubit twice")
-            self.p.ins.extend(self.expand(call.modifiers, call.name, params, qubits, call.tok, 0))
+                toks.fail(app.name, f"`{app.name.text}` is applied to the same qubit twice")
+            self.out.extend(self.lower(toks, app.modifiers, app.name, values, qubits, 0))
 
-    def expand(self, mods, name, params, qubits, at, depth):
+    def lower(self, toks, modifiers: list, name: _Token, values: list, qubits: list, depth: int) -> list:
+        """Instructions of gate `name` with parameter values on global qubits."""
         if depth > 64:
-            self.err(at, f"gate `{name}` is defined recursively")
-        if mods:
-            controls = sum(m[1] for m in mods if m[0] in ("ctrl", "negctrl"))
-            if len(qubits) <= controls:
-                self.err(at, f"`{name}` with {controls} controls needs more qubits")
-            k = len(qubits) - controls
-            body = self.expand([], name, params, list(range(k)), at, depth + 1)
-            m = np.eye(1 << k, dtype=np.complex128)
-            for col in range(1 << k):
-                v = np.zeros(1 << k, dtype=np.complex128)
-                v[col] = 1.0
-                for ins in body:
-                    v = _apply(v, ins[1].matrix(), ins[2])
-                m[:, col] = v
-            # Modifiers apply right to left: the one nearest the gate first.
-            for mod in reversed(mods):
-                if mod[0] == "inv":
-                    m = m.conj().T
-                elif mod[0] == "pow":
-                    e = _eval(mod[1], {})
-                    if e != int(e):
-                        self.err(at, "only integer powers are supported")
-                    base = m.conj().T if e < 0 else m
-                    m = np.linalg.matrix_power(base, int(abs(e)))
-                else:
-                    c = mod[1]
-                    m = _controlled(m, c, (1 << c) - 1 if mod[0] == "ctrl" else 0)
-            return [("gate", Gate("unitary", (), m), list(qubits))]
-        if name in self.p.gates:
-            d = self.p.gates[name]
-            if len(d.params) != len(params) or len(d.qubits) != len(qubits):
-                self.err(at, f"`{name}` takes {len(d.params)} parameters and {len(d.qubits)} qubits, given "
-                             f"{len(params)} and {len(qubits)}")
-            env = dict(zip(d.params, params))
-            where = dict(zip(d.qubits, qubits))
+            toks.fail(name, f"gate `{name.text}` is defined recursively")
+        if modifiers:
+            return [self.modified(toks, modifiers, name, values, qubits, depth)]
+        d = self.definitions.get(name.text)
+        if d is not None:
+            if len(d.params) != len(values) or len(d.qubits) != len(qubits):
+                toks.fail(name, f"`{name.text}` takes {len(d.params)} parameters and {len(d.qubits)} qubits, "
+                                f"given {len(values)} and {len(qubits)}")
+            env = dict(zip(d.params, values))
+            wires = dict(zip(d.qubits, qubits))
             out = []
-            for c in d.body:
-                values = [_eval(e, env) for e in c.params]
-                args = []
-                for a in c.args:
-                    if a not in where:
-                        self.err(c.tok, f"unknown qubit `{a}` in the definition of `{name}`")
-                    args.append(where[a])
-                out.extend(self.expand(c.modifiers, c.name, values, args, c.tok, depth + 1))
+            for app in d.body:
+                inner = []
+                for o in app.operands:
+                    if o.register.text not in wires:
+                        toks.fail(o.register, f"unknown qubit `{o.register.text}` in the definition of `{name.text}`")
+                    inner.append(wires[o.register.text])
+                out.extend(self.lower(toks, app.modifiers, app.name, [e(env) for e in app.params], inner, depth + 1))
             return out
-        try:
-            found = _builtin(name, params)
-        except ValueError as e:
-            self.err(at, str(e))
-        if found is None:
-            self.err(at, f"unknown gate `{name}`")
-        gate, arity = found
+        entry = _LIBRARY.get(name.text)
+        if entry is None:
+            toks.fail(name, f"unknown gate `{name.text}`")
+        count, make = entry
+        if count != len(values):
+            toks.fail(name, f"`{name.text}` takes {count} parameters, given {len(values)}")
+        gate, arity = make(values)
         if arity != len(qubits):
-            self.err(at, f"`{name}` acts on {arity} qubits, given {len(qubits)}")
+            toks.fail(name, f"`{name.text}` acts on {arity} qubits, given {len(qubits)}")
         return [("gate", gate, list(qubits))]
 
-    def definition(self):
-        self.next()
-        name, at = self.ident()
-        params = []
-        if self.is_sym("("):
-            self.next()
-            while not self.is_sym(")"):
-                params.append(self.ident()[0])
-                if self.is_sym(","):
-                    self.next()
-            self.expect(")")
-        qubits = []
-        while not self.is_sym("{"):
-            qubits.append(self.ident()[0])
-            if self.is_sym(","):
-                self.next()
-        self.expect("{")
-        body = []
-        while not self.is_sym("}"):
-            if self.peek().kind == "end":
-                self.err(at, f"unterminated definition of `{name}`")
-            if self.is_word("barrier"):
-                while not self.is_sym(";"):
-                    self.next()
-                self.expect(";")
-                continue
-            c = self.call()
-            if any(isinstance(a, tuple) for a in c.args):
-                self.err(at, f"the body of `{name}` can only use its own qubit names")
-            body.append(c)
-            self.expect(";")
-        self.expect("}")
-        self.p.gates[name] = _Definition(params, qubits, body)
+    def modified(self, toks, modifiers, name, values, qubits, depth):
+        """One unitary for a modified gate: the gate's own unitary on its
+        target qubits, then each modifier from the one nearest the gate."""
+        controls = sum(m[1] for m in modifiers if m[0] in ("ctrl", "negctrl"))
+        k = len(qubits) - controls
+        if k <= 0:
+            toks.fail(name, f"`{name.text}` with {controls} controls needs more qubits")
+        u = _unitary(self.lower(toks, [], name, values, list(range(k)), depth + 1), k)
+        for mod in reversed(modifiers):
+            if mod[0] == "inv":
+                u = u.conj().T
+            elif mod[0] == "pow":
+                e = mod[1]({})
+                if e != int(e):
+                    toks.fail(name, "only integer powers are supported")
+                u = np.linalg.matrix_power(u.conj().T if e < 0 else u, int(abs(e)))
+            else:
+                c = mod[1]
+                u = _controlled(u, c, (1 << c) - 1 if mod[0] == "ctrl" else 0)
+        return ("gate", Gate("unitary", (), u), list(qubits))
 
-    # -- if on one bit with Pauli bodies: classical feedback
-    def conditional(self):
-        at = self.next()
-        self.expect("(")
-        clbit, wanted = self.condition()
-        self.expect(")")
-        then = self.pauli_body(at)
-        other = {}
-        if self.is_word("else"):
-            self.next()
-            other = self.pauli_body(at)
-        on_one, on_zero = (then, other) if wanted else (other, then)
-        letters = {1: "X", 2: "Z", 3: "Y"}
-        for q, bits in on_zero.items():
-            if bits in letters:
-                self.p.ins.append(("gate", Gate(letters[bits].lower()), [q]))
-        for q in sorted(set(on_one) | set(on_zero)):
-            flip = on_one.get(q, 0) ^ on_zero.get(q, 0)
-            if flip in letters:
-                self.p.ins.append(("feedback", letters[flip], q, clbit))
 
-    def condition(self):
-        negated = False
-        while self.is_sym("!"):
-            self.next()
-            negated = not negated
-        name, at = self.ident()
-        if name not in self.p.cregs:
-            self.err(at, f"unknown classical bit register `{name}` in a condition")
-        first, size = self.p.cregs[name]
-        if self.is_sym("["):
-            self.next()
-            index = self.integer()
-            self.expect("]")
-            if index >= size:
-                self.err(at, f"index {index} is out of range for `{name}` of size {size}")
-            clbit = first + index
-        elif size == 1:
-            clbit = first
+# -------------------------------------------------------------- statements
+def _statement(p: _Program, toks: _Tokens):
+    tok = toks.peek()
+    if tok.kind != "name":
+        toks.fail(tok, f"expected a statement, found {toks.describe(tok)}")
+    handler = _STATEMENTS.get(tok.text)
+    if handler is not None:
+        handler(p, toks)
+    elif tok.text in _REFUSED:
+        toks.fail(tok, f"`{tok.text}` is not supported (the simulator runs gates, measurements and resets only)")
+    elif tok.text in p.cregs and toks.items[toks.at + 1].text in ("[", "="):
+        _assigned_measure(p, toks)
+    else:
+        app = _application(toks)
+        toks.require(";")
+        p.apply(toks, app)
+
+
+def _version(p, toks):
+    toks.take()
+    v = toks.take()
+    if v.kind != "number" or not 2.0 <= v.number < 4.0:
+        toks.fail(v, "only OpenQASM 2 and 3 are supported")
+    toks.require(";")
+
+
+def _include(p, toks):
+    toks.take()
+    f = toks.take()
+    if f.kind != "string":
+        toks.fail(f, "expected a file name")
+    if f.text not in ("qelib1.inc", "stdgates.inc"):
+        toks.fail(f, f"cannot include `{f.text}`: only qelib1.inc and stdgates.inc are built in")
+    toks.require(";")
+
+
+def _register_v2(p, toks):
+    quantum = toks.take().text == "qreg"
+    name = toks.name()
+    toks.require("[")
+    size = toks.index()
+    toks.require("]")
+    toks.require(";")
+    p.declare(toks, quantum, name, size)
+
+
+def _register_v3(p, toks):
+    quantum = toks.take().text == "qubit"
+    size = 1
+    if toks.accept("["):
+        size = toks.index()
+        toks.require("]")
+    name = toks.name()
+    if toks.at_symbol("="):
+        toks.fail(name, "initialising classical bits is not supported")
+    toks.require(";")
+    p.declare(toks, quantum, name, size)
+
+
+def _operand(toks: _Tokens) -> _Operand:
+    """`name`, `name[i]` or `name[start:stop]` / `name[start:step:stop]`
+    (inclusive stop)."""
+    reg = toks.name()
+    if not toks.accept("["):
+        return _Operand(reg, None)
+    parts = [toks.index()]
+    while toks.accept(":"):
+        parts.append(toks.index())
+    toks.require("]")
+    if len(parts) == 1:
+        return _Operand(reg, parts)
+    start, step, stop = (parts[0], 1, parts[1]) if len(parts) == 2 else parts[:3]
+    if step == 0:
+        toks.fail(reg, "a range step must be positive")
+    return _Operand(reg, list(range(start, stop + 1, step)))
+
+
+def _record_measures(p, toks, qubits, clbits, at):
+    if len(qubits) != len(clbits):
+        toks.fail(at, f"measuring {len(qubits)} qubits into {len(clbits)} bits")
+    p.out.extend(("measure", q, c) for q, c in zip(qubits, clbits))
+
+
+def _measure_arrow(p, toks):
+    at = toks.take()
+    qubits = p.resolve(toks, _operand(toks), True)
+    if not toks.accept("->"):
+        toks.fail(at, "a measurement must store its result (`measure q -> c;` or `c = measure q;`)")
+    clbits = p.resolve(toks, _operand(toks), False)
+    toks.require(";")
+    _record_measures(p, toks, qubits, clbits, at)
+
+
+def _assigned_measure(p, toks):
+    at = toks.peek()
+    clbits = p.resolve(toks, _operand(toks), False)
+    toks.require("=")
+    kw = toks.name()
+    if kw.text != "measure":
+        toks.fail(kw, "assigning classical values other than measurements is not supported")
+    qubits = p.resolve(toks, _operand(toks), True)
+    toks.require(";")
+    _record_measures(p, toks, qubits, clbits, at)
+
+
+def _reset(p, toks):
+    toks.take()
+    qubits = p.resolve(toks, _operand(toks), True)
+    toks.require(";")
+    p.out.extend(("reset", q) for q in qubits)
+
+
+def _barrier(p, toks):
+    toks.take()
+    qubits = []
+    while not toks.at_symbol(";") and not toks.at_end():
+        qubits.extend(p.resolve(toks, _operand(toks), True))
+        toks.accept(",")
+    toks.require(";")
+    p.out.append(("barrier", qubits or list(range(p.qubits))))
+
+
+def _global_phase(p, toks):
+    toks.skip_past(";")
+
+
+def _modifiers(toks: _Tokens) -> list:
+    """Leading `inv @`, `pow(e) @`, `ctrl(n) @`, `negctrl(n) @`."""
+    mods = []
+    while toks.peek().kind == "name" and toks.peek().text in _MODIFIERS:
+        mark = toks.at
+        tok = toks.take()
+        arg = None
+        if toks.accept("("):
+            arg = _expression(toks)
+            toks.require(")")
+        if not toks.accept("@"):
+            toks.at = mark  # a gate that happens to share the name
+            break
+        if tok.text == "inv":
+            mods.append(("inv",))
+        elif tok.text == "pow":
+            if arg is None:
+                toks.fail(tok, "`pow` needs an exponent")
+            mods.append(("pow", arg, tok))
         else:
-            self.err(at, f"a condition on `{name}`, a register of {size} bits, is not supported: only one bit can "
-                         f"be tested (`if ({name}[k])`)")
-        wanted = True
-        if self.is_sym("==") or self.is_sym("!="):
-            equal = self.next().value == "=="
-            t = self.next()
-            if t.kind == "num" and t.value in (0.0, 1.0):
-                value = t.value == 1.0
-            elif t.kind == "id" and t.value in ("true", "false"):
-                value = t.value == "true"
-            else:
-                self.err(t, f"a bit can only be compared with 0, 1, true or false, not {_describe(t)}")
-            wanted = value == equal
-        return clbit, wanted != negated
+            count = 1
+            if arg is not None:
+                x = arg({})
+                if x < 1 or x != int(x):
+                    toks.fail(tok, "a control count must be a positive integer")
+                count = int(x)
+            mods.append((tok.text, count))
+    return mods
 
-    def pauli_body(self, at):
-        block = self.is_sym("{")
-        if block:
-            self.next()
-        start = len(self.p.ins)
-        while True:
-            if block and self.is_sym("}"):
-                self.next()
-                break
-            t = self.peek()
-            if t.kind == "id" and t.value == "barrier":
-                while not self.is_sym(";") and self.peek().kind != "end":
-                    self.next()
-                self.expect(";")
-            elif t.kind == "id" and (t.value in ("measure", "reset", "if", "gate") or t.value in _UNSUPPORTED):
-                self.err(t, f"`{t.value}` inside `if` is not supported: an `if` body can only apply Pauli gates "
-                            "(x, y, z, id)")
-            elif t.kind == "id":
-                call = self.call()
-                self.expect(";")
-                before = len(self.p.ins)
-                self.top_level_call(call)
-                if not all(i[0] == "gate" and i[1].name in ("id", "x", "y", "z") for i in self.p.ins[before:]):
-                    self.err(t, f"`{call.name}` inside `if` is not supported: an `if` body can only apply Pauli "
-                                "gates (x, y, z, id), which run as classical feedback")
-            elif t.kind == "end":
-                self.err(at, "unterminated `if` block")
-            else:
-                self.err(t, f"expected a gate call, found {_describe(t)}")
-            if not block:
-                break
-        body = {}
-        for ins in self.p.ins[start:]:
-            if ins[0] == "gate":
-                bits = {"x": 1, "z": 2, "y": 3}.get(ins[1].name, 0)
-                body[ins[2][0]] = body.get(ins[2][0], 0) ^ bits
-        del self.p.ins[start:]
-        return body
+
+def _application(toks: _Tokens) -> _Application:
+    """[modifiers] name [(expr, ...)] operand, ..."""
+    mods = _modifiers(toks)
+    name = toks.name()
+    params = []
+    if toks.accept("("):
+        if not toks.at_symbol(")"):
+            params.append(_expression(toks))
+            while toks.accept(","):
+                params.append(_expression(toks))
+        toks.require(")")
+    operands = []
+    while not (toks.at_symbol(";") or toks.at_symbol("}") or toks.at_end()):
+        operands.append(_operand(toks))
+        if not toks.accept(","):
+            break
+    return _Application(mods, name, params, operands)
+
+
+def _definition(p, toks):
+    toks.take()
+    name = toks.name()
+    params = []
+    if toks.accept("("):
+        while not toks.at_symbol(")"):
+            params.append(toks.name().text)
+            toks.accept(",")
+        toks.require(")")
+    qubits = []
+    while not toks.at_symbol("{"):
+        qubits.append(toks.name().text)
+        toks.accept(",")
+    toks.require("{")
+    body = []
+    while not toks.at_symbol("}"):
+        if toks.at_end():
+            toks.fail(name, f"unterminated definition of `{name.text}`")
+        if toks.at_name("barrier"):
+            toks.skip_past(";")
+            continue
+        app = _application(toks)
+        if any(o.indices is not None for o in app.operands):
+            toks.fail(name, f"the body of `{name.text}` can only use its own qubit names")
+        body.append(app)
+        toks.require(";")
+    toks.require("}")
+    p.definitions[name.text] = _Definition(params, qubits, body)
+
+
+def _condition(p, toks) -> tuple:
+    """(classical bit, value that takes the `if` branch)."""
+    negated = False
+    while toks.accept("!"):
+        negated = not negated
+    reg = toks.name()
+    if reg.text not in p.cregs:
+        toks.fail(reg, f"unknown classical bit register `{reg.text}` in a condition")
+    first, size = p.cregs[reg.text]
+    if toks.accept("["):
+        index = toks.index()
+        toks.require("]")
+        if index >= size:
+            toks.fail(reg, f"index {index} is out of range for `{reg.text}` of size {size}")
+        clbit = first + index
+    elif size == 1:
+        clbit = first
+    else:
+        toks.fail(reg, f"a condition on `{reg.text}`, a register of {size} bits, is not supported: only one bit can "
+                       f"be tested (`if ({reg.text}[k])`)")
+    wanted = True
+    if toks.at_symbol("==") or toks.at_symbol("!="):
+        equal = toks.take().text == "=="
+        v = toks.take()
+        if v.kind == "number" and v.number in (0.0, 1.0):
+            value = v.number == 1.0
+        elif v.kind == "name" and v.text in ("true", "false"):
+            value = v.text == "true"
+        else:
+            toks.fail(v, f"a bit can only be compared with 0, 1, true or false, not {toks.describe(v)}")
+        wanted = value == equal
+    return clbit, wanted != negated
+
+
+def _pauli_branch(p, toks, at) -> dict:
+    """An `if` body: qubit -> Pauli as X/Z bits (products up to phase)."""
+    block = toks.accept("{")
+    paulis: dict = {}
+    while True:
+        if block and toks.accept("}"):
+            break
+        tok = toks.peek()
+        if tok.kind == "end":
+            toks.fail(at, "unterminated `if` block")
+        if tok.kind != "name":
+            toks.fail(tok, f"expected a gate call, found {toks.describe(tok)}")
+        if tok.text == "barrier":
+            toks.skip_past(";")
+        elif tok.text in ("measure", "reset", "if", "gate") or tok.text in _REFUSED:
+            toks.fail(tok, f"`{tok.text}` inside `if` is not supported: an `if` body can only apply Pauli gates "
+                           "(x, y, z, id)")
+        else:
+            app = _application(toks)
+            toks.require(";")
+            mark = len(p.out)
+            p.apply(toks, app)
+            emitted, p.out[mark:] = p.out[mark:], []
+            for ins in emitted:
+                if not (ins[0] == "gate" and ins[1].name in ("id", "x", "y", "z")):
+                    toks.fail(tok, f"`{app.name.text}` inside `if` is not supported: an `if` body can only apply "
+                                   "Pauli gates (x, y, z, id), which run as classical feedback")
+                q = ins[2][0]
+                paulis[q] = paulis.get(q, 0) ^ _PAULI_BITS.get(ins[1].name, 0)
+        if not block:
+            break
+    return paulis
+
+
+def _conditional(p, toks):
+    """`if (bit) body [else body]` with Pauli bodies: the else-branch's
+    Paulis always, then the difference of the branches as feedback on the
+    bit (a Pauli applied when the bit reads 1)."""
+    at = toks.take()
+    toks.require("(")
+    clbit, wanted = _condition(p, toks)
+    toks.require(")")
+    taken = _pauli_branch(p, toks, at)
+    other = {}
+    if toks.at_name("else"):
+        toks.take()
+        other = _pauli_branch(p, toks, at)
+    on_one, on_zero = (taken, other) if wanted else (other, taken)
+    for q, bits in on_zero.items():
+        if bits:
+            p.out.append(("gate", Gate(_PAULI_LETTER[bits].lower()), [q]))
+    for q in sorted(set(on_one) | set(on_zero)):
+        flip = on_one.get(q, 0) ^ on_zero.get(q, 0)
+        if flip:
+            p.out.append(("feedback", _PAULI_LETTER[flip], q, clbit))
+
+
+_STATEMENTS = {"OPENQASM": _version, "include": _include, "qreg": _register_v2, "creg": _register_v2,
+               "qubit": _register_v3, "bit": _register_v3, "gate": _definition, "if": _conditional,
+               "measure": _measure_arrow, "reset": _reset, "barrier": _barrier, "gphase": _global_phase}
+
+_prelude = _Program()
+_prelude.read(_PRELUDE)
 
 
 def parse(source: str) -> Circuit:
     """An OpenQASM 2 or 3 program as a circuit; qubits and classical bits
     are numbered in declaration order across registers."""
-    prelude = _Parser(_lex(_PRELUDE), _Program())
-    prelude.program()
-    parser = _Parser(_lex(source), _Program(gates=dict(prelude.p.gates)))
-    parser.program()
-    p = parser.p
+    p = _Program(_prelude.definitions)
+    p.read(source)
     c = Circuit(p.qubits, p.clbits)
-    c._instructions.extend(p.ins)
+    c._instructions.extend(p.out)
     return c

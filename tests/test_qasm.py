@@ -225,3 +225,32 @@ def test_run_result_has_the_binding_fields():
     r = RunResult(counts={"00": 3, "11": 5})
     assert (r.backend, r.fidelity, r.max_bond_dimension, r.peak_active_qubits) == ("statevector", None, None, None)
     assert repr(r) == 'RunResult(backend="statevector", 2 outcomes)'
+
+
+def test_expression_grammar_and_lexical_forms():
+    """Precedence as the reference's grammar (src/qasm.rs:1290-1345): + -
+    below * /, then right-associative ^ / **, and a sign binding tighter
+    than all of them (-2^2 = 4); numbers with underscores and exponents;
+    comments of both forms; unicode constants."""
+    cases = {"-2^2": 4.0, "2^3^2": 2.0 ** 9, "2**-1": 0.5, "1+2*3": 7.0, "(1+2)*3": 9.0, "8/2/2": 2.0,
+             "1_000e-3": 1.0, ".5": 0.5, "-pi/2 + π/2": 0.0, "sqrt(4)*cos(0)": 2.0, "2*-3": -6.0, "tau - 2*pi": 0.0}
+    for text, want in cases.items():
+        c = parse(f"OPENQASM 3.0;\nqubit q; // a comment\n/* block\ncomment */ rz({text}) q;")
+        (kind, gate, qubits), = c._instructions
+        assert gate.name == "rz" and gate.params[0] == pytest.approx(want, abs=1e-15), text
+    for program, message in [("OPENQASM 3.0;\n/* open", "unterminated comment"),
+                             ('OPENQASM 3.0;\ninclude "x', "unterminated string"),
+                             ("OPENQASM 3.0;\nqubit q;\nrz(1 # 2) q;", "unexpected character `#`"),
+                             ("OPENQASM 3.0;\nqubit q;\nrz(foo(1)) q;", "unknown function `foo`"),
+                             ("OPENQASM 3.0;\nqubit q;\nrz(1 +) q;", "expected an expression"),
+                             ("OPENQASM 5.0;", "only OpenQASM 2 and 3"),
+                             ("OPENQASM 3.0;\nqubit q;\nqubit q;", "already declared")]:
+        with pytest.raises(QasmError, match=message):
+            parse(program)
+
+
+def test_register_named_like_a_gate_and_gate_named_like_a_modifier():
+    c = parse("OPENQASM 3.0;\nqubit[2] q;\nbit[2] x;\nx q[0];\nx = measure q;\n"
+              "gate inv a { h a; }\ninv q[1];")
+    assert [i[0] for i in c._instructions] == ["gate", "measure", "measure", "gate"]
+    assert c._instructions[0][1].name == "x" and c._instructions[-1][1].name == "h"
