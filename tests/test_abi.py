@@ -91,3 +91,17 @@ def test_one_pass_gate_packing_equals_packing_the_ops():
                                   b._ops[f] - np.uint64(getattr(b, base).ctypes.data)), f
         for f in ("num_targets", "num_controls"):
             assert np.array_equal(a._ops[f], b._ops[f]), f
+
+
+def test_rust_bindings_mirror_the_header():
+    """rust/src/gpu/ffi.rs (the seam a qvd maintainer adds; not compiled in
+    this image, which has no Rust toolchain) declares every function of the
+    header and the same struct fields in the same order."""
+    text = open(os.path.join(ROOT, "rust", "src", "gpu", "ffi.rs")).read()
+    assert set(re.findall(r"pub fn (qvdg_[a-z0-9_]+)\(", text)) == declared_functions()
+    header = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "qvdg.h")).read(), flags=re.S)
+    for body, name in re.findall(r"typedef struct \{(.*?)\} (\w+);", header, flags=re.S):
+        c_fields = re.findall(r"(\w+);", body)
+        m = re.search(r"pub struct " + name + r" \{(.*?)\n\}", text, flags=re.S)
+        assert m, name
+        assert re.findall(r"pub (\w+):", m.group(1)) == c_fields, name
