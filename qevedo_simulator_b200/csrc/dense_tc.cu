@@ -49,8 +49,10 @@ namespace {
 
 constexpr int kThreads = 512;
 constexpr uint32_t kIterAmps = 8192;
-constexpr uint32_t kPartBytes = kIterAmps * 2 * 2;  // one bf16 part (hi or lo) of an iteration's A
-constexpr uint32_t kTmemCols = 256;                 // two buffers of 128 fp32 columns
+// Tensor memory of the direct kernel: two product buffers of 128 fp32
+// columns (D), then two operand buffers of 128 columns (A, bf16 pairs).
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kTmemA = 256;  // first A column
 
 // One iteration's products, issued by one thread: for each of the T blocks
 // of 128 groups, D = A_hi B_hi + A_hi B_lo + A_lo B_hi into tensor-memory
@@ -75,6 +77,37 @@ __device__ __forceinline__ void issue_products(const unsigned char* ah, const un
 #pragma unroll
       for (uint32_t s = 0; s < kd / 16; ++s) {
         umma_bf16(d, a0 + 16 * s, b0 + 16 * s, idesc, acc);
+        acc = 1;
+      }
+    }
+  }
+  umma_commit(bar);
+}
+
+// The direct kernel's products, A in tensor memory: for each of the T
+// blocks of 128 groups, D = A_hi B_hi + A_hi B_lo + A_lo B_hi into columns
+// `dcol` + t * 2^(K+1), A_hi of block t at `acol` + t * 2^(K+1) and A_lo
+// 2^K columns after it (each 16-element K slice is 8 columns), B in shared
+// memory; then one commit to `bar`.
+template <int K, uint32_t T = 4 / ((1u << K) / 16)>
+__device__ __forceinline__ void issue_products_tmem_a(uint32_t acol, const unsigned char* bmat, uint32_t dcol,
+                                                      uint32_t bar) {
+  constexpr uint32_t D = 1u << K, kd = 2u * D;
+  constexpr uint32_t SBO = kd * 16, BPART = kd * kd * 2;
+  tc_fence_after();
+  const uint32_t idesc = umma_idesc(kd);
+  const uint64_t dbh = umma_desc(smem_addr(bmat), 128, SBO), dbl = umma_desc(smem_addr(bmat + BPART), 128, SBO);
+#pragma unroll
+  for (uint32_t t = 0; t < T; ++t) {
+    const uint32_t d = dcol + t * kd;
+    uint32_t acc = 0;
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      const uint32_t a0 = acol + t * kd + (p == 2 ? D : 0);
+      const uint64_t b0 = p == 1 ? dbl : dbh;
+#pragma unroll
+      for (uint32_t s = 0; s < kd / 16; ++s) {
+        umma_bf16_tmem_a(d, a0 + 8 * s, b0 + 16 * s, idesc, acc);
         acc = 1;
       }
     }
@@ -119,6 +152,30 @@ __device__ __forceinline__ void write_a8(const float2* x, unsigned char* ah, uns
   *reinterpret_cast<uint4*>(al + row + cim) = l;
 }
 
+// Split 8 members (x[0..7], members 16 * chunk + 8 * q + i) of one group
+// into bf16 parts in this thread's tensor-memory lane: `acol` is the lane
+// base plus the block's first A column; real parts go to the columns of K
+// elements 16 * chunk + 8 * q.., imaginary parts 2^K elements later, low
+// parts 2^K columns after the high ones.
+template <int K>
+__device__ __forceinline__ void write_a8_tmem(const float2* x, uint32_t acol, uint32_t chunk, int q) {
+  constexpr uint32_t D = 1u << K;
+  float re[8], im[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    re[i] = x[i].x;
+    im[i] = x[i].y;
+  }
+  uint4 h, l;
+  const uint32_t cre = acol + 8 * chunk + 4 * q, cim = cre + D / 2;
+  split8(re, h, l);
+  tmem_st4(cre, h);
+  tmem_st4(cre + D, l);
+  split8(im, h, l);
+  tmem_st4(cim, h);
+  tmem_st4(cim + D, l);
+}
+
 template <int K, int VW>
 __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ psi, const DenseTcGeom g,
                                                           const uint8_t* __restrict__ bmats,
@@ -127,15 +184,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ p
   constexpr uint32_t P = D / 16;     // threads per group
   constexpr uint32_t T = 4 / P;      // blocks of 128 groups per iteration
   constexpr uint32_t GPI = T * 128;  // groups per iteration
-  constexpr uint32_t SBO = kd * 16;
-  constexpr uint32_t BLOCK = 128 * kd * 2;  // bytes of one block's A part
   constexpr uint32_t BPART = kd * kd * 2;   // bytes of one part of B
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ uint32_t tmem_slot;
   __shared__ uint8_t fixed[40];
-  unsigned char* abuf = smem;                  // buffer b: hi at 2b * kPartBytes, lo right after
-  unsigned char* bmat = smem + 4 * kPartBytes;  // B hi, then B lo
+  unsigned char* bmat = smem;  // B hi, then B lo
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t wg = uint32_t(tid) >> 7, r = uint32_t(tid) & 127u;
   const uint32_t blk = wg / P, chunk = wg % P;
@@ -203,25 +257,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ p
       for (int i = 0; i < 16; ++i) x[i] = ld_early8(psi + base + off_lo[i]);
     }
   };
-  const uint32_t row = blk * BLOCK + (r >> 3) * SBO + (r & 7) * 16;
+  // Thread (w, r) owns tensor-memory lane r: its warp's quarter of the
+  // lanes is r / 32 = w % 4.
   const uint32_t lanes = (uint32_t(warp & 3) * 32u) << 16;
   int failed = 0;
-  // One step: iteration li's members into A and its products issued (the
-  // registers then take the loads of iteration li + 2), and the previous
-  // iteration read back and stored. Returns whether another step follows.
+  // One step: iteration li's members into A (tensor memory) and its
+  // products issued (the registers then take the loads of iteration
+  // li + 2), and the previous iteration read back and stored. Returns
+  // whether another step follows.
   auto step = [&](uint64_t li, float2 (&x)[16]) -> bool {
     const uint32_t b = uint32_t(li & 1);
-    unsigned char* ah = abuf + b * 2 * kPartBytes;
-    unsigned char* al = ah + kPartBytes;
+    const uint32_t acol = kTmemA + b * 128;
     if (li < my_iters) {
-      write_a8<K>(x, ah, al, row, chunk, 0);
-      write_a8<K>(x + 8, ah, al, row, chunk, 1);
+      write_a8_tmem<K>(x, tmem + lanes + acol + blk * kd, chunk, 0);
+      write_a8_tmem<K>(x + 8, tmem + lanes + acol + blk * kd, chunk, 1);
       if (li + 2 < my_iters) load(x, next_load());
-      fence_async_shared();
+      tmem_wait_st();
     }
     tc_fence_before();
     if (__syncthreads_or(failed)) return false;
-    if (li < my_iters && tid == 0) issue_products<K>(ah, al, bmat, tmem + b * 128, smem_addr(&bar[b]));
+    if (li < my_iters && tid == 0) issue_products_tmem_a<K>(tmem + acol, bmat, tmem + b * 128, smem_addr(&bar[b]));
     if (li > 0) {
       const uint32_t pb = b ^ 1u;
       const uint32_t parity = uint32_t(((li - 1) >> 1) & 1);
@@ -474,10 +529,17 @@ __global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_
 
 template <int K, int VW>
 void launch_k(StateImpl& s, const DenseTcGeom& g, const uint8_t* bmats) {
-  const size_t smem = 4 * size_t(kPartBytes) + tc_gate_bytes(K);
+  const size_t smem = tc_gate_bytes(K);
   static bool configured = false;  // per instantiation
   if (!configured) {
     QVDG_CUDA(cudaFuncSetAttribute(k_dense_tc<K, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    // The rest of the unified L1 / shared storage as L1, which holds the
+    // global loads in flight.
+    int dev = 0, smem_sm = 0;
+    QVDG_CUDA(cudaGetDevice(&dev));
+    QVDG_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    const int percent = int(std::min<size_t>(100, (100 * (smem + 4096) + size_t(smem_sm) - 1) / size_t(smem_sm)));
+    QVDG_CUDA(cudaFuncSetAttribute(k_dense_tc<K, VW>, cudaFuncAttributePreferredSharedMemoryCarveout, percent));
     configured = true;
   }
   const unsigned grid = unsigned(std::min<uint64_t>(g.iters, uint64_t(s.sms)));
