@@ -432,6 +432,7 @@ def run_ours(args, rank: int, world: int):
                       "chosen_by": "learned cost model, judged against the greedy default" if fixed is None
                       else "--plan", "candidates_s": {k: round(v, 5) for k, v in candidates.items()},
                       "pass_ms": [round(float(x) * 1e3, 3) for x in pass_t[-1]],
+                      "pass_kind": [int(k) for k in pass_k[-1]],
                       "zero_start": {"passes": int(np.sum(pass_k[-1] == 4)),
                                      "ms": round(float(np.sum(pass_t[-1][pass_k[-1] == 4])) * 1e3, 3),
                                      "bytes": float(np.sum(pass_b[-1][pass_k[-1] == 4]))}},

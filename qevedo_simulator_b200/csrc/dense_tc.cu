@@ -18,9 +18,12 @@
 // (consecutive threads take consecutive groups, so a warp's loads of one
 // member are contiguous when bit 0 is free; with a target on bit 0 the
 // members pair into 16-byte accesses, with targets on bits 0 and 1 into
-// 32-byte ones), writes their bf16 parts into one of
-// two A buffers, and, once TMEM lane r holds the block's products, reads
-// its 16 members back and stores them where they came from. The loads of
+// 32-byte ones), writes their bf16 parts into its lane r of one of two A
+// buffers in tensor memory (tcgen05.st; the products read A from there and
+// only the gate B sits in shared memory, which keeps the L1 / shared-memory
+// path free for the global loads and stores), and, once TMEM lane r holds
+// the block's products, reads its 16 members back and stores them where
+// they came from. The loads of
 // iteration i + 1 are issued before iteration i's products, and iteration
 // i's read-back runs during iteration i + 1, so HBM traffic, the bf16 split,
 // the tensor cores and the stores overlap. Every wait on an MMA completion
@@ -53,36 +56,6 @@ constexpr uint32_t kIterAmps = 8192;
 // columns (D), then two operand buffers of 128 columns (A, bf16 pairs).
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kTmemA = 256;  // first A column
-
-// One iteration's products, issued by one thread: for each of the T blocks
-// of 128 groups, D = A_hi B_hi + A_hi B_lo + A_lo B_hi into tensor-memory
-// columns `cols` + t * 2^(K+1), then one commit to `bar`.
-template <int K, uint32_t T = 4 / ((1u << K) / 16)>
-__device__ __forceinline__ void issue_products(const unsigned char* ah, const unsigned char* al,
-                                               const unsigned char* bmat, uint32_t cols, uint32_t bar) {
-  constexpr uint32_t D = 1u << K, kd = 2u * D;
-  constexpr uint32_t SBO = kd * 16, BLOCK = 128 * kd * 2, BPART = kd * kd * 2;
-  tc_fence_after();
-  const uint32_t idesc = umma_idesc(kd);
-  const uint64_t dah = umma_desc(smem_addr(ah), 128, SBO), dal = umma_desc(smem_addr(al), 128, SBO);
-  const uint64_t dbh = umma_desc(smem_addr(bmat), 128, SBO), dbl = umma_desc(smem_addr(bmat + BPART), 128, SBO);
-#pragma unroll
-  for (uint32_t t = 0; t < T; ++t) {
-    const uint32_t d = cols + t * kd;
-    const uint64_t boff = (t * BLOCK) >> 4;
-    uint32_t acc = 0;
-#pragma unroll
-    for (int p = 0; p < 3; ++p) {
-      const uint64_t a0 = (p == 2 ? dal : dah) + boff, b0 = p == 1 ? dbl : dbh;
-#pragma unroll
-      for (uint32_t s = 0; s < kd / 16; ++s) {
-        umma_bf16(d, a0 + 16 * s, b0 + 16 * s, idesc, acc);
-        acc = 1;
-      }
-    }
-  }
-  umma_commit(bar);
-}
 
 // The direct kernel's products, A in tensor memory: for each of the T
 // blocks of 128 groups, D = A_hi B_hi + A_hi B_lo + A_lo B_hi into columns
@@ -128,28 +101,6 @@ __device__ __forceinline__ bool wait_products(uint32_t bar, uint32_t parity) {
   bool done = mbar_try_wait(bar, parity);
   while (!done && clock64() - t0 <= kWaitCycles) done = mbar_try_wait(bar, parity);
   return done;
-}
-
-// Split 8 members (x[0..7], members 16 * chunk + 8 * q + i) of one group
-// into bf16 parts at row offset `row` of A.
-template <int K>
-__device__ __forceinline__ void write_a8(const float2* x, unsigned char* ah, unsigned char* al, uint32_t row,
-                                         uint32_t chunk, int q) {
-  constexpr uint32_t D = 1u << K;
-  float re[8], im[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    re[i] = x[i].x;
-    im[i] = x[i].y;
-  }
-  uint4 h, l;
-  const uint32_t cre = (2 * chunk + q) * 128, cim = (D / 8 + 2 * chunk + q) * 128;
-  split8(re, h, l);
-  *reinterpret_cast<uint4*>(ah + row + cre) = h;
-  *reinterpret_cast<uint4*>(al + row + cre) = l;
-  split8(im, h, l);
-  *reinterpret_cast<uint4*>(ah + row + cim) = h;
-  *reinterpret_cast<uint4*>(al + row + cim) = l;
 }
 
 // Split 8 members (x[0..7], members 16 * chunk + 8 * q + i) of one group
@@ -335,12 +286,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc(float2* __restrict__ p
 // seven lowest free bits, bit 0 always among them, so a tile is contiguous
 // runs of at least 128 amplitudes). A tile is loaded with coalesced 16-byte
 // accesses (two tiles ahead, in registers) into the stage S, gathered per
-// group from S into A, multiplied, written back into S by the owning
-// threads and stored with coalesced 16-byte accesses. With two A and
-// tensor-memory buffers (NB = 2) a tile's products run while the previous
-// tile is read back and stored. Small CTAs let several run per SM (four for
-// K = 4, two for K = 5), so one CTA's barriers overlap another's memory
-// traffic. S position of tile element e: e ^ s(e), s(e) = (e >> 4 ^ e >> 8
+// group from S into A (tensor memory, as in the direct kernel), multiplied,
+// written back into S by the owning threads and stored with coalesced
+// 16-byte accesses. With two A and product buffers (NB = 2) a tile's
+// products run while the previous tile is read back and stored. Small CTAs
+// let several run per SM (four for K = 4, two for K = 5, as many as tensor
+// memory holds), so one CTA's barriers overlap another's memory traffic. S position of tile element e: e ^ s(e), s(e) = (e >> 4 ^ e >> 8
 // ^ e >> 12) & 15, which keeps element pairs (2v, 2v + 1) in one 16-byte
 // slot (swapped when s(e) is odd) and spreads the group-parallel accesses
 // over the banks.
@@ -351,6 +302,13 @@ constexpr int tile_threads() {
   return 128 * (1 << K) / 16;
 }
 
+// Tensor-memory columns of one staged CTA: NB product buffers and NB A
+// operand buffers of 2^(K+1) columns each (a power of two, at least 32).
+template <int K, int NB>
+constexpr uint32_t tile_tmem_cols() {
+  return 2u * NB * (2u << K) < 32 ? 32 : 2u * NB * (2u << K);
+}
+
 template <int K, int NB>
 __global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_dense_tc_tile(float2* __restrict__ psi,
                                                                      const DenseTcTileGeom g,
@@ -359,8 +317,6 @@ __global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_
   constexpr uint32_t D = 1u << K, kd = 2u * D;
   constexpr int NT = tile_threads<K>();      // threads: 16 members of one group each
   constexpr uint32_t TILE = 128 * D;         // amplitudes per tile
-  constexpr uint32_t PART = TILE * 2 * 2;    // bytes of one bf16 part of A
-  constexpr uint32_t SBO = kd * 16;
   constexpr uint32_t BPART = kd * kd * 2;
   constexpr int TB = 7 + K;                  // tile bits
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -368,9 +324,8 @@ __global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_
   __shared__ uint32_t tmem_slot;
   __shared__ uint8_t tile[16];
   __shared__ uint64_t dep_hi[8];
-  float2* stage = reinterpret_cast<float2*>(smem);             // TILE complex64
-  unsigned char* abuf = smem + size_t(TILE) * sizeof(float2);  // NB x (A hi, A lo)
-  unsigned char* bmat = abuf + NB * 2 * PART;                  // B hi, then B lo
+  float2* stage = reinterpret_cast<float2*>(smem);                          // TILE complex64
+  unsigned char* bmat = smem + size_t(TILE) * sizeof(float2);               // B hi, then B lo
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t r = uint32_t(tid) & 127u, chunk = uint32_t(tid) >> 7;
 
@@ -390,7 +345,8 @@ __global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[1])));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  constexpr uint32_t kCols = NB * kd < 32 ? 32 : NB * kd;  // power of two, at least 32
+  // NB product buffers (D) of kd columns, then NB operand buffers (A).
+  constexpr uint32_t kCols = tile_tmem_cols<K, NB>();
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
                  "r"(kCols));
@@ -435,7 +391,6 @@ __global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_
 #pragma unroll
     for (int j = 0; j < 8; ++j) x[j] = ld_early(psi + (base | dep_hi[j]));
   };
-  const uint32_t row = (r >> 3) * SBO + (r & 7) * 16;
   const uint32_t lanes = (uint32_t(warp & 3) * 32u) << 16;
   int failed = 0;
   // One step: tile li into the stage and gathered into A, its products
@@ -445,8 +400,7 @@ __global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_
   auto step = [&](uint64_t li, float4 (&x)[8]) -> bool {
     const bool have = li < my_iters;
     const uint32_t b = NB == 2 ? uint32_t(li & 1) : 0u;
-    unsigned char* ah = abuf + b * 2 * PART;
-    unsigned char* al = ah + PART;
+    const uint32_t acol = NB * kd + b * kd;  // this tile's A columns
     if (have) {
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
@@ -464,13 +418,13 @@ __global__ void __launch_bounds__(tile_threads<K>(), 512 / tile_threads<K>()) k_
         float2 m[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) m[i] = stage[stage_pos(member(8 * q + i))];
-        write_a8<K>(m, ah, al, row, chunk, q);
+        write_a8_tmem<K>(m, tmem + lanes + acol, chunk, q);
       }
-      fence_async_shared();
+      tmem_wait_st();
     }
     tc_fence_before();
     if (__syncthreads_or(failed)) return false;
-    if (have && tid == 0) issue_products<K, 1>(ah, al, bmat, tmem + b * kd, smem_addr(&bar[b]));
+    if (have && tid == 0) issue_products_tmem_a<K, 1>(tmem + acol, bmat, tmem + b * kd, smem_addr(&bar[b]));
     const bool back = NB == 2 ? li > 0 : have;
     if (back) {
       const uint64_t rl = NB == 2 ? li - 1 : li;
@@ -547,12 +501,13 @@ void launch_k(StateImpl& s, const DenseTcGeom& g, const uint8_t* bmats) {
   QVDG_LAUNCH_CHECK();
 }
 
-// Two A and tensor-memory buffers where they fit in shared memory (K <= 5).
+// Two A and product buffers in tensor memory: a tile's products run while
+// the previous tile is read back and stored.
 template <int K>
 void launch_tile(StateImpl& s, const DenseTcTileGeom& g, const uint8_t* bmats) {
-  constexpr int NB = K <= 5 ? 2 : 1;
+  constexpr int NB = 2;
   constexpr int NT = tile_threads<K>();
-  const size_t smem = (size_t(128) << K) * (sizeof(float2) + NB * 8) + tc_gate_bytes(K);
+  const size_t smem = (size_t(128) << K) * sizeof(float2) + tc_gate_bytes(K);
   static int per_sm = 0;  // per instantiation
   if (!per_sm) {
     QVDG_CUDA(cudaFuncSetAttribute(k_dense_tc_tile<K, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -571,7 +526,8 @@ void launch_tile(StateImpl& s, const DenseTcTileGeom& g, const uint8_t* bmats) {
     const int regs = (fa.numRegs + 7) / 8 * 8;
     const int by_smem = smem_sm / int(smem + fa.sharedSizeBytes + 1024);
     const int by_regs = regs_sm / (regs * NT);
-    per_sm = std::max(1, std::min({by_smem, by_regs, 2048 / NT}));
+    const int by_tmem = int(512 / tile_tmem_cols<K, NB>());
+    per_sm = std::max(1, std::min({by_smem, by_regs, by_tmem, 2048 / NT}));
   }
   const unsigned grid = unsigned(std::min<uint64_t>(g.iters, uint64_t(s.sms) * uint64_t(per_sm)));
   k_dense_tc_tile<K, NB><<<grid, NT, smem, s.stream>>>(static_cast<float2*>(s.amp), g, bmats, s.status);
