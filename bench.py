@@ -51,7 +51,8 @@ TRAFFIC_BYTES_PER_AMP = {0: (536.9e6 + 476.7e6) / 2 ** 26, 2: (537.0e6 + 476.5e6
                          3: (536.9e6 + 477.6e6) / 2 ** 26}
 KERNEL_OF_KIND = {0: "k_dense<float,K,...> (plain fused-gate pass, CUDA cores)",
                   2: "k_dense_tc<K,VW> (plain fused-gate pass, tensor cores)",
-                  3: "k_dense_tc_tile<K,NB> (plain fused-gate pass on bits 1-3, tensor cores)"}
+                  3: "k_dense_tc_tile<K,NB> (plain fused-gate pass on bits 1-3, tensor cores)",
+                  5: "k_dense_tc_pair<VW1,VW2> (two fused 6-qubit gates per pass, tensor cores)"}
 ROWS, COLS, DEPTH, SEED = 5, 6, 20, 2024
 SHOTS = 1000
 
@@ -361,7 +362,7 @@ def run_ours(args, rank: int, world: int):
     byt = np.concatenate(pass_b)
     kind = np.concatenate(pass_k)
     peaks = measured_peaks()
-    dom = max((0, 1, 2, 3), key=lambda k: sec[kind == k].sum())
+    dom = max((0, 1, 2, 3, 5), key=lambda k: sec[kind == k].sum())
     dsec, dbyt = sec[kind == dom], byt[kind == dom]
     avg = float(dsec.mean())
     per_launch = float(dbyt.mean())
@@ -373,13 +374,13 @@ def run_ours(args, rank: int, world: int):
     else:
         kernel = "k_stage_reg<float> (register-blocked stage)"
     traffic = args.traffic
-    if traffic is None and dom != 1:
+    if traffic is None and dom in TRAFFIC_BYTES_PER_AMP:
         traffic = TRAFFIC_BYTES_PER_AMP[dom] * 2 ** n
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": kernel,
                 "peak_source": peaks["source"], "bytes_per_launch": per_launch, "avg_launch_s": avg,
                 "traffic_source": "ncu capture of the same kernel at 26 qubits, scaled by amplitudes"
-                if args.traffic is None and dom != 1 else ("--traffic" if args.traffic else None),
+                if args.traffic is None and dom in TRAFFIC_BYTES_PER_AMP else ("--traffic" if args.traffic else None),
                 "launches_per_step": int(dsec.size // max(1, args.steps))}
     # Whole run: the bytes every pass of a step moved (zero-start passes at
     # the share of the state they touch), over the step time.
@@ -393,7 +394,7 @@ def run_ours(args, rank: int, world: int):
     e2e = []
     st.set_pass_timing(False)  # the user's path records no per-pass events
     staged = bool(tuned_opts.staged)
-    math_name = {0: "fp32", 1: "tensor", 2: "gates"}[int(tuned_opts.math)]
+    math_name = {0: "fp32", 1: "tensor", 2: "gates", 3: "tensor_pairs"}[int(tuned_opts.math)]
     e2e_settings = None
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -647,6 +648,41 @@ def run_batch(args):
     print(json.dumps(out), flush=True)
 
 
+def costmodel_training() -> dict:
+    """What the committed cost model was trained on (its training report)."""
+    path = os.path.join(ROOT, "qevedo_simulator_b200", "data", "cost_model_report.json")
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        r = json.load(f)
+    return {k: r.get(k) for k in ("training_circuits", "train_qubits", "depth", "pass_rows",
+                                  "heldout_median_abs_log_err")}
+
+
+def run_costmodel(args):
+    """The learned planner against the greedy default on held-out circuits
+    the model never saw: config-4-style mixed circuits (Haar SU(2) layers,
+    CZ/CX/iSWAP at geometric qubit distance, phase gates, 1-3-control gates)
+    at --qubits (33 by default: 64 GiB complex64 states), seeded. Each
+    circuit runs the model's pick (ranked by predicted time, no measurement)
+    and the greedy default (fusion 4, staged: the reference's defaults) once
+    from |0...0>, timed on the device."""
+    from qevedo_simulator_b200 import costmodel, library
+
+    n = args.qubits
+    model = costmodel.CostModel.load()
+    circuits = [library.mixed_ops(n, depth, 9000 + i) for i, depth in enumerate((10, 16))]
+    rows = costmodel.evaluate(model, circuits, n, all_candidates=False)
+    pick = float(sum(r["pick_s"] for r in rows))
+    default = float(sum(r["default_s"] for r in rows))
+    out = {"metric": f"learned planner vs greedy default: device seconds over held-out {n}-qubit circuits",
+           "unit": "s", "higher_is_better": False, "value": pick, "greedy_default_s": default,
+           "speedup_over_default": default / pick, "circuits": rows,
+           "workload": f"{len(circuits)} mixed circuits, {n} qubits complex64, depths 10 and 16, seeds 9000+",
+           "model": costmodel_training()}
+    print(json.dumps(out), flush=True)
+
+
 def tuned_upload_bytes(ops) -> int:
     """Upper bound of the gate-program and matrix bytes a plan uploads per
     run (complex64 matrices plus a 96-byte descriptor per op)."""
@@ -660,10 +696,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--qubits", type=int, default=30)
-    ap.add_argument("--workload", choices=["grid", "qft", "precision", "batch"], default="grid",
-                    help="grid: the 30-qubit random-circuit benchmark (the bench line); qft and precision: the "
-                         "other configurations, one JSON line each")
-    ap.add_argument("--plan", nargs=3, metavar=("FUSION", "plain|staged", "fp32|tensor"), default=None,
+    ap.add_argument("--workload", choices=["grid", "qft", "precision", "batch", "costmodel"], default="grid",
+                    help="grid: the 30-qubit random-circuit benchmark (the bench line); qft, precision, batch, "
+                         "costmodel (use --qubits 33): the other configurations, one JSON line each")
+    ap.add_argument("--plan", nargs=3, metavar=("FUSION", "plain|staged", "fp32|tensor|tensor_pairs"), default=None,
                     help="run this plan instead of the learned planner's choice")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-check", action="store_true")
@@ -684,6 +720,9 @@ def main():
     elif args.workload == "batch":
         if rank == 0:
             run_batch(args)
+    elif args.workload == "costmodel":
+        if rank == 0:
+            run_costmodel(args)
     else:
         run_ours(args, rank, world)
 
