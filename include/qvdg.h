@@ -71,7 +71,7 @@ enum { QVDG_PLANNER_GREEDY = 0, QVDG_PLANNER_LEARNED = 1 };
  * real matrix products on the tensor cores, operands split into bf16 high and
  * low parts with fp32 accumulation (hi*hi + hi*lo + lo*hi, about 16
  * significant bits per product; diagonal and 1-2 qubit gates stay fp32). */
-enum { QVDG_MATH_FP32 = 0, QVDG_MATH_TENSOR = 1, QVDG_MATH_GATES = 2 };
+enum { QVDG_MATH_FP32 = 0, QVDG_MATH_TENSOR = 1, QVDG_MATH_GATES = 2, QVDG_MATH_TENSOR_PAIRS = 3 };
 
 /* Simulator options. Reference: simulator::Options, src/simulator.rs:37-66
  * (defaults max_fused_qubits = 4, region_bits = Some(14)). */
@@ -98,7 +98,10 @@ typedef struct {
    * 4-6 qubits in plain passes (staged = 0), run on the tensor cores as
    * split-bf16 products (hi*hi + hi*lo + lo*hi) accumulated in fp32.
    * QVDG_MATH_GATES: plain passes apply a fused group of 4-5 qubits member
-   * gate by member gate in registers instead of as its product matrix. */
+   * gate by member gate in registers instead of as its product matrix.
+   * QVDG_MATH_TENSOR_PAIRS (complex64, plain): as TENSOR, and two
+   * consecutive fused 6-qubit gates without controls share one pass over
+   * the state (the second applied to the first's output on chip). */
   uint32_t math;
 } qvdg_options;
 

@@ -46,7 +46,7 @@ class QvdgStats(ct.Structure):
         return out
 
 
-MATH_NAMES = {0: "fp32", 1: "tensor", 2: "gates"}
+MATH_NAMES = {0: "fp32", 1: "tensor", 2: "gates", 3: "tensor_pairs"}
 
 
 def settings_dict(o: QvdgOptions) -> dict:

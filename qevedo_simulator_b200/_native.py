@@ -151,7 +151,7 @@ def set_device(device: int):
     check(lib().qvdg_set_device(int(device)))
 
 
-MATH = {"fp32": 0, "tensor": 1, "gates": 2}
+MATH = {"fp32": 0, "tensor": 1, "gates": 2, "tensor_pairs": 3}
 PLANNERS = {"greedy": 0, "learned": 1}
 COST_MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "cost_model.npz")
 _models_registered = set()
@@ -218,7 +218,9 @@ def options(max_fused_qubits: int = 4, staged: bool = True, tile_qubits: int = 0
     `math="tensor"` runs fused dense gates on the tensor cores (complex64
     states only): 3-6 qubit gates inside staged tiles, 4-6 qubit gates as
     plain passes; `math="gates"` makes plain passes
-    apply a fused 4-5 qubit group gate by gate in registers."""
+    apply a fused 4-5 qubit group gate by gate in registers;
+    `math="tensor_pairs"` is "tensor" with two fused 6-qubit gates per plain
+    pass where they have no controls."""
     o = QvdgOptions()
     o.max_fused_qubits = int(max_fused_qubits)
     o.staged = 1 if staged else 0

@@ -47,6 +47,7 @@ def candidates() -> list:
         out.append((f"plain-gates-f{f}", options(f, staged=False, math="gates")))
     for f in (4, 5, 6):
         out.append((f"plain-tensor-f{f}", options(f, staged=False, math="tensor")))
+    out.append(("plain-tensor-pairs-f6", options(6, staged=False, math="tensor_pairs")))
     out.append(("staged-cuda", options(4, staged=True)))
     for f in (4, 5):
         out.append((f"staged-tensor-f{f}", options(f, staged=True, math="tensor")))
@@ -331,6 +332,8 @@ def main(argv=None):
     ap.add_argument("--eval-circuits", type=int, default=6)
     ap.add_argument("--big-qubits", type=int, default=33)
     ap.add_argument("--big-circuits", type=int, default=2)
+    ap.add_argument("--qft-circuits", type=int, default=0,
+                    help="QFT circuits added to the training set (sizes cycle through --train-qubits)")
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--out", default=MODEL_PATH)
     ap.add_argument("--report", default=None)
@@ -340,6 +343,12 @@ def main(argv=None):
     for i in range(a.circuits):
         n, d = _spec(1000 + i, a.train_qubits, a.depth)
         by_n.setdefault(n, []).append(library_mixed(n, d, 1000 + i))
+    sizes = sorted(set(a.train_qubits))
+    for i in range(a.qft_circuits):
+        from . import library
+
+        n = sizes[i % len(sizes)]
+        by_n.setdefault(n, []).append(library.qft(n).ops())
     xs, ts = [], []
     for n, lists in sorted(by_n.items()):
         x, t = collect(lists, n, repeats=1)
@@ -357,7 +366,9 @@ def main(argv=None):
     pred = model.mlp.forward(x[test])
     err = np.abs(pred - t[test])
     report = {
-        "training_circuits": a.circuits, "train_qubits": a.train_qubits, "depth": a.depth,
+        "training_circuits": a.circuits + a.qft_circuits, "mixed_circuits": a.circuits, "qft_circuits": a.qft_circuits,
+        "train_qubits": sorted(set(a.train_qubits)), "depth": a.depth,
+        "candidates": [name for name, _ in candidates()],
         "pass_rows": int(len(t)), "collect_s": collect_s, "train_s": train_s, "train_loss": loss,
         "heldout_rows": int(test.sum()), "heldout_median_abs_log_err": float(np.median(err)),
         "heldout_p90_abs_log_err": float(np.quantile(err, 0.9)),

@@ -535,7 +535,8 @@ qvdg_status qvdg_plan_create(uint32_t num_qubits, uint32_t precision_bits, const
       upload_plan(plan->program, precision_bits, &plan->device, &plan->dev);
       // Tensor-core plain plans pick their fusion by the cost from |0...0>;
       // the pick for any other state is kept beside it where it differs.
-      if (!opt.staged && opt.math == QVDG_MATH_TENSOR && opt.max_fused_qubits >= 5 && num_qubits >= 13) {
+      if (!opt.staged && (opt.math == QVDG_MATH_TENSOR || opt.math == QVDG_MATH_TENSOR_PAIRS) &&
+          opt.max_fused_qubits >= 5 && num_qubits >= 13) {
         Program general = build_program(t, hops, opt, FusionSearch::Thorough, false);
         if (general.features != plan->program.features || general.run_layout != plan->program.run_layout) {
           general.gates = num_ops;

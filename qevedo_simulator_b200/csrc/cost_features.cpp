@@ -155,4 +155,21 @@ void pass_features(const Target& t, const PlannedPass& p, const LoweredPass& lp,
   f[29] = float(realish) / 64.f;
 }
 
+void pair_features(const Target& t, const PlannedPass& second, float* f) {
+  // A pass of two fused gates: the marker, the second gate's targets in the
+  // position features, two tensor-core gates of width 5-6.
+  f[21] = 1.f;
+  f[23] = 2.f / 16.f;
+  uint32_t lo = uint32_t(f[9] * 32.f + 0.5f), hi = uint32_t(f[10] * 32.f + 0.5f), low4 = uint32_t(f[11] * 6.f + 0.5f);
+  for (uint32_t q : second.ops[0].targets) {
+    const uint32_t ph = t.layout[q];
+    lo = std::min(lo, ph);
+    hi = std::max(hi, ph);
+    if (ph < 4) ++low4;
+  }
+  f[9] = float(lo) / 32.f;
+  f[10] = float(hi) / 32.f;
+  f[11] = float(low4) / 6.f;
+}
+
 }  // namespace qvdg

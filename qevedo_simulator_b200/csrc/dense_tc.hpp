@@ -29,6 +29,35 @@ struct DenseTcTileGeom {
   uint8_t fpos[16];    // tile positions of the 7 free tile bits, ascending
 };
 
+// Two fused 6-qubit gates in one plain pass (dense_tc_pair.cu): an
+// iteration covers the 8192 amplitudes of 13 bits I (both gates' targets
+// and the lowest other bits); gate 1's groups are loaded, multiplied on the
+// tensor cores, transposed through shared memory into gate 2's groups,
+// multiplied again and stored.
+struct DenseTcPairGeom {
+  uint64_t iters;              // 2^(n - 13)
+  uint64_t imask;              // physical bits of I
+  uint64_t grp1[7], grp2[7];   // offset of group bit j: the j-th lowest bit of I outside the gate's targets
+  uint64_t hi1[4], hi2[4];     // offset of members 16 c.. (targets 4 and 5)
+  uint32_t lo1[16], lo2[16];   // offset of members i = 0..15 (targets 0-3, below bit 32)
+  uint16_t lgrp1[7], lgrp2[7]; // the same as positions in the shared-memory transpose buffer (swizzled)
+  uint16_t lhi1[4], lhi2[4];
+  uint16_t llo1[16], llo2[16];
+  uint32_t b1_offset, b2_offset;  // byte offsets of the gates' bf16 matrices in the tensor-core blob
+  uint8_t ibits[16];              // the 13 bits of I, ascending
+  int32_t vw1, vw2;               // access width in complex64 of gate 1's loads and gate 2's stores (1, 2, 4)
+};
+
+// The pair geometry for gates on physical targets t1 and t2 (6 each,
+// ascending) of an n-qubit state, with the gates' bf16 matrices at
+// b1_offset and b2_offset; the shared-memory swizzle is chosen so both
+// gates' group-parallel accesses are free of bank conflicts where possible.
+DenseTcPairGeom dense_tc_pair_geom(uint32_t n, const std::vector<uint32_t>& t1, const std::vector<uint32_t>& t2,
+                                   size_t b1_offset, size_t b2_offset);
+// Whether two gates (physical targets, no controls) can share a pair pass.
+bool dense_tc_pair_ok(uint32_t n, int bits, const std::vector<uint32_t>& t1, const std::vector<uint32_t>& t2);
+void launch_dense_tc_pair(StateImpl& s, const DenseTcPairGeom& g, const uint8_t* tc_blob);
+
 // Whether a dense gate with these targets (physical) and controls runs on
 // the tensor-core plain pass: complex64, 4-6 targets, at least one CTA
 // iteration (8192 amplitudes) of selected groups, and the four lowest

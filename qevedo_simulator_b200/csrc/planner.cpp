@@ -59,8 +59,10 @@ std::vector<qvdg_options> learned_candidates(int bits) {
   std::vector<qvdg_options> c;
   for (uint32_t f = 2; f <= 5; ++f) c.push_back(make(f, 0, QVDG_MATH_FP32));
   for (uint32_t f = 4; f <= 5; ++f) c.push_back(make(f, 0, QVDG_MATH_GATES));
-  if (bits == 32)
+  if (bits == 32) {
     for (uint32_t f = 4; f <= 6; ++f) c.push_back(make(f, 0, QVDG_MATH_TENSOR));
+    c.push_back(make(6, 0, QVDG_MATH_TENSOR_PAIRS));
+  }
   c.push_back(make(4, 1, QVDG_MATH_FP32));
   if (bits == 32)
     for (uint32_t f = 4; f <= 5; ++f) c.push_back(make(f, 1, QVDG_MATH_TENSOR));

@@ -43,6 +43,8 @@ struct Program {
 };
 
 void pass_features(const Target& t, const PlannedPass& p, const LoweredPass& lp, const StageUpload& up, float* f);
+// Adds the second gate of a pair pass to its first gate's features.
+void pair_features(const Target& t, const PlannedPass& second, float* f);
 
 // How hard a tensor-core plain plan searches for fewer passes: the seed
 // lookahead fusions only, plus narrow beam searches, or plus wider ones too.

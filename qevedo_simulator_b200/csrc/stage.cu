@@ -515,7 +515,9 @@ void launch_pass(StateImpl& s, const LoweredPass& lp, const DeviceUpload& dev) {
     return;
   }
   if (!lp.staged) {
-    if (lp.plain.tensor)
+    if (lp.pair)
+      launch_dense_tc_pair(s, *lp.pair, dev.tc);
+    else if (lp.plain.tensor)
       launch_dense_tc(s, lp.plain, dev.tc);
     else
       launch_plain_gate(s, lp.plain, dev.mats);

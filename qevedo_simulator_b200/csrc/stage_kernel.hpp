@@ -3,8 +3,10 @@
 
 #include <stdint.h>
 
+#include <memory>
 #include <vector>
 
+#include "dense_tc.hpp"
 #include "engine.hpp"
 #include "host.hpp"
 
@@ -48,7 +50,9 @@ struct LoweredPass {
   bool block = false;  // plain pass of k_block (geo.L = group qubits, geo.tile_bits = their physical bits)
   TileGeom geo{};
   size_t gate_offset = 0;  // first TileGate of this pass in the upload
-  PlainGate plain;         // when !staged
+  PlainGate plain;         // when !staged (a pair pass: its first gate)
+  // Two fused gates in one plain pass on the tensor cores (dense_tc_pair.cu).
+  std::shared_ptr<const DenseTcPairGeom> pair;
 };
 
 struct DeviceUpload {
@@ -79,6 +83,9 @@ struct PlainTcBlob {
   std::vector<uint8_t> blob;
 };
 bool plain_tc_eligible(const Target& t, const PlannedPass& p, const StageConfig& cfg);
+// Pads a tensor-core blob to a 16-byte boundary (the kernels copy it in
+// 16-byte vectors).
+void blob_align(std::vector<uint8_t>& blob);
 PlainTcBlob plain_tc_blob(const Target& t, const HOp& op);
 // `pre`: the pass's plain_tc_blob when the caller computed it already
 // (moved from).

@@ -178,8 +178,12 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
   prog.target = t;
   prog.gates = ops.size();
   const size_t max_fused = std::max<uint32_t>(opt.max_fused_qubits, 1);
-  prog.cfg = stage_config(t, opt.tile_qubits, opt.staged && opt.math == QVDG_MATH_TENSOR);
-  prog.cfg.plain_tensor = !opt.staged && opt.math == QVDG_MATH_TENSOR && t.bits == 32;
+  // Tensor-core plain passes, singly or (TENSOR_PAIRS) two fused 6-qubit
+  // gates per pass.
+  const bool tensor_math = opt.math == QVDG_MATH_TENSOR || opt.math == QVDG_MATH_TENSOR_PAIRS;
+  const bool pairs = !opt.staged && opt.math == QVDG_MATH_TENSOR_PAIRS && t.bits == 32;
+  prog.cfg = stage_config(t, opt.tile_qubits, opt.staged && tensor_math);
+  prog.cfg.plain_tensor = !opt.staged && tensor_math && t.bits == 32;
   std::vector<PlannedPass> passes;
   // Tensor-core plain passes' bf16 matrices (by pass; empty for the others).
   std::vector<PlainTcBlob> blobs;
@@ -201,7 +205,7 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     // the reference's greedy fusion.
     const FusionInput fin = fusion_input(ops, [](const HOp&) { return true; });
     std::vector<FusedGroup> groups = fuse_groups_lookahead(fin, max_fused, 0);
-    if (opt.math == QVDG_MATH_TENSOR && max_fused >= 5 && t.n >= 13) {
+    if (tensor_math && max_fused >= 5 && t.n >= 13) {
       // Candidate fusions and, for each, the three qubits to place on
       // physical bits 1-3 (a relabel that costs nothing on a |0...0> state
       // and one swap pass otherwise): the pair with the lowest estimated
@@ -405,8 +409,53 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
   }
   prog.upload.tc.reserve(tc_bytes);
   const double state_bytes = double(uint64_t(t.bits == 32 ? 8 : 16) << t.n);
+  // Passes that may share a pass with the next one: after the zero-start
+  // prefix of a run from |0...0> (those passes keep their own variants).
+  size_t pair_from = passes.size();
+  if (pairs) {
+    pair_from = 0;
+    if (from_zero) {
+      uint64_t touched = 0;
+      const uint64_t all = t.n >= 64 ? ~uint64_t(0) : (uint64_t(1) << t.n) - 1;
+      for (const PlannedPass& p : passes) {
+        if (p.staged || p.block || p.ops.size() != 1) break;
+        for (uint32_t q : p.ops[0].targets) touched |= uint64_t(1) << q;
+        for (auto& c : p.ops[0].controls) touched |= uint64_t(1) << c.first;
+        if (touched == all) break;
+        ++pair_from;
+      }
+    }
+  }
+  auto pairable = [&](size_t i) {
+    if (i < pair_from || i + 1 >= passes.size()) return false;
+    const PlannedPass &a = passes[i], &b = passes[i + 1];
+    if (a.staged || a.block || b.staged || b.block || a.ops.size() != 1 || b.ops.size() != 1) return false;
+    if (!a.ops[0].controls.empty() || !b.ops[0].controls.empty()) return false;
+    if (blobs[i].blob.empty() || blobs[i + 1].blob.empty()) return false;
+    return dense_tc_pair_ok(tt.n, tt.bits, blobs[i].targets, blobs[i + 1].targets);
+  };
   for (size_t pi = 0; pi < passes.size(); ++pi) {
     const PlannedPass& p = passes[pi];
+    if (pairable(pi)) {
+      // Two fused 6-qubit gates in one pass: both blobs in the upload, the
+      // pass described by its first gate and the pair geometry.
+      LoweredPass lp = lower_pass(tt, p, prog.cfg, prog.upload, &blobs[pi]);
+      blob_align(prog.upload.tc);
+      const size_t off2 = prog.upload.tc.size();
+      prog.upload.tc.insert(prog.upload.tc.end(), blobs[pi + 1].blob.begin(), blobs[pi + 1].blob.end());
+      lp.pair = std::make_shared<const DenseTcPairGeom>(
+          dense_tc_pair_geom(tt.n, lp.plain.targets, blobs[pi + 1].targets, lp.plain.tc_offset, off2));
+      prog.passes.push_back(std::move(lp));
+      prog.features.resize(prog.features.size() + kPassFeatures);
+      float* f = prog.features.data() + prog.features.size() - kPassFeatures;
+      pass_features(tt, p, prog.passes.back(), prog.upload, f);
+      pair_features(tt, passes[pi + 1], f);
+      prog.kernels += 2;
+      prog.pass_bytes.push_back(2.0 * state_bytes);
+      prog.bytes += 2.0 * state_bytes;
+      ++pi;
+      continue;
+    }
     prog.passes.push_back(lower_pass(tt, p, prog.cfg, prog.upload, blobs[pi].blob.empty() ? nullptr : &blobs[pi]));
     prog.features.resize(prog.features.size() + kPassFeatures);
     pass_features(tt, p, prog.passes.back(), prog.upload, prog.features.data() + prog.features.size() - kPassFeatures);
@@ -562,7 +611,7 @@ void run_program(StateImpl& s, const Program& p, const DeviceUpload& dev, qvdg_s
       const LoweredPass& lp = pass(i);
       int kind = lp.staged ? 1 : 0;
       if (!lp.staged && lp.plain.tensor)
-        kind = dense_tc_staged(s.n, lp.plain.targets, lp.plain.controls.size()) ? 3 : 2;
+        kind = lp.pair ? 5 : (dense_tc_staged(s.n, lp.plain.targets, lp.plain.controls.size()) ? 3 : 2);
       if (i < zero && p.zero_pass_bytes[i] < p.pass_bytes[i]) kind = 4;  // a zero-start pass
       s.pass_kinds.push_back(kind);
     }

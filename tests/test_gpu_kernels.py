@@ -441,3 +441,76 @@ def test_plain_passes_applying_groups_gate_by_gate(oracle, bits, kind):
             st.set_amplitudes(initial)
             stats = st.apply_ops(ops, options(fuse, staged=False, math="gates"))
             assert max_distance(st.amplitudes(), expected) < TOL[bits] * 50, (kind, fuse, stats)
+
+
+@pytest.mark.parametrize("n", [14, 17])
+def test_tensor_core_pair_passes_match_naive(oracle, n):
+    """Two fused 6-qubit gates in one pass (math="tensor_pairs"): targets
+    disjoint or shared, on bit 0 or bits 0 and 1 for either gate (16- and
+    32-byte accesses on the load or the store side), on bits 1-3, low and
+    high, in any order. Where both gates' warp accesses stay coalesced the
+    pair runs as one pass of kind 5 (the planner's features mark it), else as
+    two single passes; every case matches the naive oracle."""
+    from qevedo_simulator_b200 import costmodel
+
+    rng = np.random.Generator(np.random.PCG64(900 + n))
+    paired = 0
+    initial = random_state(rng, n)
+    h = n - 1
+    layouts = [([0, 1, 2, 3, 4, 5], [6, 7, 8, 9, 10, 11]), ([6, 7, 8, 9, 10, 11], [0, 1, 2, 3, 4, 5]),
+               ([0, 5, 9, 11, 12, h], [1, 5, 7, 9, 10, 12]), ([h, 2, 7, 4, 9, 3], [0, 1, h, 8, 6, 4]),
+               ([1, 2, 3, 8, 10, 12], [2, 3, 4, 5, 6, 7]), ([7, 8, 9, 10, 11, 12], [h, h - 1, h - 2, 4, 5, 6]),
+               ([0, 1, 3, 6, 9, 12], [0, 2, 4, 6, 8, 10]), ([5, 6, 7, 8, 9, 10], [5, 6, 7, 8, 9, 11])]
+    for a, b in layouts:
+        ops = [Op(a, [], random_unitary(rng, 6)), Op(b, [], random_unitary(rng, 6))]
+        expected = oracle.naive_apply_ops(initial, ops)
+        with DeviceState(n, 32) as st:
+            st.set_amplitudes(initial)
+            st.set_pass_timing(True)
+            stats = st.apply_ops(ops, options(6, staged=False, math="tensor_pairs"))
+            kinds = list(st.pass_times()[2])
+            err = max_distance(st.amplitudes(), expected) / np.max(np.abs(expected))
+        assert err < TC_REL_TOL, (n, a, b, err)
+        rows = costmodel.plan_features(ops, n, options(6, staged=False, math="tensor_pairs"))
+        if rows.shape[0] == 1 and rows[0, 21] == 1:
+            paired += 1
+            assert kinds == [5] and stats["passes"] == 1 and stats["kernels"] == 2, (a, b, kinds, stats)
+        else:
+            assert 5 not in kinds and stats["passes"] == 2, (a, b, kinds, stats)
+    assert paired >= 4
+
+
+@pytest.mark.parametrize("kind", ["grid", "mixed", "qft", "gates"])
+def test_tensor_core_pair_circuits(oracle, kind):
+    """Whole circuits with pair passes (tensor_pairs at fusion 6; groups with
+    controls or fewer than 6 qubits keep single passes), one-shot from a
+    random state and as a plan run from |0...0> (its zero-start prefix stays
+    single), against the naive oracle."""
+    from qevedo_simulator_b200 import Plan, library
+
+    n = 16
+    if kind == "grid":
+        ops = library.random_grid_circuit(4, 4, 14, seed=61).ops()
+    elif kind == "mixed":
+        ops = library.mixed_ops(n, 8, seed=62)
+    elif kind == "qft":
+        ops = library.qft(n).ops()
+    else:
+        ops = library.random_gate_circuit(n, 150, seed=63).ops()
+    initial = random_state(np.random.Generator(np.random.PCG64(64)), n)
+    expected = oracle.naive_apply_ops(initial, ops)
+    opts = options(6, staged=False, math="tensor_pairs")
+    with DeviceState(n, 32) as st:
+        st.set_amplitudes(initial)
+        st.set_pass_timing(True)
+        st.apply_ops(ops, opts)
+        err = max_distance(st.amplitudes(), expected) / np.max(np.abs(expected))
+        assert err < TC_CIRCUIT_TOL, (kind, err)
+        if kind in ("grid", "qft"):
+            assert 5 in set(st.pass_times()[2].tolist())
+        zero = oracle.naive_statevector(ops, n)
+        with Plan(ops, n, 32, opts) as plan:
+            st.zero()
+            st.execute(plan)
+            err = max_distance(st.amplitudes(), zero) / np.max(np.abs(zero))
+        assert err < TC_CIRCUIT_TOL, (kind, "plan", err)

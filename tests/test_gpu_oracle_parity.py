@@ -23,6 +23,7 @@ ABS_TOL = {32: 1e-6, 64: 1e-12}
 
 PATHS = {
     32: [("plain-tensor-f6", options(6, staged=False, math="tensor")),
+         ("plain-tensor-pairs-f6", options(6, staged=False, math="tensor_pairs")),
          ("plain-tensor-f5", options(5, staged=False, math="tensor")),
          ("plain-tensor-f4", options(4, staged=False, math="tensor")),
          ("staged-tensor-f4", options(4, staged=True, math="tensor")),
@@ -103,6 +104,7 @@ def test_grid_circuits_against_the_fast_oracle_in_f64(oracle, n):
     ref = _fast_oracle_f64(oracle, ops, n)
     try:
         for bits, name, opts in [(32, "plain-tensor-f6", options(6, staged=False, math="tensor")),
+                                 (32, "plain-tensor-pairs-f6", options(6, staged=False, math="tensor_pairs")),
                                  (32, "staged-cuda", options(4, staged=True)),
                                  (32, "plain-f4", options(4, staged=False)),
                                  (64, "plain-f4", options(4, staged=False))]:
@@ -123,6 +125,7 @@ def test_qft_24_from_gaussian_against_the_fast_oracle_in_f64(oracle):
     ref = _fast_oracle_f64(oracle, ops, n, psi)
     try:
         for bits, opts in [(32, options(6, staged=False, math="tensor")), (32, options(5, staged=True, math="tensor")),
+                           (32, options(6, staged=False, math="tensor_pairs")),
                            (64, options(4, staged=False))]:
             with DeviceState(n, bits) as st:
                 st.set_amplitudes(psi)

@@ -14,7 +14,7 @@ def test_candidates_match_the_cost_model_list():
     c32 = [settings_dict(o) for o in _native.planner_candidates(32)]
     assert c32 == [settings_dict(o) for _, o in costmodel.candidates()], names
     c64 = [settings_dict(o) for o in _native.planner_candidates(64)]
-    assert c64 == [c for c in c32 if c["math"] != "tensor"]
+    assert c64 == [c for c in c32 if c["math"] not in ("tensor", "tensor_pairs")]
     assert all(o.planner == _native.PLANNERS["greedy"] for o in _native.planner_candidates(32))
 
 
