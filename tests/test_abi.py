@@ -78,8 +78,21 @@ def test_one_pass_gate_packing_equals_packing_the_ops():
     from qevedo_simulator_b200._abi import PackedOps
     from qevedo_simulator_b200.circuit import gate_op, packed_gate_ops
 
+    from qevedo_simulator_b200 import Circuit, Gate
+    from qevedo_simulator_b200.circuit import _CONTROLLED
+
+    rng = np.random.Generator(np.random.PCG64(8))
+    every = Circuit(5)
+    for name, (controls, _) in sorted(_CONTROLLED.items()):
+        arity = controls + (2 if name == "cswap" else 1)
+        params = (0.37,) if name in ("cp", "crx", "cry", "crz") else ()
+        every._instructions.append(("gate", Gate(name, params),
+                                    [int(q) for q in rng.permutation(5)[:arity]]))
+    q = np.linalg.qr(rng.standard_normal((8, 8)) + 1j * rng.standard_normal((8, 8)))[0]
+    u2 = np.linalg.qr(rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2)))[0]
+    every.unitary(q, [4, 0, 2]).unitary(u2, [3])
     for c in (library.random_grid_circuit(3, 4, 6, 3), library.qft(9), library.random_gate_circuit(8, 200, 5),
-              library.ghz(5)):
+              library.ghz(5), every):
         ins = c._instructions
         a = PackedOps([gate_op(i[1], i[2]) for i in ins if i[0] == "gate"])
         b = packed_gate_ops(ins)

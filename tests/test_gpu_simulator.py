@@ -309,3 +309,21 @@ def test_qasm_teleportation_with_feedback_runs():
     r = run(c, 4000, seed=11)
     ones = sum(v for k, v in r.counts.items() if k[0] == "1")
     assert abs(ones / 4000 - math.sin(0.45) ** 2) < 0.03
+
+
+def test_run_and_statevector_on_openqasm_text():
+    """OpenQASM text through run() and statevector() gives what the parsed
+    circuit gives (the reference's wrappers take either), and the threads and
+    MPS keywords leave the state-vector results unchanged."""
+    from qevedo_simulator_b200 import qasm
+
+    text = ('OPENQASM 2.0;\ninclude "qelib1.inc";\nqreg q[3];\ncreg c[3];\n'
+            'h q[0];\ncx q[0],q[1];\nry(0.7) q[2];\ncz q[1],q[2];\nmeasure q -> c;')
+    parsed = qasm.parse(text)
+    a = run(text, 5000, seed=11)
+    b = run(parsed, 5000, seed=11, threads=2, max_bond_dimension=16, truncation_threshold=1e-8)
+    assert a.counts == b.counts and sum(a.counts.values()) == 5000
+    unitary = text.replace("measure q -> c;", "")
+    sv = statevector(qasm.parse(unitary))
+    assert np.array_equal(statevector(unitary, threads="cores"), sv)
+    assert np.array_equal(statevector(unitary, threads=2), sv)
