@@ -85,6 +85,73 @@ __global__ void __launch_bounds__(kThreads) k_dense(cplx_t<T>* __restrict__ psi,
   }
 }
 
+// Dense gates whose targets all lie in index bits 0-4 (the lane bits of a
+// warp row of 32 consecutive amplitudes), with controls above them: the
+// GPU form of the reference's in-register lane permutations for targets
+// inside a SIMD vector (src/kernels.rs:185, 273, xor_perm). A warp takes
+// whole rows, lane l holding amplitude l of the row (one coalesced 256- or
+// 512-byte access); the other members of its group are in the lanes whose
+// target bits differ, and come over by warp shuffles. Lane l computes its
+// own output, row r(l) of the gate (r = its target bits in matrix order),
+// held in registers, so neither shared memory nor a second pass over the
+// row is needed. Each thread keeps R rows in flight.
+struct LaneGeom {
+  uint64_t rows;           // warp rows of 32 amplitudes the controls select
+  uint64_t control_value;  // control bits that must be 1
+  uint8_t fixed[40];       // bits 0-4 and the control positions, ascending
+  int32_t num_fixed;
+  uint8_t targets[4];      // target positions (matrix bit order), all below 5
+};
+
+template <typename T, int K, int R>
+__global__ void __launch_bounds__(kThreads) k_dense_lanes(cplx_t<T>* __restrict__ psi, const LaneGeom g,
+                                                          const cplx_t<T>* __restrict__ mat) {
+  constexpr int D = 1 << K;
+  __shared__ uint8_t fixed[40];
+  if (threadIdx.x < 40) fixed[threadIdx.x] = g.fixed[threadIdx.x];
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t tmask = 0, row = 0;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    tmask |= 1u << g.targets[j];
+    row |= ((lane >> g.targets[j]) & 1u) << j;
+  }
+  cplx_t<T> m[D];
+  int src[D];
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    m[c] = mat[row * D + c];
+    uint32_t p = lane & ~tmask;
+#pragma unroll
+    for (int j = 0; j < K; ++j) p |= uint32_t((c >> j) & 1) << g.targets[j];
+    src[c] = int(p);
+  }
+  const uint64_t warps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  const uint64_t first = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  for (uint64_t w0 = first * R; w0 < g.rows; w0 += warps * R) {
+    uint64_t base[R];
+    cplx_t<T> x[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      base[q] = w0 + q < g.rows ? (insert_zeros(w0 + q, fixed, g.num_fixed) | g.control_value) + lane : ~uint64_t(0);
+      if (base[q] != ~uint64_t(0)) x[q] = psi[base[q]];
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      cplx_t<T> acc = make_c<T>(T(0), T(0));
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        cplx_t<T> y;
+        y.x = __shfl_sync(0xffffffffu, x[q].x, src[c]);
+        y.y = __shfl_sync(0xffffffffu, x[q].y, src[c]);
+        cmac<T>(acc, m[c], y);
+      }
+      if (base[q] != ~uint64_t(0)) psi[base[q]] = acc;
+    }
+  }
+}
+
 // Dense gates with targets among the low index bits: each thread's group is
 // then a short contiguous run and a warp's loads stride by the run length.
 // Instead, a block stages a tile of 2^13 amplitudes -- index bits 0..Lb-1
@@ -322,6 +389,35 @@ void dense_pick(StateImpl& s, const DenseGeom& g, const void* mat, bool bit0_fre
   dense_launch<T, K, 1, false>(s, g, mat);
 }
 
+template <typename T, int K>
+void lanes_launch(StateImpl& s, const LaneGeom& g, const void* mat) {
+  constexpr int R = 4;
+  const uint64_t warps_needed = (g.rows + R - 1) / R;
+  const unsigned grid = grid_for(s, warps_needed * 32);
+  k_dense_lanes<T, K, R><<<grid, kThreads, 0, s.stream>>>(static_cast<cplx_t<T>*>(s.amp), g,
+                                                          static_cast<const cplx_t<T>*>(mat));
+  QVDG_LAUNCH_CHECK();
+}
+
+template <typename T>
+void lanes_pick(StateImpl& s, const PlainGate& pg, uint64_t control_value, const std::vector<uint8_t>& ctrl,
+                const void* mat) {
+  LaneGeom g{};
+  g.rows = uint64_t(1) << (s.n - 5 - ctrl.size());
+  g.control_value = control_value;
+  std::vector<uint8_t> fixed = {0, 1, 2, 3, 4};
+  fixed.insert(fixed.end(), ctrl.begin(), ctrl.end());
+  std::sort(fixed.begin(), fixed.end());
+  g.num_fixed = int(fixed.size());
+  for (size_t i = 0; i < fixed.size(); ++i) g.fixed[i] = fixed[i];
+  for (size_t j = 0; j < pg.targets.size(); ++j) g.targets[j] = uint8_t(pg.targets[j]);
+  switch (pg.targets.size()) {
+    case 1: return lanes_launch<T, 1>(s, g, mat);
+    case 2: return lanes_launch<T, 2>(s, g, mat);
+    default: return lanes_launch<T, 3>(s, g, mat);
+  }
+}
+
 template <typename T>
 void plain_gate(StateImpl& s, const PlainGate& pg, const void* matrices) {
   const int k = int(pg.targets.size());
@@ -365,6 +461,13 @@ void plain_gate(StateImpl& s, const PlainGate& pg, const void* matrices) {
     g.offsets[h] = o;
   }
   const bool bit0_free = fixed.empty() || fixed[0] != 0;
+  // Targets all in the lane bits 0-4 (controls above them): warp shuffles.
+  {
+    bool lanes = k <= 3 && s.n >= 5;
+    for (uint32_t t : pg.targets) lanes = lanes && t < 5;
+    for (uint8_t cq : ctrl) lanes = lanes && cq >= 5;
+    if (lanes) return lanes_pick<T>(s, pg, control_value, ctrl, mat);
+  }
   // complex64, no controls, targets (nearly) all among bits 0-3 -- each
   // group one short contiguous run -- and a state of at least one tile:
   // stage tiles through shared memory (coalesced) instead. With fewer low

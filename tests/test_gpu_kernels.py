@@ -514,3 +514,26 @@ def test_tensor_core_pair_circuits(oracle, kind):
             st.execute(plan)
             err = max_distance(st.amplitudes(), zero) / np.max(np.abs(zero))
         assert err < TC_CIRCUIT_TOL, (kind, "plan", err)
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_low_qubit_gates_by_warp_shuffles(oracle, bits):
+    """Dense 1-3 qubit gates whose targets all lie in index bits 0-4 (the lanes
+    of a warp row), with no controls or controls above bit 4, run as warp
+    shuffles within rows of 32 amplitudes (k_dense_lanes): every target
+    layout against the naive oracle, from one row (5 qubits) to many."""
+    rng = np.random.Generator(np.random.PCG64(77 + bits))
+    for n in (5, 6, 9, 14, 18):
+        initial = random_state(rng, n)
+        for case in range(12):
+            k = 1 + case % 3
+            qubits = [int(q) for q in rng.permutation(5)[:k]]
+            high = list(range(5, n))
+            nc = int(rng.integers(0, min(len(high), 2) + 1))
+            controls = [(int(q), bool(rng.integers(2))) for q in rng.permutation(high)[:nc]] if high else []
+            m = random_unitary(rng, k)
+            expected = oracle.naive_apply_ops(initial, [Op(qubits, controls, m)])
+            with DeviceState(n, bits) as st:
+                st.set_amplitudes(initial)
+                st.apply(m, qubits, controls)
+                assert max_distance(st.amplitudes(), expected) < TOL[bits], (n, qubits, controls)
