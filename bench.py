@@ -20,6 +20,10 @@ time of the public `run()` call (host planning, uploads from pinned memory,
 1000 shots, outcomes back to the host) and the CPU baseline are reported
 beside it. With N GPUs each rank runs its own circuit (replicas; the state
 does not shard in this engine) and the step time is the max over ranks.
+At N = 1 the line also carries `other_configs`: the QFT at 30 qubits, the
+precision form at 32 qubits with 1M shots, the batched HEA form and the
+learned planner against the greedy default at 33 qubits, each measured once
+(--skip-others leaves them out).
 
 Reference arm (--impl reference): the reference's CPU engine, restated in C++
 (oracle/; the Rust crate cannot be built here), on all host threads, on a
@@ -405,7 +409,7 @@ def run_ours(args, rank: int, world: int):
     e2e_s = max_over_ranks(float(np.mean(e2e)), dist)
     h2d = tuned_upload_bytes(ops) + 8 * SHOTS
     d2h = 8 * SHOTS + 16
-    cpu, err = None, None
+    cpu, err, others = None, None, None
     if rank == 0 and world == 1 and not args.skip_cpu:
         cpu = cpu_baseline(ops, n, layer_prefix_ops(circuit, n), budget_s=args.cpu_budget)
         cpu["cpu"] = host_cpu_model()
@@ -414,6 +418,8 @@ def run_ours(args, rank: int, world: int):
             st.zero()
             st.execute(tuned)
             err = oracle_f64_error(ops, n, st)
+    if rank == 0 and world == 1 and not args.skip_others and fixed is None:
+        others = other_configs()
     if rank == 0:
         line = {
             "metric": METRIC, "value": step, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -440,6 +446,7 @@ def run_ours(args, rank: int, world: int):
             "plain": {"s": plain_s, "passes": plain_info["passes"], "kernels": plain_info["kernels"]},
             "tuned_over_plain": step / plain_s,
             "max_amp_err_vs_oracle_f64": err,
+            "other_configs": others,
             "gates": info["gates"],
             "wall_s_timed_region": wall,
         }
@@ -467,6 +474,113 @@ def timed_plan(st, plan, initial=None, repeats: int = 2):
             sec, byt, _ = st.pass_times()
     st.set_pass_timing(False)
     return best, sec, byt
+
+
+def other_configs() -> dict:
+    """The other configurations, measured once each in the default run so
+    the bench line carries them (device seconds, CUDA events): QFT at 30
+    qubits on a general state, the precision form at 32 qubits, the batched
+    HEA form, and the learned planner against the greedy default at 33
+    qubits. Each is independent: a failure is reported in its entry."""
+    from qevedo_simulator_b200 import Batch, Circuit, DeviceState, Plan, _native, costmodel, library, options
+
+    out = {}
+
+    def timed(name, fn):
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as e:  # reported, not raised: the headline line must still print
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = round(time.perf_counter() - t0, 2)
+
+    _native.ensure_cost_model()
+
+    def learned(ops, n, from_zero):
+        chosen, _ = _native.plan_choose(ops, n, from_zero=from_zero)
+        return chosen
+
+    def prepare(st, n):
+        # A general state: a layer of H and RZ(0.1 + 0.07 q) on every qubit.
+        c = Circuit(n)
+        for q in range(n):
+            c.h(q).rz(0.1 + 0.07 * q, q)
+        st.zero()
+        st.apply_ops(c.ops(), options(4, staged=False))
+
+    def qft30():
+        n = 30
+        ops = library.qft(n).ops()
+        res = {"workload": "QFT 30 qubits complex64 on a general state (H and RZ layer), textbook H + controlled "
+                           "phases, no final swaps"}
+        with DeviceState(n, 32) as st:
+            for label, opts in (("learned", learned(ops, n, False)), ("plain-f4", options(4, staged=False))):
+                with Plan(ops, n, 32, opts) as plan:
+                    best = float("inf")
+                    for _ in range(2):
+                        prepare(st, n)
+                        best = min(best, st.execute(plan)["gate_seconds"])
+                    res[label] = {"s": best, "passes": plan.info()["passes"], "settings": plan.info()["settings"]}
+        res["learned_over_plain"] = res["learned"]["s"] / res["plain-f4"]["s"]
+        return res
+
+    def precision32():
+        n = 32
+        ops = library.random_grid_circuit(4, 8, DEPTH, SEED).ops()
+        res = {"workload": "grid circuit 4x8 depth 20, 32 qubits complex64 (32 GiB) from |0...0>, 1M shots"}
+        with DeviceState(n, 32) as st:
+            with Plan(ops, n, 32, options(planner="learned")) as plan:
+                st.zero()
+                s = st.execute(plan)
+                res["s"], res["passes"], res["settings"] = s["gate_seconds"], s["passes"], s["settings"]
+            u = np.random.Generator(np.random.PCG64(SEED)).random(1_000_000)
+            t0 = time.perf_counter()
+            st.sample_unordered(u)
+            res["sample_1M_s"] = time.perf_counter() - t0
+            res["norm_sqr"] = st.norm_sqr()
+        return res
+
+    def batch():
+        count, sample = 4096, 16
+        specs = library.hea_batch(count, seed=SEED)
+        circuits = [(w, library.hea_layers(w, l, s), "cx") for w, l, s in specs]
+        b = Batch(circuits)
+        b.run()
+        times = [b.run()[1] for _ in range(3)]
+        b.close()
+        per = 0.0
+        rng = np.random.Generator(np.random.PCG64(SEED))
+        for i in sorted(rng.choice(count, size=sample, replace=False).tolist()):
+            w, gates = circuits[i][0], circuits[i][1]
+            c = Circuit(w)
+            for layer in gates:
+                for q in range(w):
+                    c.unitary(layer[q], [q])
+                for q in range(w - 1):
+                    c.cx(q, q + 1)
+            with DeviceState(w, 32) as st:
+                t0 = time.perf_counter()
+                st.apply_ops(c.ops(), options(4, staged=False))
+                st.expect_z_all()
+                per += time.perf_counter() - t0
+        per_circuit_s = per / sample * count
+        return {"workload": "4096 HEA circuits, width U{10..22}, layers U{4..12}, to <Z_q>, one graph-captured "
+                            "persistent launch", "s": float(min(times)), "per_circuit_path_s": per_circuit_s,
+                "per_circuit_sample": sample, "speedup": per_circuit_s / float(min(times))}
+
+    def costmodel33():
+        n = 33
+        ops = library.mixed_ops(n, 10, 9000)
+        model = costmodel.CostModel.load()
+        row = costmodel.evaluate(model, [ops], n, all_candidates=False)[0]
+        return {"workload": "one held-out mixed circuit, 33 qubits complex64 (64 GiB), depth 10, seed 9000",
+                "pick": row["pick"], "pick_s": row["pick_s"], "greedy_default_s": row["default_s"],
+                "speedup": row["default_s"] / row["pick_s"]}
+
+    for name, fn in (("qft30", qft30), ("precision32", precision32), ("batch_hea", batch),
+                     ("costmodel33", costmodel33)):
+        timed(name, fn)
+    return out
 
 
 def run_qft(args):
@@ -703,6 +817,8 @@ def main():
                     help="run this plan instead of the learned planner's choice")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-check", action="store_true")
+    ap.add_argument("--skip-others", action="store_true",
+                    help="leave out the other configurations (QFT, precision form, batch, cost model at 33 qubits)")
     ap.add_argument("--cpu-budget", type=float, default=25.0)
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the dominant kernel from an ncu capture (roofline.traffic)")
