@@ -49,3 +49,33 @@ def test_fused_ops_of_an_empty_circuit_and_staged_plans():
     assert costmodel.fused_ops([], 14, options(6, staged=False, math="tensor")) == []
     with pytest.raises(ValueError, match="plain plans only"):
         costmodel.fused_ops(library.qft(14).ops(), 14, options(4, staged=True))
+
+
+def test_pair_passes_in_plans():
+    """math="tensor_pairs" keeps the tensor-core fusion (the same fused ops in
+    the same order) and merges consecutive fused 6-qubit passes without
+    controls into pair passes (features marked) only where both gates' warp
+    accesses stay coalesced: two gates on high, disjoint qubits (13-bit
+    iteration with one low bit) stay single; gates that leave bits 0-3 free
+    pair."""
+    import numpy as np
+
+    from qevedo_simulator_b200 import Op
+
+    ops = library.random_grid_circuit(5, 6, 20, seed=2024).ops()
+    single = options(6, staged=False, math="tensor")
+    pairs = options(6, staged=False, math="tensor_pairs")
+    a = costmodel.plan_features(ops, 30, single)
+    b = costmodel.plan_features(ops, 30, pairs)
+    marked = int(np.sum(b[:, 21] == 1))
+    assert marked >= 1 and b.shape[0] == a.shape[0] - marked
+    fa = costmodel.fused_ops(ops, 30, single)
+    fb = costmodel.fused_ops(ops, 30, pairs)
+    assert [f.targets for f in fa] == [f.targets for f in fb]
+    rng = np.random.Generator(np.random.PCG64(3))
+    u = np.linalg.qr(rng.standard_normal((64, 64)) + 1j * rng.standard_normal((64, 64)))[0]  # dense
+    scattered = [Op([8, 10, 12, 14, 16, 18], [], u), Op([9, 11, 13, 15, 17, 19], [], u)]
+    assert costmodel.plan_features(scattered, 24, pairs).shape[0] == 2
+    overlapping = [Op([8, 10, 12, 14, 16, 18], [], u), Op([8, 10, 12, 15, 17, 19], [], u)]
+    rows = costmodel.plan_features(overlapping, 24, pairs)
+    assert rows.shape[0] == 1 and rows[0, 21] == 1
