@@ -392,10 +392,6 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       if (plain_tc_eligible(rt, p, prog.cfg)) blobs[products[j]] = plain_tc_blob(rt, p.ops[0]);
     }, wide ? 0u : 1u);
   }
-  if (fused) {
-    if (opt.staged) throw Error(QVDG_ERR_INVALID, "fused ops exist for plain plans only");
-    for (const PlannedPass& p : passes) fused->insert(fused->end(), p.ops.begin(), p.ops.end());
-  }
   // Passes are lowered on the layout they run with.
   Target run_target = t;
   if (!prog.run_layout.empty()) run_target.layout = prog.run_layout;
@@ -426,34 +422,76 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       }
     }
   }
-  auto pairable = [&](size_t i) {
-    if (i < pair_from || i + 1 >= passes.size()) return false;
-    const PlannedPass &a = passes[i], &b = passes[i + 1];
-    if (a.staged || a.block || b.staged || b.block || a.ops.size() != 1 || b.ops.size() != 1) return false;
-    if (!a.ops[0].controls.empty() || !b.ops[0].controls.empty()) return false;
-    if (blobs[i].blob.empty() || blobs[i + 1].blob.empty()) return false;
-    return dense_tc_pair_ok(tt.n, tt.bits, blobs[i].targets, blobs[i + 1].targets);
-  };
-  for (size_t pi = 0; pi < passes.size(); ++pi) {
+  // Pairing: each pass after the zero-start prefix takes as its partner the
+  // first of the next few passes that pairs with it (dense_tc_pair_ok) and
+  // shares no qubit with any pass between them, moved up next to it (the
+  // passes it jumps commute with it). `order` is the execution order,
+  // `pair_next[k]` marks order[k] pairing with order[k + 1].
+  std::vector<size_t> order;
+  std::vector<char> pair_next;
+  {
+    auto eligible = [&](size_t i) {
+      const PlannedPass& q = passes[i];
+      return !q.staged && !q.block && q.ops.size() == 1 && q.ops[0].controls.empty() && !blobs[i].blob.empty() &&
+             q.ops[0].targets.size() == 6;
+    };
+    auto mask = [&](size_t i) {
+      uint64_t m = 0;
+      for (const HOp& op : passes[i].ops) {
+        for (uint32_t q : op.targets) m |= uint64_t(1) << q;
+        for (auto& c : op.controls) m |= uint64_t(1) << c.first;
+      }
+      for (uint32_t q : passes[i].block_qubits) m |= uint64_t(1) << q;
+      return m;
+    };
+    constexpr size_t kWindow = 8;
+    std::vector<char> used(passes.size(), 0);
+    for (size_t i = 0; i < passes.size(); ++i) {
+      if (used[i]) continue;
+      used[i] = 1;
+      order.push_back(i);
+      pair_next.push_back(0);
+      if (!pairs || i < pair_from || !eligible(i)) continue;
+      uint64_t between = 0;
+      for (size_t j = i + 1; j < passes.size() && j <= i + kWindow; ++j) {
+        if (used[j]) continue;
+        if (eligible(j) && !(mask(j) & between) &&
+            dense_tc_pair_ok(tt.n, tt.bits, blobs[i].targets, blobs[j].targets)) {
+          used[j] = 1;
+          pair_next.back() = 1;
+          order.push_back(j);
+          pair_next.push_back(0);
+          break;
+        }
+        between |= mask(j);
+      }
+    }
+  }
+  if (fused) {
+    if (opt.staged) throw Error(QVDG_ERR_INVALID, "fused ops exist for plain plans only");
+    for (size_t i : order) fused->insert(fused->end(), passes[i].ops.begin(), passes[i].ops.end());
+  }
+  for (size_t k = 0; k < order.size(); ++k) {
+    const size_t pi = order[k];
     const PlannedPass& p = passes[pi];
-    if (pairable(pi)) {
+    if (pair_next[k]) {
       // Two fused 6-qubit gates in one pass: both blobs in the upload, the
       // pass described by its first gate and the pair geometry.
+      const size_t pj = order[++k];
       LoweredPass lp = lower_pass(tt, p, prog.cfg, prog.upload, &blobs[pi]);
       blob_align(prog.upload.tc);
       const size_t off2 = prog.upload.tc.size();
-      prog.upload.tc.insert(prog.upload.tc.end(), blobs[pi + 1].blob.begin(), blobs[pi + 1].blob.end());
+      prog.upload.tc.insert(prog.upload.tc.end(), blobs[pj].blob.begin(), blobs[pj].blob.end());
       lp.pair = std::make_shared<const DenseTcPairGeom>(
-          dense_tc_pair_geom(tt.n, lp.plain.targets, blobs[pi + 1].targets, lp.plain.tc_offset, off2));
+          dense_tc_pair_geom(tt.n, lp.plain.targets, blobs[pj].targets, lp.plain.tc_offset, off2));
       prog.passes.push_back(std::move(lp));
       prog.features.resize(prog.features.size() + kPassFeatures);
       float* f = prog.features.data() + prog.features.size() - kPassFeatures;
       pass_features(tt, p, prog.passes.back(), prog.upload, f);
-      pair_features(tt, passes[pi + 1], f);
+      pair_features(tt, passes[pj], f);
       prog.kernels += 2;
       prog.pass_bytes.push_back(2.0 * state_bytes);
       prog.bytes += 2.0 * state_bytes;
-      ++pi;
       continue;
     }
     prog.passes.push_back(lower_pass(tt, p, prog.cfg, prog.upload, blobs[pi].blob.empty() ? nullptr : &blobs[pi]));

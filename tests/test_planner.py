@@ -30,7 +30,8 @@ def test_fused_programs_equal_the_circuit(oracle, kind):
     psi = random_state(np.random.Generator(np.random.PCG64(40)), n)
     expected = oracle.naive_apply_ops(psi, ops)
     plans = [options(4, staged=False), options(5, staged=False, math="tensor"),
-             options(6, staged=False, math="tensor"), options(5, staged=False, math="gates")]
+             options(6, staged=False, math="tensor"), options(5, staged=False, math="gates"),
+             options(6, staged=False, math="tensor_pairs")]
     for opts in plans:
         for from_zero in (False, True):
             fused = costmodel.fused_ops(ops, n, opts, from_zero=from_zero)
@@ -41,8 +42,8 @@ def test_fused_programs_equal_the_circuit(oracle, kind):
             assert err < 1e-10, (kind, opts.max_fused_qubits, opts.math, from_zero, err)
         # The general-state fusion is the one the cost model's features describe.
         rows = costmodel.plan_features(ops, n, opts)
-        if opts.math != 2:
-            assert rows.shape[0] == len(costmodel.fused_ops(ops, n, opts))
+        if opts.math != 2:  # a pair pass (feature 21) applies two fused ops
+            assert rows.shape[0] + int(np.sum(rows[:, 21] == 1)) == len(costmodel.fused_ops(ops, n, opts))
 
 
 def test_fused_ops_of_an_empty_circuit_and_staged_plans():
@@ -52,12 +53,12 @@ def test_fused_ops_of_an_empty_circuit_and_staged_plans():
 
 
 def test_pair_passes_in_plans():
-    """math="tensor_pairs" keeps the tensor-core fusion (the same fused ops in
-    the same order) and merges consecutive fused 6-qubit passes without
-    controls into pair passes (features marked) only where both gates' warp
-    accesses stay coalesced: two gates on high, disjoint qubits (13-bit
-    iteration with one low bit) stay single; gates that leave bits 0-3 free
-    pair."""
+    """math="tensor_pairs" keeps the tensor-core fusion (the same fused ops;
+    a pass may move up past passes it commutes with to meet its partner) and
+    merges fused 6-qubit passes without controls into pair passes (features
+    marked) only where both gates' warp accesses stay coalesced: two gates on
+    high, disjoint qubits (13-bit iteration with one low bit) stay single;
+    gates that leave bits 0-3 free pair."""
     import numpy as np
 
     from qevedo_simulator_b200 import Op
@@ -71,7 +72,9 @@ def test_pair_passes_in_plans():
     assert marked >= 1 and b.shape[0] == a.shape[0] - marked
     fa = costmodel.fused_ops(ops, 30, single)
     fb = costmodel.fused_ops(ops, 30, pairs)
-    assert [f.targets for f in fa] == [f.targets for f in fb]
+    # the same fused ops; a pair's second pass may move up past passes it
+    # commutes with (no shared qubit)
+    assert sorted(map(tuple, (f.targets for f in fa))) == sorted(map(tuple, (f.targets for f in fb)))
     rng = np.random.Generator(np.random.PCG64(3))
     u = np.linalg.qr(rng.standard_normal((64, 64)) + 1j * rng.standard_normal((64, 64)))[0]  # dense
     scattered = [Op([8, 10, 12, 14, 16, 18], [], u), Op([9, 11, 13, 15, 17, 19], [], u)]
