@@ -40,9 +40,9 @@ struct DenseTcPairGeom {
   uint64_t grp1[7], grp2[7];   // offset of group bit j: the j-th lowest bit of I outside the gate's targets
   uint64_t hi1[4], hi2[4];     // offset of members 16 c.. (targets 4 and 5)
   uint32_t lo1[16], lo2[16];   // offset of members i = 0..15 (targets 0-3, below bit 32)
-  uint16_t lgrp1[7], lgrp2[7]; // the same as positions in the shared-memory transpose buffer (swizzled)
-  uint16_t lhi1[4], lhi2[4];
-  uint16_t llo1[16], llo2[16];
+  uint32_t lgrp1[7], lgrp2[7]; // the same as byte offsets in the shared-memory transpose buffer (swizzled)
+  uint32_t lhi1[4], lhi2[4];
+  uint32_t llo1[16], llo2[16];
   uint32_t b1_offset, b2_offset;  // byte offsets of the gates' bf16 matrices in the tensor-core blob
   uint8_t ibits[16];              // the 13 bits of I, ascending
   int32_t vw1, vw2;               // access width in complex64 of gate 1's loads and gate 2's stores (1, 2, 4)

@@ -7,29 +7,37 @@
 // An iteration covers the 8192 amplitudes spanned by 13 bits I: the
 // targets of both gates and the lowest other bits. Gate 1 sees them as 128
 // groups of 64 members (groups over I minus its targets), gate 2 as another
-// 128 groups. Persistent CTAs of 512 threads; thread (w, r) owns 16 members
-// of group r for either gate (w / 4 picks which 16), as in the single-gate
-// kernel (dense_tc.cu), and tensor-memory lane r holds group r:
+// 128 groups. Persistent CTAs of 16 compute warps and one issuing
+// warpgroup; compute thread (w, r) owns 16 members of group r for either
+// gate (w / 4 picks which 16), as in the single-gate kernel (dense_tc.cu),
+// and tensor-memory lane r holds group r:
 //
 //   1. gate 1's members come from HBM (loaded two iterations ahead into
 //      registers), are split into bf16 high and low parts and written to
-//      the A buffer in tensor memory; one thread issues the products
-//      A_hi B1_hi + A_hi B1_lo + A_lo B1_hi (fp32 accumulation);
+//      the A operand in tensor memory; the issuing thread then runs the
+//      products A_hi B1_hi + A_hi B1_lo + A_lo B1_hi (fp32 accumulation);
 //   2. the products are read back (tcgen05.ld) and written into a 64 KB
-//      shared-memory buffer at the amplitudes' positions in I; after a CTA
-//      barrier every thread reads its 16 members of gate 2's group r from
-//      it, splits them into the same A buffer, and the products with B2
-//      are issued;
-//   3. one iteration later gate 2's products are read back and stored to
-//      HBM where gate 2's members lie.
+//      shared-memory buffer at the amplitudes' positions in I; after a
+//      barrier of the compute warps every thread reads its 16 members of
+//      gate 2's group r from it, splits them into the same A operand, and
+//      the products with B2 run;
+//   3. gate 2's products are read back and stored to HBM where gate 2's
+//      members lie.
 //
-// Two sets of tensor-memory buffers (A and D, 256 columns each) alternate
-// between iterations, so iteration i's first products run while iteration
-// i - 1 is stored. Positions in the transpose buffer are XOR-swizzled (low
-// four index bits with a host-chosen linear map of the high ones) so that
-// both gates' group-parallel accesses hit distinct banks. Every wait on a
-// product barrier is bounded: on timeout the kernel records an error, all
-// threads leave at the next CTA barrier and the tensor memory is freed.
+// Two iterations are in flight, each with its own tensor-memory slot (A and
+// D, 128 columns each), so that the compute warps' work on one slot
+// overlaps the products of the other. The products are issued by a thread
+// of their own because issuing holds that thread until the tensor cores
+// have nearly finished them (measured on B200: 24 products of M = N = 128,
+// K = 16 keep the issuing thread about as long as they run, about 67 cycles
+// each). Compute warps and the issuing thread hand slots to each other
+// through mbarriers: the compute warps arrive on "ready" barriers, the
+// products complete "done" barriers (tcgen05.commit). Positions in the
+// transpose buffer are XOR-swizzled (low four index bits with a host-chosen
+// linear map of the high ones) so that both gates' group-parallel accesses
+// hit distinct banks. Every wait is bounded: on timeout the kernel records
+// an error, every thread leaves its loop, and the tensor memory is freed
+// after a bounded wait for the products still in flight.
 
 #include <cuda_runtime.h>
 
@@ -65,6 +73,13 @@ __device__ __forceinline__ void load16(const float2* psi, uint64_t base, const u
   }
 }
 
+// The same members into L2 (no registers held while the lines arrive).
+template <int VW>
+__device__ __forceinline__ void prefetch16(const float2* psi, uint64_t base, const uint32_t* lo) {
+#pragma unroll
+  for (int m = 0; m < 16 / VW; ++m) asm volatile("prefetch.global.L2 [%0];" ::"l"(psi + base + lo[VW * m]));
+}
+
 // Eight members 8 hh .. 8 hh + 7 of one group from registers to HBM.
 template <int VW>
 __device__ __forceinline__ void store8(float2* psi, uint64_t base, const uint32_t* lo, int hh, const float* re,
@@ -83,36 +98,112 @@ __device__ __forceinline__ void store8(float2* psi, uint64_t base, const uint32_
   }
 }
 
+// Threads: 16 compute warps (512 threads: group r = tid % 128, member
+// chunk tid / 128) and a fifth warpgroup whose first thread issues the
+// products (an issuing thread is held until its products are nearly done,
+// so it does nothing else). Launched at 96 registers a thread (640 x 96 =
+// 61440); the issuing warpgroup keeps 32 and the compute warps take 112
+// (128 x 32 + 512 x 112 = 61440).
+constexpr int kPairThreads = kThreads + 128;
+constexpr uint32_t kIssueRegs = 32, kComputeRegs = 112;
+constexpr uint32_t kComputeWarps = kThreads / 32;
+
+// Barrier among the 512 compute threads (named barrier 1), returning
+// whether any of them passed a nonzero `flag`.
+__device__ __forceinline__ bool compute_sync_or(int flag) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.s32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(out)
+      : "r"(flag), "n"(kThreads)
+      : "memory");
+  return out != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Bounded wait for a barrier phase that also gives up when another thread
+// of the CTA has raised `abort` (then or on its own timeout it returns
+// false; a timeout raises `abort` and the status word).
+__device__ __forceinline__ bool wait_or_abort(uint32_t bar, uint32_t parity, volatile int* abort, int* status) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*abort) return false;
+    if (clock64() - t0 > kWaitCycles) {
+      *abort = 1;
+      atomicExch(status, 1);
+      return false;
+    }
+  }
+  return true;
+}
+
+// Gate products of one slot, D = A_hi B_hi + A_hi B_lo + A_lo B_hi with A
+// in tensor memory (`acol`: A_hi, A_lo 64 columns later), B in shared
+// memory (hi, then lo), fp32 into `dcol`; then one commit to `bar`. Loops
+// kept rolled: the issuing thread runs on few registers.
+__device__ __forceinline__ void issue_pair_products(uint32_t acol, const unsigned char* bmat, uint32_t dcol,
+                                                    uint32_t bar) {
+  constexpr uint32_t kd = 128, SBO = kd * 16, BPART = kd * kd * 2;
+  tc_fence_after();
+  const uint32_t idesc = umma_idesc(kd);
+  const uint64_t dbh = umma_desc(smem_addr(bmat), 128, SBO), dbl = umma_desc(smem_addr(bmat + BPART), 128, SBO);
+  uint32_t acc = 0;
+#pragma unroll 1
+  for (int p = 0; p < 3; ++p) {
+    const uint32_t a0 = acol + (p == 2 ? 64u : 0u);
+    const uint64_t b0 = p == 1 ? dbl : dbh;
+#pragma unroll 1
+    for (uint32_t s = 0; s < kd / 16; ++s) {
+      umma_bf16_tmem_a(dcol, a0 + 8 * s, b0 + 16 * s, idesc, acc);
+      acc = 1;
+    }
+  }
+  umma_commit(bar);
+}
+
 template <int VW1, int VW2>
-__global__ void __launch_bounds__(kThreads, 1) k_dense_tc_pair(float2* __restrict__ psi, const DenseTcPairGeom g,
-                                                               const uint8_t* __restrict__ bmats,
-                                                               int* __restrict__ status) {
+__global__ void __launch_bounds__(kPairThreads, 1) k_dense_tc_pair(float2* __restrict__ psi, const DenseTcPairGeom g,
+                                                                   const uint8_t* __restrict__ bmats,
+                                                                   int* __restrict__ status) {
   constexpr uint32_t D = 64;
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar1[2], bar2[2];
+  // ready*: the compute warps' operands (and freed products) of a slot are
+  // in place for gate 1's / gate 2's products; done*: those products
+  // completed (tcgen05.commit).
+  __shared__ __align__(8) uint64_t ready1[2], ready2[2], done1[2], done2[2];
   __shared__ uint32_t tmem_slot;
   __shared__ uint8_t ibits[16];
-  unsigned char* bmat1 = smem;                            // gate 1: B hi, then B lo
-  unsigned char* bmat2 = smem + kPairBytes;               // gate 2
-  float2* xbuf = reinterpret_cast<float2*>(smem + 2 * kPairBytes);  // 8192 complex64
+  __shared__ volatile int abort;
+  unsigned char* bmat1 = smem;                                        // gate 1: B hi, then B lo
+  unsigned char* bmat2 = smem + kPairBytes;                           // gate 2
+  unsigned char* xbytes = smem + 2 * kPairBytes;                    // 8192 complex64, byte offsets
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t r = uint32_t(tid) & 127u, chunk = uint32_t(tid) >> 7;
 
   if (tid < 16) ibits[tid] = g.ibits[tid];
+  if (tid == 0) abort = 0;
   {
     const uint4* s1 = reinterpret_cast<const uint4*>(bmats + g.b1_offset);
     const uint4* s2 = reinterpret_cast<const uint4*>(bmats + g.b2_offset);
     uint4* d1 = reinterpret_cast<uint4*>(bmat1);
     uint4* d2 = reinterpret_cast<uint4*>(bmat2);
-    for (uint32_t i = tid; i < kPairBytes / 16; i += kThreads) {
+    for (uint32_t i = tid; i < kPairBytes / 16; i += kPairThreads) {
       d1[i] = s1[i];
       d2[i] = s2[i];
     }
   }
   if (tid == 0) {
     for (int b = 0; b < 2; ++b) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar1[b])));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar2[b])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&ready1[b])), "n"(kComputeWarps));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&ready2[b])), "n"(kComputeWarps));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&done1[b])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&done2[b])));
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -126,128 +217,177 @@ __global__ void __launch_bounds__(kThreads, 1) k_dense_tc_pair(float2* __restric
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
-
-  // This thread's group r and member chunk, for either gate: HBM offset of
-  // its group and chunk, and its position (swizzled) in the transpose
-  // buffer; member i adds lo*[i] / XORs llo*[i].
-  uint64_t gb1 = chunk == 0 ? g.hi1[0] : chunk == 1 ? g.hi1[1] : chunk == 2 ? g.hi1[2] : g.hi1[3];
-  uint64_t gb2 = chunk == 0 ? g.hi2[0] : chunk == 1 ? g.hi2[1] : chunk == 2 ? g.hi2[2] : g.hi2[3];
-  uint32_t lb1 = chunk == 0 ? g.lhi1[0] : chunk == 1 ? g.lhi1[1] : chunk == 2 ? g.lhi1[2] : g.lhi1[3];
-  uint32_t lb2 = chunk == 0 ? g.lhi2[0] : chunk == 1 ? g.lhi2[1] : chunk == 2 ? g.lhi2[2] : g.lhi2[3];
-#pragma unroll
-  for (int j = 0; j < 7; ++j)
-    if ((r >> j) & 1u) {
-      gb1 += g.grp1[j];
-      gb2 += g.grp2[j];
-      lb1 ^= g.lgrp1[j];
-      lb2 ^= g.lgrp2[j];
-    }
-  uint32_t lo1[16], lo2[16];
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    lo1[i] = g.lo1[i];
-    lo2[i] = g.lo2[i];
-  }
   const uint64_t my_iters = blockIdx.x < g.iters ? (g.iters - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  // Iteration bases (the bits outside I), advanced by a running deposit.
-  const uint64_t dstep = insert_zeros(gridDim.x, ibits, 13);
-  uint64_t dload = insert_zeros(blockIdx.x, ibits, 13), dstore = dload;
-  const uint32_t lanes = (uint32_t(warp & 3) * 32u) << 16;
-  int failed = 0;
+  const uint64_t periods = (my_iters + 1) / 2;
 
-  auto load = [&](float2 (&x)[16]) {
-    load16<VW1>(psi, dload + gb1, lo1, x);
-    dload = dep_add(dload, dstep, g.imask);
-  };
-  // Step li: gate 1 of iteration li from registers into A and its products
-  // issued; iteration li - 1 (gate 2's products, issued in the last step)
-  // stored; iteration li's products transposed into gate 2's groups and
-  // its second products issued. Returns whether another step follows.
-  auto step = [&](uint64_t li, float2 (&x)[16]) -> bool {
-    const bool have = li < my_iters;
-    const uint32_t b = uint32_t(li & 1);
-    const uint32_t acol = kTmemA + b * 128, dcol = b * 128;
-    const uint32_t parity = uint32_t((li >> 1) & 1);
-    if (have) {
-      write_a8_tmem<6>(x, tmem + lanes + acol, chunk, 0);
-      write_a8_tmem<6>(x + 8, tmem + lanes + acol, chunk, 1);
-      if (li + 2 < my_iters) load(x);
-      tmem_wait_st();
+  // Period j runs iterations a = 2j (slot 0) and b = 2j + 1 (slot 1). The
+  // issuing thread takes, in order, M1(a), M1(b), M2(a), M2(b), each once
+  // its slot's compute warps have arrived on the ready barrier; the
+  // compute warps meanwhile
+  //   1. store a - 2 (slot 0) and put gate 1 of a into A  -> ready1[0]
+  //   2. store b - 2 (slot 1) and put gate 1 of b into A  -> ready1[1]
+  //   3. transpose a into gate 2's groups in A             -> ready2[0]
+  //   4. transpose b                                      -> ready2[1]
+  // so every step's SM work overlaps a product issued earlier, and no
+  // compute warp waits for the issue of a product.
+  if (warp >= int(kComputeWarps)) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kIssueRegs));
+    if (tid == kThreads) {
+      uint32_t n10 = 0, n11 = 0, n20 = 0, n21 = 0;  // products issued per slot and gate
+      const uint32_t iters32 = uint32_t(my_iters), periods32 = uint32_t(periods);  // at most 2^27 (n <= 40)
+#pragma unroll 1
+      for (uint32_t j = 0; j < periods32; ++j) {
+        const bool hb = 2 * j + 1 < iters32;
+        const uint32_t par = j & 1;
+        if (!wait_or_abort(smem_addr(&ready1[0]), par, &abort, status)) break;
+        issue_pair_products(tmem + kTmemA, bmat1, tmem, smem_addr(&done1[0]));
+        ++n10;
+        if (hb) {
+          if (!wait_or_abort(smem_addr(&ready1[1]), par, &abort, status)) break;
+          issue_pair_products(tmem + kTmemA + 128, bmat1, tmem + 128, smem_addr(&done1[1]));
+          ++n11;
+        }
+        if (!wait_or_abort(smem_addr(&ready2[0]), par, &abort, status)) break;
+        issue_pair_products(tmem + kTmemA, bmat2, tmem, smem_addr(&done2[0]));
+        ++n20;
+        if (hb) {
+          if (!wait_or_abort(smem_addr(&ready2[1]), par, &abort, status)) break;
+          issue_pair_products(tmem + kTmemA + 128, bmat2, tmem + 128, smem_addr(&done2[1]));
+          ++n21;
+        }
+      }
+      // Every issued product completes before the tensor memory is freed
+      // (bounded: after a timeout a barrier may never complete).
+      if (n10 > 0) wait_products(smem_addr(&done1[0]), (n10 - 1) & 1);
+      if (n11 > 0) wait_products(smem_addr(&done1[1]), (n11 - 1) & 1);
+      if (n20 > 0) wait_products(smem_addr(&done2[0]), (n20 - 1) & 1);
+      if (n21 > 0) wait_products(smem_addr(&done2[1]), (n21 - 1) & 1);
     }
-    tc_fence_before();
-    if (__syncthreads_or(failed)) return false;
-    if (have && tid == 0) issue_products_tmem_a<6>(tmem + acol, bmat1, tmem + dcol, smem_addr(&bar1[b]));
-    if (li > 0) {
-      // Store iteration li - 1: gate 2's products in the other buffers.
-      const uint32_t pb = b ^ 1u;
-      const uint32_t pparity = uint32_t(((li - 1) >> 1) & 1);
+  } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kComputeRegs));
+    const uint32_t lanes = (uint32_t(warp & 3) * 32u) << 16;
+    // This thread's group r and member chunk (members 16 chunk .. + 15), for
+    // either gate: HBM offset of its group and chunk, and its position
+    // (swizzled) in the transpose buffer; member i adds lo*[i] / XORs llo*[i].
+    uint64_t gb1 = chunk == 0 ? g.hi1[0] : chunk == 1 ? g.hi1[1] : chunk == 2 ? g.hi1[2] : g.hi1[3];
+    uint64_t gb2 = chunk == 0 ? g.hi2[0] : chunk == 1 ? g.hi2[1] : chunk == 2 ? g.hi2[2] : g.hi2[3];
+    uint32_t lb1 = chunk == 0 ? g.lhi1[0] : chunk == 1 ? g.lhi1[1] : chunk == 2 ? g.lhi1[2] : g.lhi1[3];
+    uint32_t lb2 = chunk == 0 ? g.lhi2[0] : chunk == 1 ? g.lhi2[1] : chunk == 2 ? g.lhi2[2] : g.lhi2[3];
+#pragma unroll
+    for (int j = 0; j < 7; ++j)
+      if ((r >> j) & 1u) {
+        gb1 += g.grp1[j];
+        gb2 += g.grp2[j];
+        lb1 ^= g.lgrp1[j];
+        lb2 ^= g.lgrp2[j];
+      }
+    // Iteration bases (the bits outside I), advanced by a running deposit
+    // in iteration order, one for the loads and one for the stores.
+    const uint64_t dstep = insert_zeros(gridDim.x, ibits, 13);
+    uint64_t dload = insert_zeros(blockIdx.x, ibits, 13), dstore = dload, dpre = dload;
+    int failed = 0;
+
+    auto load = [&](float2 (&x)[16]) {
+      load16<VW1>(psi, dload + gb1, g.lo1, x);
+      dload = dep_add(dload, dstep, g.imask);
+    };
+    // Warp-uniform wait (tcgen05.ld and .st after it are warp-wide).
+    auto wait = [&](uint64_t* bar, uint32_t parity) {
+      const bool ok = __all_sync(0xffffffffu, wait_or_abort(smem_addr(bar), parity, &abort, status));
+      if (!ok) failed = 1;
+      return ok;
+    };
+    // The warp's tensor-memory writes and reads are done: one arrival.
+    auto arrive = [&](uint64_t* bar) {
+      tc_fence_before();
+      __syncwarp();
+      if ((tid & 31) == 0) mbar_arrive(smem_addr(bar));
+    };
+    // Gate 2's products in slot s (the next iteration in store order) to HBM.
+    auto store_slot = [&](uint32_t s, uint32_t parity) {
       const uint64_t base = dstore + gb2;
       dstore = dep_add(dstore, dstep, g.imask);
-      // Warp-uniform outcome: tcgen05.ld below is a warp-wide instruction.
-      if (!__all_sync(0xffffffffu, wait_products(smem_addr(&bar2[pb]), pparity))) {
-        failed = 1;
-        atomicExch(status, 1);
-      } else {
+      if (failed || !wait(&done2[s], parity)) return;
+      tc_fence_after();
+      const uint32_t taddr = tmem + lanes + s * 128 + 16 * chunk;
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        float re[8], im[8];
+        tmem_ld8(taddr + 8 * hh, re);
+        tmem_ld8(taddr + D + 8 * hh, im);
+        tmem_wait_ld();
+        store8<VW2>(psi, base, g.lo2, hh, re, im);
+      }
+    };
+    auto write_gate1 = [&](uint32_t s, float2 (&x)[16], bool more) {
+      if (failed) return;
+      const uint32_t acol = tmem + lanes + kTmemA + s * 128;
+      write_a8_tmem<6>(x, acol, chunk, 0);
+      write_a8_tmem<6>(x + 8, acol, chunk, 1);
+      if (more) load(x);
+      tmem_wait_st();
+    };
+    // Gate 1's products in slot s through the transpose buffer into gate
+    // 2's groups in slot s's A; false when the CTA stops.
+    auto transpose = [&](uint32_t s, uint32_t parity) -> bool {
+      if (!failed && wait(&done1[s], parity)) {
         tc_fence_after();
-        const uint32_t taddr = tmem + lanes + pb * 128 + 16 * chunk;
+        const uint32_t taddr = tmem + lanes + s * 128 + 16 * chunk;
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
           float re[8], im[8];
           tmem_ld8(taddr + 8 * hh, re);
           tmem_ld8(taddr + D + 8 * hh, im);
           tmem_wait_ld();
-          store8<VW2>(psi, base, lo2, hh, re, im);
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+            *reinterpret_cast<float2*>(xbytes + (lb1 ^ g.llo1[8 * hh + i])) = make_float2(re[i], im[i]);
         }
       }
-    }
-    if (have && !failed) {
-      // Gate 1's products of iteration li into the transpose buffer.
-      if (!__all_sync(0xffffffffu, wait_products(smem_addr(&bar1[b]), parity))) {
-        failed = 1;
-        atomicExch(status, 1);
-      } else {
-        tc_fence_after();
-        const uint32_t taddr = tmem + lanes + dcol + 16 * chunk;
-#pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
-          float re[8], im[8];
-          tmem_ld8(taddr + 8 * hh, re);
-          tmem_ld8(taddr + D + 8 * hh, im);
-          tmem_wait_ld();
-#pragma unroll
-          for (int i = 0; i < 8; ++i) xbuf[lb1 ^ g.llo1[8 * hh + i]] = make_float2(re[i], im[i]);
-        }
-      }
-    }
-    tc_fence_before();
-    if (__syncthreads_or(failed)) return false;
-    if (have) {
-      // Gate 2's groups from the transpose buffer into A.
+      if (compute_sync_or(failed)) return false;
+      const uint32_t acol = tmem + lanes + kTmemA + s * 128;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         float2 m[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) m[i] = xbuf[lb2 ^ g.llo2[8 * q + i]];
-        write_a8_tmem<6>(m, tmem + lanes + acol, chunk, q);
+        for (int i = 0; i < 8; ++i) m[i] = *reinterpret_cast<const float2*>(xbytes + (lb2 ^ g.llo2[8 * q + i]));
+        write_a8_tmem<6>(m, acol, chunk, q);
       }
       tmem_wait_st();
+      arrive(&ready2[s]);
+      // The buffer is free for the next transpose once every warp read it.
+      return !compute_sync_or(0);
+    };
+
+    float2 xa[16], xb[16];
+    if (my_iters > 0) load(xa);
+    if (my_iters > 1) load(xb);
+    for (uint64_t j = 0; j < periods; ++j) {
+      const bool hb = 2 * j + 1 < my_iters;
+      const uint32_t par = uint32_t(j & 1), ppar = uint32_t((j + 1) & 1);
+      if (j > 0) store_slot(0, ppar);
+      write_gate1(0, xa, 2 * j + 2 < my_iters);
+      arrive(&ready1[0]);
+      if (j > 0) store_slot(1, ppar);
+      if (hb) {
+        write_gate1(1, xb, 2 * j + 3 < my_iters);
+        arrive(&ready1[1]);
+      }
+      if (!transpose(0, par)) {
+        failed = 1;
+        break;
+      }
+      if (hb && !transpose(1, par)) {
+        failed = 1;
+        break;
+      }
     }
-    tc_fence_before();
-    __syncthreads();
-    if (have && tid == 0) issue_products_tmem_a<6>(tmem + acol, bmat2, tmem + dcol, smem_addr(&bar2[b]));
-    return have;
-  };
-  // Two register sets in flight, so each iteration's loads are issued two
-  // iterations ahead of their use; the step after the last iteration only
-  // stores it.
-  float2 xa[16], xb[16];
-  if (my_iters > 0) load(xa);
-  if (my_iters > 1) load(xb);
-  if (my_iters > 0) {
-    for (uint64_t li = 0;; li += 2) {
-      if (!step(li, xa)) break;
-      if (!step(li + 1, xb)) break;
+    if (!failed && periods > 0) {
+      const uint32_t last = uint32_t((periods - 1) & 1);
+      store_slot(0, last);
+      if (my_iters % 2 == 0) store_slot(1, last);
     }
+    if (failed) abort = 1;
   }
   tc_fence_before();
   __syncthreads();
@@ -264,10 +404,16 @@ void launch_pair(StateImpl& s, const DenseTcPairGeom& g, const uint8_t* bmats) {
   if (!configured) {
     QVDG_CUDA(cudaFuncSetAttribute(k_dense_tc_pair<VW1, VW2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(smem)));
+    // The register split (setmaxnreg) must fit in what the CTA is launched
+    // with, or the compute warps would wait for registers forever.
+    cudaFuncAttributes fa{};
+    QVDG_CUDA(cudaFuncGetAttributes(&fa, k_dense_tc_pair<VW1, VW2>));
+    if (uint64_t(fa.numRegs) * kPairThreads < uint64_t(kThreads) * kComputeRegs + 128ull * kIssueRegs)
+      throw Error(QVDG_ERR_INVALID, "internal: pair kernel compiled with too few registers for its register split");
     configured = true;
   }
   const unsigned grid = unsigned(std::min<uint64_t>(g.iters, uint64_t(s.sms)));
-  k_dense_tc_pair<VW1, VW2><<<grid, kThreads, smem, s.stream>>>(static_cast<float2*>(s.amp), g, bmats, s.status);
+  k_dense_tc_pair<VW1, VW2><<<grid, kPairThreads, smem, s.stream>>>(static_cast<float2*>(s.amp), g, bmats, s.status);
   QVDG_LAUNCH_CHECK();
 }
 
@@ -383,13 +529,13 @@ DenseTcPairGeom dense_tc_pair_geom(uint32_t n, const std::vector<uint32_t>& t1, 
   for (int k = 0; k < 2; ++k) {
     const std::vector<uint32_t>& t = *tg[k];
     uint64_t* grp_off = k == 0 ? g.grp1 : g.grp2;
-    uint16_t* lgrp = k == 0 ? g.lgrp1 : g.lgrp2;
+    uint32_t* lgrp = k == 0 ? g.lgrp1 : g.lgrp2;
     for (int j = 0; j < 7; ++j) {
       grp_off[j] = uint64_t(1) << grp[k][j];
-      lgrp[j] = uint16_t(swz(1u << local(grp[k][j])));
+      lgrp[j] = 8 * swz(1u << local(grp[k][j]));
     }
     uint64_t* hi = k == 0 ? g.hi1 : g.hi2;
-    uint16_t* lhi = k == 0 ? g.lhi1 : g.lhi2;
+    uint32_t* lhi = k == 0 ? g.lhi1 : g.lhi2;
     for (uint32_t c = 0; c < 4; ++c) {
       uint64_t o = 0;
       uint32_t l = 0;
@@ -399,10 +545,10 @@ DenseTcPairGeom dense_tc_pair_geom(uint32_t n, const std::vector<uint32_t>& t1, 
           l |= 1u << local(t[4 + j]);
         }
       hi[c] = o;
-      lhi[c] = uint16_t(swz(l));
+      lhi[c] = 8 * swz(l);
     }
     uint32_t* lo = k == 0 ? g.lo1 : g.lo2;
-    uint16_t* llo = k == 0 ? g.llo1 : g.llo2;
+    uint32_t* llo = k == 0 ? g.llo1 : g.llo2;
     for (uint32_t i = 0; i < 16; ++i) {
       uint64_t o = 0;
       uint32_t l = 0;
@@ -412,7 +558,7 @@ DenseTcPairGeom dense_tc_pair_geom(uint32_t n, const std::vector<uint32_t>& t1, 
           l |= 1u << local(t[j]);
         }
       lo[i] = uint32_t(o);
-      llo[i] = uint16_t(swz(l));
+      llo[i] = 8 * swz(l);
     }
   }
   // Members 4m..4m+3 are neighbours in HBM when bits 0 and 1 are targets,
