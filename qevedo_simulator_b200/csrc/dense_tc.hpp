@@ -56,6 +56,9 @@ DenseTcPairGeom dense_tc_pair_geom(uint32_t n, const std::vector<uint32_t>& t1, 
                                    size_t b1_offset, size_t b2_offset);
 // Whether two gates (physical targets, no controls) can share a pair pass.
 bool dense_tc_pair_ok(uint32_t n, int bits, const std::vector<uint32_t>& t1, const std::vector<uint32_t>& t2);
+// The layout part of that test on physical target masks (6 targets each;
+// complex64, at least 14 qubits and targets below bit 32 assumed).
+bool dense_tc_pair_masks_ok(uint64_t m1, uint64_t m2);
 void launch_dense_tc_pair(StateImpl& s, const DenseTcPairGeom& g, const uint8_t* tc_blob);
 
 // Whether a dense gate with these targets (physical) and controls runs on

@@ -448,30 +448,39 @@ std::vector<uint32_t> pair_bits(const std::vector<uint32_t>& t1, const std::vect
 // runs of at least 16 amplitudes (128 bytes), or of at least 4 within 1024
 // amplitudes. Elsewhere a warp touches many scattered sectors and the pass
 // runs several times slower than two single passes (measured at 30 qubits).
-bool pair_gate_coalesced(const std::vector<uint32_t>& t, const std::vector<uint32_t>& ibits) {
-  const uint32_t vw = t[0] == 0 ? (t[1] == 1 ? 4u : 2u) : 1u;
-  std::vector<uint32_t> lanes;
-  for (uint32_t q : ibits)
-    if (lanes.size() < 5 && std::find(t.begin(), t.end(), q) == t.end()) lanes.push_back(q);
-  uint32_t run = vw, next = vw == 4 ? 2u : (vw == 2 ? 1u : 0u);
-  for (uint32_t q : lanes) {
-    if (q != next) break;
-    run *= 2;
-    ++next;
+// `t`: the gate's physical targets, `imask`: the iteration's bits.
+bool pair_gate_coalesced(uint64_t t, uint64_t imask) {
+  const uint32_t vw = (t & 1) ? ((t & 2) ? 4u : 2u) : 1u;
+  uint64_t rest = imask & ~t, lanes = 0;
+  for (int k = 0; k < 5 && rest; ++k) {
+    const uint64_t low = rest & (~rest + 1);
+    lanes |= low;
+    rest ^= low;
   }
-  return run >= 16 || (run >= 4 && lanes.back() <= 9);
+  const uint32_t next = vw == 4 ? 2u : (vw == 2 ? 1u : 0u);
+  // Lane bits next, next + 1, ... each double the contiguous run.
+  const uint32_t k = uint32_t(__builtin_ctzll(~(lanes >> next)));
+  const uint32_t run = vw << std::min(k, 5u);
+  const uint32_t last = lanes ? uint32_t(63 - __builtin_clzll(lanes)) : 0u;
+  return run >= 16 || (run >= 4 && last <= 9);
 }
 
 }  // namespace
 
+bool dense_tc_pair_masks_ok(uint64_t m1, uint64_t m2) {
+  if (__builtin_popcountll(m1) != 6 || __builtin_popcountll(m2) != 6) return false;
+  uint64_t imask = m1 | m2;  // both gates' targets and the lowest other bits, 13 in all
+  while (__builtin_popcountll(imask) < 13) imask |= ~imask & (imask + 1);
+  return pair_gate_coalesced(m1, imask) && pair_gate_coalesced(m2, imask);
+}
+
 bool dense_tc_pair_ok(uint32_t n, int bits, const std::vector<uint32_t>& t1, const std::vector<uint32_t>& t2) {
   if (bits != 32 || n < 14 || t1.size() != 6 || t2.size() != 6) return false;
   if (!dense_tc_ok(n, bits, t1, 0) || !dense_tc_ok(n, bits, t2, 0)) return false;
-  std::vector<uint32_t> a(t1), b(t2);
-  std::sort(a.begin(), a.end());
-  std::sort(b.begin(), b.end());
-  const std::vector<uint32_t> ibits = pair_bits(a, b);
-  return pair_gate_coalesced(a, ibits) && pair_gate_coalesced(b, ibits);
+  uint64_t m1 = 0, m2 = 0;
+  for (uint32_t q : t1) m1 |= uint64_t(1) << q;
+  for (uint32_t q : t2) m2 |= uint64_t(1) << q;
+  return dense_tc_pair_masks_ok(m1, m2);
 }
 
 DenseTcPairGeom dense_tc_pair_geom(uint32_t n, const std::vector<uint32_t>& t1, const std::vector<uint32_t>& t2,

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <functional>
+#include <random>
 #include <cstring>
 #include <string>
 
@@ -171,6 +172,120 @@ Target target_of(const StateImpl& s) {
   t.layout = s.layout;
   return t;
 }
+
+namespace {
+
+// Logical qubits a pass touches (targets, controls, a block's qubits).
+uint64_t pass_qubits(const PlannedPass& p) {
+  uint64_t m = 0;
+  for (const HOp& op : p.ops) {
+    for (uint32_t q : op.targets) m |= uint64_t(1) << q;
+    for (auto& c : op.controls) m |= uint64_t(1) << c.first;
+  }
+  for (uint32_t q : p.block_qubits) m |= uint64_t(1) << q;
+  return m;
+}
+
+// The zero-start prefix of a run from |0...0>: the plain single-op passes
+// before the one after which every qubit has been touched.
+size_t zero_prefix(const std::vector<PlannedPass>& passes, uint32_t n) {
+  const uint64_t all = n >= 64 ? ~uint64_t(0) : (uint64_t(1) << n) - 1;
+  uint64_t touched = 0;
+  size_t k = 0;
+  for (const PlannedPass& p : passes) {
+    if (p.staged || p.block || p.ops.size() != 1) break;
+    touched |= pass_qubits(p);
+    if (touched == all) break;
+    ++k;
+  }
+  return k;
+}
+
+constexpr size_t kPairWindow = 8;  // how far ahead a pass looks for its partner
+
+// Whether a pass is a candidate for a pair pass by its structure: one dense
+// 6-qubit op without controls.
+bool pair_candidate(const PlannedPass& p) {
+  return !p.staged && !p.block && p.ops.size() == 1 && p.ops[0].controls.empty() && !p.ops[0].diagonal &&
+         p.ops[0].targets.size() == 6;
+}
+
+// Pairs that the pairing below would make on `layout` (logical -> physical),
+// by the layout test alone.
+size_t count_pairs(const std::vector<PlannedPass>& passes, size_t from, const std::vector<uint64_t>& logical,
+                   const std::vector<uint64_t>& touches, const std::vector<char>& candidate,
+                   const std::vector<uint32_t>& layout) {
+  std::vector<uint64_t> phys(passes.size(), 0);
+  for (size_t i = 0; i < passes.size(); ++i)
+    if (candidate[i])
+      for (uint64_t m = logical[i]; m; m &= m - 1) phys[i] |= uint64_t(1) << layout[__builtin_ctzll(m)];
+  std::vector<char> used(passes.size(), 0);
+  size_t pairs = 0;
+  for (size_t i = 0; i < passes.size(); ++i) {
+    if (used[i]) continue;
+    used[i] = 1;
+    if (i < from || !candidate[i]) continue;
+    uint64_t between = 0;
+    for (size_t j = i + 1; j < passes.size() && j <= i + kPairWindow; ++j) {
+      if (used[j]) continue;
+      if (candidate[j] && !(touches[j] & between) && dense_tc_pair_masks_ok(phys[i], phys[j])) {
+        used[j] = 1;
+        ++pairs;
+        break;
+      }
+      between |= touches[j];
+    }
+  }
+  return pairs;
+}
+
+// From |0...0> a run may take any layout for free. Physical bits 0-3 set a
+// single tensor-core pass's variant and cost; the bits above them only
+// decide which passes may pair (their warps' accesses stay coalesced). So
+// the logical qubits on physical bits 4..min(n, 32) - 1 are permuted to
+// pair more passes: hill climbing over swaps of two of them (moves that
+// keep the count are taken too), `steps` tries from a fixed seed. On the
+// 30-qubit grid circuit at fusion 6 the planner's layout pairs 6 of the 34
+// passes after the zero-start prefix; permuted, 10. Returns whether
+// `layout` changed.
+bool pair_layout(const std::vector<PlannedPass>& passes, uint32_t n, int steps, std::vector<uint32_t>& layout) {
+  const size_t from = zero_prefix(passes, n);
+  std::vector<uint64_t> logical(passes.size(), 0), touches(passes.size(), 0);
+  std::vector<char> candidate(passes.size(), 0);
+  size_t count = 0;
+  for (size_t i = 0; i < passes.size(); ++i) {
+    touches[i] = pass_qubits(passes[i]);
+    candidate[i] = pair_candidate(passes[i]);
+    if (candidate[i]) {
+      for (uint32_t q : passes[i].ops[0].targets) logical[i] |= uint64_t(1) << q;
+      count += i >= from;
+    }
+  }
+  if (count < 2) return false;
+  std::vector<uint32_t> movable;  // logical qubits on the bits that may move
+  for (uint32_t q = 0; q < n; ++q)
+    if (layout[q] >= 4 && layout[q] < std::min<uint32_t>(n, 32)) movable.push_back(q);
+  if (movable.size() < 2) return false;
+  std::vector<uint32_t> trial = layout;
+  const size_t start = count_pairs(passes, from, logical, touches, candidate, trial);
+  size_t best = start;
+  std::mt19937 rng(2024);
+  for (int s = 0; s < steps; ++s) {
+    const uint32_t a = movable[rng() % movable.size()], b = movable[rng() % movable.size()];
+    if (a == b) continue;
+    std::swap(trial[a], trial[b]);
+    const size_t c = count_pairs(passes, from, logical, touches, candidate, trial);
+    if (c >= best)
+      best = c;
+    else
+      std::swap(trial[a], trial[b]);
+  }
+  if (best <= start) return false;
+  layout = trial;
+  return true;
+}
+
+}  // namespace
 
 Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_options& opt,
                       FusionSearch search, bool from_zero, std::vector<HOp>* fused) {
@@ -380,15 +495,20 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       p.ops.resize(1);
       products.push_back(gi);
     }
-    // Each product and, for a tensor-core pass, its bf16 matrices (on the
-    // layout the passes run with) in one task.
+    // The products, then (on the layout the passes run with) the
+    // tensor-core passes' bf16 matrices, on host threads.
+    const bool wide = max_fused >= 5 && products.size() >= 8;
+    parallel_for(products.size(), [&](size_t j) { passes[products[j]].ops[0] = fuse_group(ops, groups[products[j]]); },
+                 wide ? 0u : 1u);
+    if (pairs && from_zero && t.n >= 14) {
+      std::vector<uint32_t> layout = prog.run_layout.empty() ? t.layout : prog.run_layout;
+      if (pair_layout(passes, t.n, search == FusionSearch::Thorough ? 1024 : 256, layout)) prog.run_layout = layout;
+    }
     Target rt = t;
     if (!prog.run_layout.empty()) rt.layout = prog.run_layout;
     blobs.resize(passes.size());
-    const bool wide = max_fused >= 5 && products.size() >= 8;
     parallel_for(products.size(), [&](size_t j) {
       PlannedPass& p = passes[products[j]];
-      p.ops[0] = fuse_group(ops, groups[products[j]]);
       if (plain_tc_eligible(rt, p, prog.cfg)) blobs[products[j]] = plain_tc_blob(rt, p.ops[0]);
     }, wide ? 0u : 1u);
   }
@@ -408,20 +528,7 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
   // Passes that may share a pass with the next one: after the zero-start
   // prefix of a run from |0...0> (those passes keep their own variants).
   size_t pair_from = passes.size();
-  if (pairs) {
-    pair_from = 0;
-    if (from_zero) {
-      uint64_t touched = 0;
-      const uint64_t all = t.n >= 64 ? ~uint64_t(0) : (uint64_t(1) << t.n) - 1;
-      for (const PlannedPass& p : passes) {
-        if (p.staged || p.block || p.ops.size() != 1) break;
-        for (uint32_t q : p.ops[0].targets) touched |= uint64_t(1) << q;
-        for (auto& c : p.ops[0].controls) touched |= uint64_t(1) << c.first;
-        if (touched == all) break;
-        ++pair_from;
-      }
-    }
-  }
+  if (pairs) pair_from = from_zero ? zero_prefix(passes, t.n) : 0;
   // Pairing: each pass after the zero-start prefix takes as its partner the
   // first of the next few passes that pairs with it (dense_tc_pair_ok) and
   // shares no qubit with any pass between them, moved up next to it (the
@@ -435,16 +542,6 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       return !q.staged && !q.block && q.ops.size() == 1 && q.ops[0].controls.empty() && !blobs[i].blob.empty() &&
              q.ops[0].targets.size() == 6;
     };
-    auto mask = [&](size_t i) {
-      uint64_t m = 0;
-      for (const HOp& op : passes[i].ops) {
-        for (uint32_t q : op.targets) m |= uint64_t(1) << q;
-        for (auto& c : op.controls) m |= uint64_t(1) << c.first;
-      }
-      for (uint32_t q : passes[i].block_qubits) m |= uint64_t(1) << q;
-      return m;
-    };
-    constexpr size_t kWindow = 8;
     std::vector<char> used(passes.size(), 0);
     for (size_t i = 0; i < passes.size(); ++i) {
       if (used[i]) continue;
@@ -453,9 +550,9 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
       pair_next.push_back(0);
       if (!pairs || i < pair_from || !eligible(i)) continue;
       uint64_t between = 0;
-      for (size_t j = i + 1; j < passes.size() && j <= i + kWindow; ++j) {
+      for (size_t j = i + 1; j < passes.size() && j <= i + kPairWindow; ++j) {
         if (used[j]) continue;
-        if (eligible(j) && !(mask(j) & between) &&
+        if (eligible(j) && !(pass_qubits(passes[j]) & between) &&
             dense_tc_pair_ok(tt.n, tt.bits, blobs[i].targets, blobs[j].targets)) {
           used[j] = 1;
           pair_next.back() = 1;
@@ -463,7 +560,7 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
           pair_next.push_back(0);
           break;
         }
-        between |= mask(j);
+        between |= pass_qubits(passes[j]);
       }
     }
   }
