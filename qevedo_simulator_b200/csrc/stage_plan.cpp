@@ -239,15 +239,39 @@ size_t count_pairs(const std::vector<PlannedPass>& passes, size_t from, const st
   return pairs;
 }
 
-// From |0...0> a run may take any layout for free. Physical bits 0-3 set a
-// single tensor-core pass's variant and cost; the bits above them only
-// decide which passes may pair (their warps' accesses stay coalesced). So
-// the logical qubits on physical bits 4..min(n, 32) - 1 are permuted to
-// pair more passes: hill climbing over swaps of two of them (moves that
-// keep the count are taken too), `steps` tries from a fixed seed. On the
-// 30-qubit grid circuit at fusion 6 the planner's layout pairs 6 of the 34
-// passes after the zero-start prefix; permuted, 10. Returns whether
-// `layout` changed.
+// From |0...0> a run may take any layout for free.
+//
+// Physical bit 0: a qubit that no pass has touched yet becomes a control of
+// value 0 in the zero-start passes, halving the amplitudes they move, except
+// on bits 0-1, where it would save no DRAM sectors. So bit 0 takes the
+// qubit touched first among those on bits 4 and up, where it touched later
+// (30-qubit grid circuit: the last qubits touched then both sit on high
+// bits, and four zero-start passes move a quarter of the state instead of
+// half). Returns whether `layout` changed.
+bool zero_start_layout(const std::vector<PlannedPass>& passes, uint32_t n, std::vector<uint32_t>& layout) {
+  const size_t prefix = zero_prefix(passes, n);
+  std::vector<size_t> first(n, passes.size());  // first pass touching each logical qubit
+  for (size_t i = passes.size(); i-- > 0;)
+    for (uint64_t m = pass_qubits(passes[i]); m; m &= m - 1) first[__builtin_ctzll(m)] = i;
+  uint32_t q0 = 0;
+  while (layout[q0] != 0) ++q0;
+  if (first[q0] == 0 || prefix == 0) return false;
+  uint32_t pick = q0;
+  for (uint32_t q = 0; q < n; ++q)
+    if (layout[q] >= 4 && layout[q] < std::min<uint32_t>(n, 32) && first[q] < first[pick]) pick = q;
+  if (pick == q0) return false;
+  std::swap(layout[q0], layout[pick]);
+  return true;
+}
+
+// Physical bits 0-3 set a single tensor-core pass's variant and cost; the
+// bits above them only decide which passes may pair (their warps' accesses
+// stay coalesced). So the logical qubits on physical bits 4..min(n, 32) - 1
+// are permuted to pair more passes: hill climbing over swaps of two of them
+// (moves that keep the count are taken too), `steps` tries from a fixed
+// seed. On the 30-qubit grid circuit at fusion 6 the planner's layout pairs
+// 6 of the 34 passes after the zero-start prefix; permuted, 10. Returns
+// whether `layout` changed.
 bool pair_layout(const std::vector<PlannedPass>& passes, uint32_t n, int steps, std::vector<uint32_t>& layout) {
   const size_t from = zero_prefix(passes, n);
   std::vector<uint64_t> logical(passes.size(), 0), touches(passes.size(), 0);
@@ -500,9 +524,11 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
     const bool wide = max_fused >= 5 && products.size() >= 8;
     parallel_for(products.size(), [&](size_t j) { passes[products[j]].ops[0] = fuse_group(ops, groups[products[j]]); },
                  wide ? 0u : 1u);
-    if (pairs && from_zero && t.n >= 14) {
+    if (prog.cfg.plain_tensor && max_fused >= 5 && from_zero && t.n >= 14) {
       std::vector<uint32_t> layout = prog.run_layout.empty() ? t.layout : prog.run_layout;
-      if (pair_layout(passes, t.n, search == FusionSearch::Thorough ? 1024 : 256, layout)) prog.run_layout = layout;
+      bool moved = zero_start_layout(passes, t.n, layout);
+      if (pairs) moved = pair_layout(passes, t.n, search == FusionSearch::Thorough ? 1024 : 256, layout) || moved;
+      if (moved) prog.run_layout = layout;
     }
     Target rt = t;
     if (!prog.run_layout.empty()) rt.layout = prog.run_layout;
