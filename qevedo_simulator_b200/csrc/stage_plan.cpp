@@ -210,103 +210,185 @@ bool pair_candidate(const PlannedPass& p) {
          p.ops[0].targets.size() == 6;
 }
 
-// Pairs that the pairing below would make on `layout` (logical -> physical),
-// by the layout test alone.
-size_t count_pairs(const std::vector<PlannedPass>& passes, size_t from, const std::vector<uint64_t>& logical,
-                   const std::vector<uint64_t>& touches, const std::vector<char>& candidate,
-                   const std::vector<uint32_t>& layout) {
-  std::vector<uint64_t> phys(passes.size(), 0);
-  for (size_t i = 0; i < passes.size(); ++i)
-    if (candidate[i])
-      for (uint64_t m = logical[i]; m; m &= m - 1) phys[i] |= uint64_t(1) << layout[__builtin_ctzll(m)];
-  std::vector<char> used(passes.size(), 0);
-  size_t pairs = 0;
-  for (size_t i = 0; i < passes.size(); ++i) {
-    if (used[i]) continue;
-    used[i] = 1;
-    if (i < from || !candidate[i]) continue;
-    uint64_t between = 0;
-    for (size_t j = i + 1; j < passes.size() && j <= i + kPairWindow; ++j) {
-      if (used[j]) continue;
-      if (candidate[j] && !(touches[j] & between) && dense_tc_pair_masks_ok(phys[i], phys[j])) {
-        used[j] = 1;
-        ++pairs;
-        break;
+// What the layout search knows of a plan's passes: the zero-start prefix,
+// each pass's logical target mask and touched qubits, and which passes may
+// pair by their structure.
+struct PairSearch {
+  size_t from = 0;
+  std::vector<uint64_t> logical, touches;
+  std::vector<char> candidate;
+  size_t count = 0;  // candidates after the prefix
+
+  PairSearch(const std::vector<PlannedPass>& passes, uint32_t n)
+      : from(zero_prefix(passes, n)), logical(passes.size(), 0), touches(passes.size(), 0),
+        candidate(passes.size(), 0) {
+    for (size_t i = 0; i < passes.size(); ++i) {
+      touches[i] = pass_qubits(passes[i]);
+      candidate[i] = pair_candidate(passes[i]);
+      if (candidate[i]) {
+        for (uint32_t q : passes[i].ops[0].targets) logical[i] |= uint64_t(1) << q;
+        count += i >= from;
       }
-      between |= touches[j];
     }
   }
-  return pairs;
-}
 
-// From |0...0> a run may take any layout for free.
+  // Pairs that the pairing below would make on `layout` (logical ->
+  // physical), by the layout test alone (about 1.4 us for 45 passes).
+  size_t pairs(const std::vector<uint32_t>& layout) const {
+    const size_t np = logical.size();
+    std::vector<uint64_t> phys(np, 0);
+    for (size_t i = 0; i < np; ++i)
+      if (candidate[i])
+        for (uint64_t m = logical[i]; m; m &= m - 1) phys[i] |= uint64_t(1) << layout[__builtin_ctzll(m)];
+    std::vector<char> used(np, 0);
+    size_t made = 0;
+    for (size_t i = 0; i < np; ++i) {
+      if (used[i]) continue;
+      used[i] = 1;
+      if (i < from || !candidate[i]) continue;
+      uint64_t between = 0;
+      for (size_t j = i + 1; j < np && j <= i + kPairWindow; ++j) {
+        if (used[j]) continue;
+        if (candidate[j] && !(touches[j] & between) && dense_tc_pair_masks_ok(phys[i], phys[j])) {
+          used[j] = 1;
+          ++made;
+          break;
+        }
+        between |= touches[j];
+      }
+    }
+    return made;
+  }
+
+  // Hill climbing over swaps of two `movable` qubits' positions (moves that
+  // keep the count are taken too), `steps` tries per climb, from `layout`
+  // and from `restarts` - 1 shuffles of it; `layout` becomes the best found.
+  // Returns its pair count.
+  size_t climb(const std::vector<uint32_t>& movable, int steps, int restarts, std::mt19937& rng,
+               std::vector<uint32_t>& layout) const {
+    size_t best = pairs(layout);
+    if (movable.size() < 2) return best;
+    std::vector<uint32_t> best_layout = layout;
+    for (int r = 0; r < restarts; ++r) {
+      std::vector<uint32_t> trial = layout;
+      if (r > 0) {
+        std::vector<uint32_t> pos;
+        for (uint32_t q : movable) pos.push_back(trial[q]);
+        std::shuffle(pos.begin(), pos.end(), rng);
+        for (size_t k = 0; k < movable.size(); ++k) trial[movable[k]] = pos[k];
+      }
+      size_t cur = pairs(trial);
+      for (int s = 0; s < steps; ++s) {
+        const uint32_t a = movable[rng() % movable.size()], b = movable[rng() % movable.size()];
+        if (a == b) continue;
+        std::swap(trial[a], trial[b]);
+        const size_t c = pairs(trial);
+        if (c >= cur)
+          cur = c;
+        else
+          std::swap(trial[a], trial[b]);
+      }
+      if (cur > best) {
+        best = cur;
+        best_layout = trial;
+      }
+    }
+    layout = best_layout;
+    return best;
+  }
+};
+
+// From |0...0> a run may take any layout for free; plain tensor-core plans
+// from |0...0> (fusion 5-6) place their qubits as follows. Bits 1-3 keep
+// the planner's choice (they set a single tensor-core pass's variant and
+// cost).
 //
-// Physical bit 0: a qubit that no pass has touched yet becomes a control of
-// value 0 in the zero-start passes, halving the amplitudes they move, except
-// on bits 0-1, where it would save no DRAM sectors. So bit 0 takes the
-// qubit touched first among those on bits 4 and up, where it touched later
-// (30-qubit grid circuit: the last qubits touched then both sit on high
-// bits, and four zero-start passes move a quarter of the state instead of
-// half). Returns whether `layout` changed.
-bool zero_start_layout(const std::vector<PlannedPass>& passes, uint32_t n, std::vector<uint32_t>& layout) {
+// - The top bits: a qubit that no pass has touched yet becomes a control of
+//   value 0 in the zero-start passes, so they move only the amplitudes
+//   where it is 0. The kZeroStartTop qubits touched last are idle in the
+//   heaviest of those passes; on the top bits below min(n, 32) they leave
+//   them contiguous runs of the state.
+// - Bit 0 (and bit 1) inside a DRAM sector saves nothing as a zero control,
+//   so bit 0 takes a qubit touched early: the first touched, or with pair
+//   passes the one among the kBitZeroTries touched first with which the
+//   most passes pair.
+// - With pair passes the bits above 3 (but the top ones) only decide which
+//   passes may pair (their warps' accesses stay coalesced): hill climbing
+//   over their permutations pairs more passes.
+//
+// On the 30-qubit grid circuit at fusion 6: 4.3 -> 3.3 ms of zero-start
+// passes (the last two qubits touched on bits 28-29, a quarter of the
+// state in four of them) and 9-11 pairs instead of 6. Returns whether
+// `layout` changed.
+constexpr size_t kZeroStartTop = 2;
+
+bool zero_start_layout(const std::vector<PlannedPass>& passes, uint32_t n, bool pairs, bool thorough,
+                       std::vector<uint32_t>& layout) {
   const size_t prefix = zero_prefix(passes, n);
+  if (prefix == 0) return false;
+  const std::vector<uint32_t> given = layout;
   std::vector<size_t> first(n, passes.size());  // first pass touching each logical qubit
   for (size_t i = passes.size(); i-- > 0;)
     for (uint64_t m = pass_qubits(passes[i]); m; m &= m - 1) first[__builtin_ctzll(m)] = i;
+  const uint32_t top = std::min<uint32_t>(n, 32);
+  std::vector<uint32_t> at(n);  // physical -> logical
+  auto place = [&](uint32_t q, uint32_t p) {
+    for (uint32_t x = 0; x < n; ++x) at[layout[x]] = x;
+    const uint32_t other = at[p];
+    std::swap(layout[q], layout[other]);
+  };
+  // The top bits.
+  std::vector<uint32_t> late;
+  for (uint32_t q = 0; q < n; ++q)
+    if (layout[q] >= 4 && layout[q] < top && first[q] > 0) late.push_back(q);
+  std::stable_sort(late.begin(), late.end(), [&](uint32_t a, uint32_t b) { return first[a] > first[b]; });
+  if (late.size() > kZeroStartTop) late.resize(kZeroStartTop);
+  uint64_t fixed = 0;
+  for (size_t k = 0; k < late.size(); ++k) {
+    place(late[k], top - 1 - uint32_t(k));
+    fixed |= uint64_t(1) << late[k];
+  }
+  // Bit 0: candidates touched early, on the bits that may move.
   uint32_t q0 = 0;
   while (layout[q0] != 0) ++q0;
-  if (first[q0] == 0 || prefix == 0) return false;
-  uint32_t pick = q0;
+  std::vector<uint32_t> early;
   for (uint32_t q = 0; q < n; ++q)
-    if (layout[q] >= 4 && layout[q] < std::min<uint32_t>(n, 32) && first[q] < first[pick]) pick = q;
-  if (pick == q0) return false;
-  std::swap(layout[q0], layout[pick]);
-  return true;
-}
-
-// Physical bits 0-3 set a single tensor-core pass's variant and cost; the
-// bits above them only decide which passes may pair (their warps' accesses
-// stay coalesced). So the logical qubits on physical bits 4..min(n, 32) - 1
-// are permuted to pair more passes: hill climbing over swaps of two of them
-// (moves that keep the count are taken too), `steps` tries from a fixed
-// seed. On the 30-qubit grid circuit at fusion 6 the planner's layout pairs
-// 6 of the 34 passes after the zero-start prefix; permuted, 10. Returns
-// whether `layout` changed.
-bool pair_layout(const std::vector<PlannedPass>& passes, uint32_t n, int steps, std::vector<uint32_t>& layout) {
-  const size_t from = zero_prefix(passes, n);
-  std::vector<uint64_t> logical(passes.size(), 0), touches(passes.size(), 0);
-  std::vector<char> candidate(passes.size(), 0);
-  size_t count = 0;
-  for (size_t i = 0; i < passes.size(); ++i) {
-    touches[i] = pass_qubits(passes[i]);
-    candidate[i] = pair_candidate(passes[i]);
-    if (candidate[i]) {
-      for (uint32_t q : passes[i].ops[0].targets) logical[i] |= uint64_t(1) << q;
-      count += i >= from;
+    if (layout[q] >= 4 && layout[q] < top && !((fixed >> q) & 1) && first[q] < first[q0]) early.push_back(q);
+  std::stable_sort(early.begin(), early.end(), [&](uint32_t a, uint32_t b) { return first[a] < first[b]; });
+  auto movable_of = [&](const std::vector<uint32_t>& l) {
+    std::vector<uint32_t> mv;
+    for (uint32_t q = 0; q < n; ++q)
+      if (l[q] >= 4 && l[q] < top && !((fixed >> q) & 1)) mv.push_back(q);
+    return mv;
+  };
+  std::mt19937 rng(2024);
+  if (!pairs) {
+    if (!early.empty()) std::swap(layout[q0], layout[early[0]]);
+    return layout != given;
+  }
+  const PairSearch search(passes, n);
+  if (search.count < 2) {
+    if (!early.empty()) std::swap(layout[q0], layout[early[0]]);
+    return layout != given;
+  }
+  // Bit 0 by a short climb per candidate, then the full climb.
+  const size_t tries = std::min<size_t>(early.size(), thorough ? 24 : 8);
+  std::vector<uint32_t> best = layout;
+  size_t best_pairs = 0;
+  bool any = false;
+  for (size_t k = 0; k < tries; ++k) {
+    std::vector<uint32_t> l = layout;
+    std::swap(l[q0], l[early[k]]);
+    const size_t c = search.climb(movable_of(l), 128, thorough ? 2 : 1, rng, l);
+    if (!any || c > best_pairs) {
+      best = l;
+      best_pairs = c;
+      any = true;
     }
   }
-  if (count < 2) return false;
-  std::vector<uint32_t> movable;  // logical qubits on the bits that may move
-  for (uint32_t q = 0; q < n; ++q)
-    if (layout[q] >= 4 && layout[q] < std::min<uint32_t>(n, 32)) movable.push_back(q);
-  if (movable.size() < 2) return false;
-  std::vector<uint32_t> trial = layout;
-  const size_t start = count_pairs(passes, from, logical, touches, candidate, trial);
-  size_t best = start;
-  std::mt19937 rng(2024);
-  for (int s = 0; s < steps; ++s) {
-    const uint32_t a = movable[rng() % movable.size()], b = movable[rng() % movable.size()];
-    if (a == b) continue;
-    std::swap(trial[a], trial[b]);
-    const size_t c = count_pairs(passes, from, logical, touches, candidate, trial);
-    if (c >= best)
-      best = c;
-    else
-      std::swap(trial[a], trial[b]);
-  }
-  if (best <= start) return false;
-  layout = trial;
-  return true;
+  layout = best;
+  search.climb(movable_of(layout), thorough ? 1024 : 256, thorough ? 4 : 2, rng, layout);
+  return layout != given;
 }
 
 }  // namespace
@@ -526,9 +608,7 @@ Program build_program(const Target& t, const std::vector<HOp>& ops, const qvdg_o
                  wide ? 0u : 1u);
     if (prog.cfg.plain_tensor && max_fused >= 5 && from_zero && t.n >= 14) {
       std::vector<uint32_t> layout = prog.run_layout.empty() ? t.layout : prog.run_layout;
-      bool moved = zero_start_layout(passes, t.n, layout);
-      if (pairs) moved = pair_layout(passes, t.n, search == FusionSearch::Thorough ? 1024 : 256, layout) || moved;
-      if (moved) prog.run_layout = layout;
+      if (zero_start_layout(passes, t.n, pairs, search == FusionSearch::Thorough, layout)) prog.run_layout = layout;
     }
     Target rt = t;
     if (!prog.run_layout.empty()) rt.layout = prog.run_layout;
