@@ -50,9 +50,14 @@ METRIC = "30q random-circuit s & HBM GB/s vs peak, tuned vs plain GPU at <=1e-6 
 # ncu captures at 26 qubits (2^26 amplitudes per launch; a full-size launch
 # scales by its amplitude count), by pass kind: 0 k_dense<float,4,2,1>
 # (536.9 MB read + 476.7 MB written), 2 k_dense_tc<6,0> (537.0 + 476.5 MB),
-# 3 k_dense_tc_tile<4,2> (536.9 + 477.6 MB).
+# 3 k_dense_tc_tile<4,2> (536.9 + 477.6 MB), 5 k_dense_tc_pair<4,2>
+# (537.1 + 477.3 MB).
 TRAFFIC_BYTES_PER_AMP = {0: (536.9e6 + 476.7e6) / 2 ** 26, 2: (537.0e6 + 476.5e6) / 2 ** 26,
-                         3: (536.9e6 + 477.6e6) / 2 ** 26}
+                         3: (536.9e6 + 477.6e6) / 2 ** 26, 5: (537.1e6 + 477.3e6) / 2 ** 26}
+# Tensor-core work a pair pass executes per amplitude: two gates, each three
+# bf16 products of the real block form (M = N = K = 128 per 64-amplitude
+# group), 2 x 3 x 2 x 128^3 / 8192.
+PAIR_FLOPS_PER_AMP = 2 * 3 * 2 * 128 ** 3 / 8192
 KERNEL_OF_KIND = {0: "k_dense<float,K,...> (plain fused-gate pass, CUDA cores)",
                   2: "k_dense_tc<K,VW> (plain fused-gate pass, tensor cores)",
                   3: "k_dense_tc_tile<K,NB> (plain fused-gate pass on bits 1-3, tensor cores)",
@@ -78,8 +83,9 @@ def measured_peaks() -> dict:
     if os.path.exists(path):
         with open(path) as f:
             d = json.load(f)
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops_sustained": float(d.get("bf16_tflops_sustained", 1400.0)),
+                "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
 
 
 class ClockSampler:
@@ -386,6 +392,27 @@ def run_ours(args, rank: int, world: int):
                 "traffic_source": "ncu capture of the same kernel at 26 qubits, scaled by amplitudes"
                 if args.traffic is None and dom in TRAFFIC_BYTES_PER_AMP else ("--traffic" if args.traffic else None),
                 "launches_per_step": int(dsec.size // max(1, args.steps))}
+    if dom == 5:
+        # A pair pass applies two gates per state pass; it is bound by the
+        # tensor pipe and shared-memory traffic rather than HBM.
+        flops = PAIR_FLOPS_PER_AMP * 2 ** n
+        roofline["gates_per_launch"] = 2
+        roofline["gate_pass_gbs"] = 2 * achieved
+        roofline["tensor"] = {"achieved": flops / avg / 1e12, "peak": peaks["bf16_tflops_sustained"],
+                              "unit": "TFLOP/s", "frac": flops / avg / 1e12 / peaks["bf16_tflops_sustained"],
+                              "flops_per_launch": flops,
+                              "note": "executed bf16 products (bf16x3 of the real block form) vs sustained bf16 peak"}
+    # Every whole-state pass kind of the tuned plan, the same way.
+    roofline["by_kernel"] = []
+    for k in (0, 1, 2, 3, 5):
+        ks, kb = sec[kind == k], byt[kind == k]
+        if ks.size == 0:
+            continue
+        gbs = float(kb.sum() / ks.sum() / 1e9)
+        roofline["by_kernel"].append({"kernel": KERNEL_OF_KIND.get(k, "stage kernel"), "pass_kind": k,
+                                      "launches_per_step": int(ks.size // max(1, args.steps)),
+                                      "avg_launch_s": float(ks.mean()), "achieved": gbs,
+                                      "frac": gbs / peaks["hbm_gbs"], "share_of_passes": float(ks.sum() / sec.sum())})
     # Whole run: the bytes every pass of a step moved (zero-start passes at
     # the share of the state they touch), over the step time.
     run_bytes = float(np.mean([b.sum() for b in pass_b]))
