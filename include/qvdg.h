@@ -284,6 +284,14 @@ qvdg_status qvdg_plan_execute(qvdg_state* state, const qvdg_plan* plan, qvdg_sta
 qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
                                const qvdg_options* options, float* out, size_t capacity, size_t* num_passes);
 
+/* The same for the program a plan runs from |0...0> (from_zero != 0): its
+ * fusion, layout and pair passes (the layout search pairs more passes
+ * there), each row describing the whole pass (host only). from_zero = 0 is
+ * qvdg_plan_features. */
+qvdg_status qvdg_plan_features_from(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                                    const qvdg_options* options, int32_t from_zero, float* out, size_t capacity,
+                                    size_t* num_passes);
+
 /* The ops a plain plan's passes apply, in order, on logical qubits (host
  * only): each fused group as its product matrix, a pass applied gate by gate
  * as its member gates. The fusion is the one a plan picks for a state

@@ -74,6 +74,9 @@ _SIGNATURES = {
     "qvdg_plan_features": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(QvdgOp), ct.c_size_t,
                                       ct.POINTER(QvdgOptions), ct.POINTER(ct.c_float), ct.c_size_t,
                                       ct.POINTER(ct.c_size_t)]),
+    "qvdg_plan_features_from": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(QvdgOp), ct.c_size_t,
+                                           ct.POINTER(QvdgOptions), ct.c_int32, ct.POINTER(ct.c_float), ct.c_size_t,
+                                           ct.POINTER(ct.c_size_t)]),
     "qvdg_plan_fused_ops": (ct.c_int, [ct.c_uint32, ct.c_uint32, ct.POINTER(QvdgOp), ct.c_size_t,
                                        ct.POINTER(QvdgOptions), ct.c_int32, ct.POINTER(ct.c_uint32),
                                        ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint8),

@@ -60,14 +60,15 @@ def default_options():
     return options(4, staged=True)
 
 
-def plan_features(ops, num_qubits: int, opts, precision_bits: int = 32) -> np.ndarray:
-    """Per-pass feature rows of the plan `opts` builds for `ops` (host only)."""
+def plan_features(ops, num_qubits: int, opts, precision_bits: int = 32, from_zero: bool = False) -> np.ndarray:
+    """Per-pass feature rows of the plan `opts` builds for `ops` (host only),
+    for a general state or, with `from_zero`, the program run from |0...0>."""
     packed = PackedOps(ops)
     count = ct.c_size_t()
     # A plan has at most one pass per op: one call fills every row.
     rows = np.zeros((max(len(ops), 1), FEATURES), dtype=np.float32)
-    check(lib().qvdg_plan_features(num_qubits, precision_bits, packed.array, packed.count, ct.byref(opts),
-                                   _fptr(rows), rows.shape[0], ct.byref(count)))
+    check(lib().qvdg_plan_features_from(num_qubits, precision_bits, packed.array, packed.count, ct.byref(opts),
+                                        1 if from_zero else 0, _fptr(rows), rows.shape[0], ct.byref(count)))
     if count.value > rows.shape[0]:
         raise RuntimeError("more passes than ops")
     return rows[:count.value]

@@ -690,6 +690,12 @@ qvdg_status qvdg_expect_pauli(const qvdg_state* st, const uint32_t* qubits, cons
 
 qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
                                const qvdg_options* options, float* out, size_t capacity, size_t* num_passes) {
+  return qvdg_plan_features_from(num_qubits, precision_bits, ops, num_ops, options, 0, out, capacity, num_passes);
+}
+
+qvdg_status qvdg_plan_features_from(uint32_t num_qubits, uint32_t precision_bits, const qvdg_op* ops, size_t num_ops,
+                                    const qvdg_options* options, int32_t from_zero, float* out, size_t capacity,
+                                    size_t* num_passes) {
   return guarded([&] {
     require(precision_bits == 32 || precision_bits == 64, "precision must be 32 or 64 bits");
     require(num_qubits >= 1 && num_qubits <= 40, "a state needs 1 to 40 qubits");
@@ -700,8 +706,10 @@ qvdg_status qvdg_plan_features(uint32_t num_qubits, uint32_t precision_bits, con
     t.n = num_qubits;
     t.bits = int(precision_bits);
     for (uint32_t q = 0; q < num_qubits; ++q) t.layout.push_back(q);
-    // The program for any state: the cost model predicts whole passes.
-    const Program prog = build_program(t, lower_ops(ops, num_ops, num_qubits), opt, FusionSearch::Thorough, false);
+    // The program for any state, or the one a plan runs from |0...0> (its
+    // fusion, layout and pairing; the rows describe whole passes).
+    const Program prog =
+        build_program(t, lower_ops(ops, num_ops, num_qubits), opt, FusionSearch::Thorough, from_zero != 0);
     const size_t rows = prog.passes.size();
     if (num_passes) *num_passes = rows;
     if (out) std::memcpy(out, prog.features.data(), std::min(rows, capacity) * kPassFeatures * sizeof(float));

@@ -151,6 +151,9 @@ extern "C" {
     pub fn qvdg_plan_features(num_qubits: u32, precision_bits: u32, ops: *const qvdg_op, num_ops: usize,
                               options: *const qvdg_options, out: *mut c_float, capacity: usize,
                               num_passes: *mut usize) -> qvdg_status;
+    pub fn qvdg_plan_features_from(num_qubits: u32, precision_bits: u32, ops: *const qvdg_op, num_ops: usize,
+                                   options: *const qvdg_options, from_zero: i32, out: *mut c_float,
+                                   capacity: usize, num_passes: *mut usize) -> qvdg_status;
     pub fn qvdg_plan_fused_ops(num_qubits: u32, precision_bits: u32, ops: *const qvdg_op, num_ops: usize,
                                options: *const qvdg_options, from_zero: i32, num_targets: *mut u32,
                                num_controls: *mut u32, qubits: *mut u32, control_values: *mut u8,

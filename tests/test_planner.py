@@ -82,3 +82,26 @@ def test_pair_passes_in_plans():
     overlapping = [Op([8, 10, 12, 14, 16, 18], [], u), Op([8, 10, 12, 15, 17, 19], [], u)]
     rows = costmodel.plan_features(overlapping, 24, pairs)
     assert rows.shape[0] == 1 and rows[0, 21] == 1
+
+
+def test_layout_from_zero_pairs_more_passes():
+    """From |0...0> a plan may take any layout: the planner puts the qubits
+    touched last on the top bits, an early-touched qubit on bit 0, and
+    permutes the bits above 3 so that more passes pair (the pairing's layout
+    test on bit masks). The 30-qubit grid circuit (5x6, depth 20) then runs
+    in 33 passes with 12 pairs, against 35 passes and 10 pairs on the layout
+    a general state keeps; single-pass (math="tensor") plans keep their pass
+    count."""
+    import numpy as np
+
+    ops = library.random_grid_circuit(5, 6, 20, seed=2024).ops()
+    pairs = options(6, staged=False, math="tensor_pairs")
+    general = costmodel.plan_features(ops, 30, pairs)
+    zero = costmodel.plan_features(ops, 30, pairs, from_zero=True)
+    pz, pg = int(np.sum(zero[:, 21] == 1)), int(np.sum(general[:, 21] == 1))
+    assert pz >= 11 and pz > pg, (pz, pg)
+    assert zero.shape[0] < general.shape[0]
+    # every pass applies one fused op or two (a pair): the same 45 ops
+    assert zero.shape[0] + pz == general.shape[0] + pg
+    single = options(6, staged=False, math="tensor")
+    assert int(np.sum(costmodel.plan_features(ops, 30, single, from_zero=True)[:, 21] == 1)) == 0
