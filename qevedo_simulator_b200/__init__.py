@@ -14,9 +14,10 @@ libqvdgpu.so behind the C ABI of include/qvdg.h; there is no CPU fallback.
 
 from . import library, qasm
 from ._native import Batch, DeviceState, Plan, QvdgError, options, set_device
+from .sharded import ShardedStateVector
 from .circuit import Circuit, Gate, Op, gate_op
 from .simulator import RunResult, count_outcomes, estimate, run, statevector
 
 __all__ = ["Batch", "Circuit", "Gate", "Op", "gate_op", "DeviceState", "Plan", "QvdgError", "options", "set_device", "RunResult", "run",
-           "statevector", "count_outcomes", "estimate", "library", "qasm"]
+           "statevector", "count_outcomes", "estimate", "library", "qasm", "ShardedStateVector"]
 __version__ = "0.1.0"
