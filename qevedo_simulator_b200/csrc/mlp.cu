@@ -200,13 +200,21 @@ void ensure(qvdg_mlp* m, size_t rows) {
   m->cap = rows;
 }
 
+// Row-parallel launches take rows in the grid's y dimension (at most 65535
+// blocks of kTile rows): larger row counts go in chunks.
+constexpr int kChunkRows = 65535 * kTile;
+
 void forward(qvdg_mlp* m, const Acts& a, int rows) {
   const Views p = views(m->params, m->in, m->hid);
   const dim3 blk(kTile, kTile);
   const int h = int(m->hid), in = int(m->in);
-  k_dense_fwd<true><<<grid2(h, rows), blk, 0, m->stream>>>(a.X, rows, in, p.W1, p.b1, h, a.A1);
-  k_dense_fwd<true><<<grid2(h, rows), blk, 0, m->stream>>>(a.A1, rows, h, p.W2, p.b2, h, a.A2);
-  k_dense_fwd<false><<<grid2(1, rows), blk, 0, m->stream>>>(a.A2, rows, h, p.W3, p.b3, 1, a.y);
+  for (int r0 = 0; r0 < rows; r0 += kChunkRows) {
+    const int rc = std::min(kChunkRows, rows - r0);
+    const size_t o = size_t(r0);
+    k_dense_fwd<true><<<grid2(h, rc), blk, 0, m->stream>>>(a.X + o * in, rc, in, p.W1, p.b1, h, a.A1 + o * h);
+    k_dense_fwd<true><<<grid2(h, rc), blk, 0, m->stream>>>(a.A1 + o * h, rc, h, p.W2, p.b2, h, a.A2 + o * h);
+    k_dense_fwd<false><<<grid2(1, rc), blk, 0, m->stream>>>(a.A2 + o * h, rc, h, p.W3, p.b3, 1, a.y + o);
+  }
   QVDG_LAUNCH_CHECK();
 }
 
@@ -221,9 +229,17 @@ float backward(qvdg_mlp* m, const Acts& a, int rows) {
   k_mse<<<nb, 256, 0, m->stream>>>(a.y, a.t, rows, a.dy, a.partial);
   // output layer: dZ3 = dy (rows x 1)
   k_dense_dw<<<grid2(h, 1), blk, 0, m->stream>>>(a.dy, a.A2, rows, h, 1, g.W3, g.b3);
-  k_dense_dx<true><<<grid2(h, rows), blk, 0, m->stream>>>(a.dy, p.W3, rows, h, 1, a.A2, a.dZ2);
+  for (int r0 = 0; r0 < rows; r0 += kChunkRows) {
+    const int rc = std::min(kChunkRows, rows - r0);
+    const size_t o = size_t(r0);
+    k_dense_dx<true><<<grid2(h, rc), blk, 0, m->stream>>>(a.dy + o, p.W3, rc, h, 1, a.A2 + o * h, a.dZ2 + o * h);
+  }
   k_dense_dw<<<grid2(h, h), blk, 0, m->stream>>>(a.dZ2, a.A1, rows, h, h, g.W2, g.b2);
-  k_dense_dx<true><<<grid2(h, rows), blk, 0, m->stream>>>(a.dZ2, p.W2, rows, h, h, a.A1, a.dZ1);
+  for (int r0 = 0; r0 < rows; r0 += kChunkRows) {
+    const int rc = std::min(kChunkRows, rows - r0);
+    const size_t o = size_t(r0);
+    k_dense_dx<true><<<grid2(h, rc), blk, 0, m->stream>>>(a.dZ2 + o * h, p.W2, rc, h, h, a.A1 + o * h, a.dZ1 + o * h);
+  }
   k_dense_dw<<<grid2(in, h), blk, 0, m->stream>>>(a.dZ1, a.X, rows, in, h, g.W1, g.b1);
   QVDG_LAUNCH_CHECK();
   std::vector<float> part(static_cast<size_t>(nb));

@@ -337,10 +337,11 @@ bool zero_start_layout(const std::vector<PlannedPass>& passes, uint32_t n, bool 
     const uint32_t other = at[p];
     std::swap(layout[q], layout[other]);
   };
-  // The top bits.
+  // The top bits (bit 0's qubit among the candidates: a qubit touched late
+  // gains nothing there).
   std::vector<uint32_t> late;
   for (uint32_t q = 0; q < n; ++q)
-    if (layout[q] >= 4 && layout[q] < top && first[q] > 0) late.push_back(q);
+    if ((layout[q] == 0 || (layout[q] >= 4 && layout[q] < top)) && first[q] > 0) late.push_back(q);
   std::stable_sort(late.begin(), late.end(), [&](uint32_t a, uint32_t b) { return first[a] > first[b]; });
   if (late.size() > kZeroStartTop) late.resize(kZeroStartTop);
   uint64_t fixed = 0;

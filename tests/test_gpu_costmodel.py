@@ -60,6 +60,28 @@ def test_kernels_match_numpy(inputs, hidden, rows):
         assert np.array_equal(m.get_params(), params * np.float32(0.5))
 
 
+def test_kernels_over_a_million_rows():
+    """Row-parallel launches take rows in the grid's y dimension (at most
+    65535 blocks of 16 rows): more rows than that (training sets of over a
+    million pass timings) go in chunks. Forward, gradients and the final
+    training loss over 1.1M rows match numpy."""
+    rows, inputs, hidden = 1_100_000, 7, 20
+    rng = np.random.Generator(np.random.PCG64(17))
+    x = rng.standard_normal((rows, inputs)).astype(np.float32)
+    t = rng.standard_normal(rows).astype(np.float32)
+    with costmodel.MLP(inputs, hidden, seed=5) as m:
+        params = m.get_params()
+        y_ref, grads = numpy_mlp(params, x, inputs, hidden)
+        y = m.forward(x)
+        assert np.allclose(y, y_ref, rtol=1e-4, atol=1e-4 * np.abs(y_ref).max())
+        loss, g = m.gradients(x, t)
+        loss_ref, g_ref = grads(t)
+        assert loss == pytest.approx(loss_ref, rel=1e-3)
+        assert np.abs(g - g_ref).max() <= 1e-3 * np.abs(g_ref).max() + 1e-6
+        final = m.train(x, t, epochs=1, batch=4096, lr=1e-3, seed=3)
+        assert np.isfinite(final) and final < 1.05 * loss
+
+
 def test_training_fits_a_smooth_function():
     rng = np.random.Generator(np.random.PCG64(9))
     x = rng.uniform(0, 1, (2048, 32)).astype(np.float32)
