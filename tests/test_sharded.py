@@ -74,6 +74,25 @@ def _circuit(n, seed):
     ops.append(Op([n - 1, n - 2, 1], [], np.diag(np.exp(1j * rng.uniform(0, 6.3, 8)))))
     ops.append(Op([n - 1], [(2, True)], np.diag([1.0, np.exp(0.7j)])))
     ops.append(Op([0], [(n - 1, True), (n - 2, False)], np.array([[0, 1], [1, 0]], dtype=np.complex128)))
+    # diagonals whose targets may all be global: a phase per rank, with and
+    # without a local control
+    ops.append(Op([n - 1], [], np.diag([np.exp(-0.3j), np.exp(0.3j)])))
+    ops.append(Op([n - 2, n - 1], [(0, False)], np.diag(np.exp(1j * np.array([0.1, 0.5, 0.9, 1.3])))))
+    ops.append(Op([n - 1, n - 2], [(0, True), (1, True)], np.diag(np.exp(1j * np.array([0.2, 0.4, 0.6, 0.8])))))
+    ops.extend(library.mixed_ops(n, 1, seed=seed + 2))
+    return ops
+
+
+def _global_diagonals(global_q, local_q):
+    from qevedo_simulator_b200 import Op
+
+    g, l0, l1 = global_q[-1], local_q[0], local_q[1]
+    ops = [Op([g], [], np.diag([np.exp(-0.3j), np.exp(0.3j)])),
+           Op([g], [(l0, True)], np.diag([np.exp(0.2j), np.exp(-0.5j)])),
+           Op([l1, g], [(l0, False)], np.diag(np.exp(1j * np.array([0.1, 0.5, 0.9, 1.3]))))]
+    if len(global_q) > 1:
+        ops.append(Op([global_q[0], g], [(l1, True)], np.diag(np.exp(1j * np.array([0.2, 0.4, 0.6, 0.8])))))
+        ops.append(Op([l0], [(global_q[0], True)], np.array([[0, 1], [1, 0]], dtype=np.complex128)))
     return ops
 
 
@@ -85,7 +104,7 @@ def _rank(rank, world, port, n, seed, out):
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from qevedo_simulator_b200.sharded import ShardedStateVector
-    from test_sharded import OracleEngine, _circuit
+    from test_sharded import OracleEngine, _circuit, _global_diagonals
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -95,8 +114,13 @@ def _rank(rank, world, port, n, seed, out):
         sv = ShardedStateVector(n, engine=OracleEngine(n - k))
         ops = _circuit(n, seed)
         info = sv.apply_ops(ops)
+        # Diagonals on the qubits that are global now (every rank knows the
+        # same placement): phases per rank, with and without local controls.
+        more = _global_diagonals(sv.global_q, sv.local_q)
+        after = sv.apply_ops(more)
+        assert after["exchanges"] == 0
         amps = sv.amplitudes()
-        out.put((rank, amps, info, sv.norm_sqr(), sv.probability_one(n - 1), sv.probability_one(0)))
+        out.put((rank, amps, info, sv.norm_sqr(), sv.probability_one(n - 1), sv.probability_one(0), more))
     finally:
         dist.destroy_process_group()
 
@@ -115,8 +139,9 @@ def test_sharded_state_matches_the_oracle(world, n):
     for p in procs:
         p.join(120)
         assert p.exitcode == 0
-    ref = oracle.naive_statevector(_circuit(n, 11 + world), n)
-    for rank, amps, info, norm, p_top, p_low in got:
+    more = got[0][6]
+    ref = oracle.naive_statevector(_circuit(n, 11 + world) + more, n)
+    for rank, amps, info, norm, p_top, p_low, _ in got:
         assert np.abs(amps - ref).max() < 1e-12, rank
         assert info["exchanges"] >= 1  # the ops on the top qubits moved them
         assert abs(norm - 1.0) < 1e-12
