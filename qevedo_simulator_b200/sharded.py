@@ -172,7 +172,14 @@ class DistTransport:
 class ShardedStateVector:
     """An n-qubit state over the ranks of a transport (by default the
     torch.distributed group: a power of two of ranks, each with its own
-    GPU), starting in |0...0>."""
+    GPU), starting in |0...0>. Under NCCL each rank first selects its GPU
+    for torch and for the library (`torch.cuda.set_device(local_rank)`,
+    `qevedo_simulator_b200.set_device(local_rank)`).
+
+        >>> sv = ShardedStateVector(36)          # 4 ranks: 2^34 amplitudes each
+        >>> sv.apply_ops(circuit.ops())          # {'exchanges': ..., 'batches': ...}
+        >>> sv.probability_one(35), sv.norm_sqr()
+    """
 
     def __init__(self, num_qubits: int, precision_bits: int = 32, group=None, engine=None, lookahead: int = 32,
                  transport=None):
