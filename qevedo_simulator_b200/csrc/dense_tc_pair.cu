@@ -73,13 +73,6 @@ __device__ __forceinline__ void load16(const float2* psi, uint64_t base, const u
   }
 }
 
-// The same members into L2 (no registers held while the lines arrive).
-template <int VW>
-__device__ __forceinline__ void prefetch16(const float2* psi, uint64_t base, const uint32_t* lo) {
-#pragma unroll
-  for (int m = 0; m < 16 / VW; ++m) asm volatile("prefetch.global.L2 [%0];" ::"l"(psi + base + lo[VW * m]));
-}
-
 // Eight members 8 hh .. 8 hh + 7 of one group from registers to HBM.
 template <int VW>
 __device__ __forceinline__ void store8(float2* psi, uint64_t base, const uint32_t* lo, int hh, const float* re,
