@@ -45,6 +45,10 @@ def test_host_only_calls_need_no_device():
     assert "precision" in lib.qvdg_last_error().decode()
     assert lib.qvdg_state_destroy(None) == 0
     assert lib.qvdg_norm_sqr(None, None) == 1
+    n = ct.c_size_t(99)
+    assert lib.qvdg_plan_features_from(50, 32, None, 0, None, 1, None, 0, ct.byref(n)) == 1
+    assert "qubits" in lib.qvdg_last_error().decode()
+    assert lib.qvdg_plan_features_from(4, 32, None, 0, None, 1, None, 0, ct.byref(n)) == 0 and n.value == 0
 
 
 def test_batch_validation_needs_no_device():

@@ -105,3 +105,21 @@ def test_layout_from_zero_pairs_more_passes():
     assert zero.shape[0] + pz == general.shape[0] + pg
     single = options(6, staged=False, math="tensor")
     assert int(np.sum(costmodel.plan_features(ops, 30, single, from_zero=True)[:, 21] == 1)) == 0
+
+
+@pytest.mark.parametrize("kind", ["qft", "mixed"])
+def test_programs_from_zero_apply_every_fused_op(kind):
+    """From |0...0> (zero-start passes, layout search, pair passes) a plan
+    still applies each fused op in exactly one pass: the passes plus the
+    pairs (a pair applies two ops) give the fused-op count of the same
+    from-zero fusion, for the QFT and for mixed circuits."""
+    import numpy as np
+
+    n = 26
+    ops = library.qft(n).ops() if kind == "qft" else library.mixed_ops(n, 8, seed=4)
+    for opts in (options(6, staged=False, math="tensor_pairs"), options(6, staged=False, math="tensor"),
+                 options(5, staged=False, math="tensor")):
+        rows = costmodel.plan_features(ops, n, opts, from_zero=True)
+        fused = costmodel.fused_ops(ops, n, opts, from_zero=True)
+        pairs = int(np.sum(rows[:, 21] == 1))
+        assert rows.shape[0] + pairs == len(fused), (kind, opts.math, opts.max_fused_qubits)
