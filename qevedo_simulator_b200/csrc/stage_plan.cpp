@@ -372,22 +372,21 @@ bool zero_start_layout(const std::vector<PlannedPass>& passes, uint32_t n, bool 
     if (!early.empty()) std::swap(layout[q0], layout[early[0]]);
     return layout != given;
   }
-  // Bit 0 by a short climb per candidate, then the full climb.
+  // Bit 0 by a short climb per candidate (on host threads, each seeded by
+  // its candidate: the result does not depend on the thread count), then
+  // the full climb.
   const size_t tries = std::min<size_t>(early.size(), thorough ? 24 : 8);
-  std::vector<uint32_t> best = layout;
-  size_t best_pairs = 0;
-  bool any = false;
-  for (size_t k = 0; k < tries; ++k) {
-    std::vector<uint32_t> l = layout;
-    std::swap(l[q0], l[early[k]]);
-    const size_t c = search.climb(movable_of(l), 128, thorough ? 2 : 1, rng, l);
-    if (!any || c > best_pairs) {
-      best = l;
-      best_pairs = c;
-      any = true;
-    }
-  }
-  layout = best;
+  std::vector<std::vector<uint32_t>> found(tries, layout);
+  std::vector<size_t> made(tries, 0);
+  parallel_for(tries, [&](size_t k) {
+    std::mt19937 r(uint32_t(2024 + k));
+    std::swap(found[k][q0], found[k][early[k]]);
+    made[k] = search.climb(movable_of(found[k]), 128, thorough ? 2 : 1, r, found[k]);
+  });
+  size_t pick = tries;
+  for (size_t k = 0; k < tries; ++k)
+    if (pick == tries || made[k] > made[pick]) pick = k;
+  if (pick < tries) layout = found[pick];
   search.climb(movable_of(layout), thorough ? 1024 : 256, thorough ? 4 : 2, rng, layout);
   return layout != given;
 }
